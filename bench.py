@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark of the FP64 pseudo-spectral SSP-RK3 step (forced Kolmogorov flow).
+
+Workload (default): N^3 = 128^3 on the 2pi-periodic box, f = (sin 4y, 0, 0),
+Re = 200, laminar profile plus a seeded 1e-3 divergence-free perturbation,
+dt from CFL 0.3 on the laminar peak velocity, FP64 throughout.  A "step" is
+one RK3_SSP step (3 right-hand sides).  The metric is RK3 steps/s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--N 128]
+
+--impl ours       : the CUDA library (libns3d_b200.so) through its C ABI.
+--impl reference  : the reference's own CUDA path (unmodified sources built
+                    for sm_100a with cuFFT, oracle/_ref) on the same GPU and
+                    workload.
+Multi-GPU runs (torchrun) are independent replicas, one per GPU (the path
+does not shard); value = steps of all ranks / max elapsed over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--N", type=int, default=128)
+    ap.add_argument("--Re", type=float, default=200.0)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def traffic_from_profiles(kernel: str, N: int):
+    """DRAM bytes per launch from the committed ncu summary, if there is one."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        # | kernel | N | dram_bytes_per_launch | ...
+        c = [x.strip() for x in line.strip().strip("|").split("|")]
+        if len(c) >= 3 and c[0] == kernel and c[1] == str(N):
+            try:
+                return float(c[2])
+            except ValueError:
+                return None
+    return None
+
+
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(x: float, pg):
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    import torch
+
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+
+
+def workload(N, Re, seed):
+    from ns3dperiodic_b200 import workload as W
+
+    U, F = W.kolmogorov_state(N, Re, seed)
+    return U, F, W.kolmogorov_dt(N, Re)
+
+
+def sizes(N):
+    nc = N * N * (N // 2 + 1)
+    Sc, Sr = 16 * nc, 8 * N ** 3
+    return nc, Sc, Sr
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (numpy/scipy pocketfft) on the host cores
+# ---------------------------------------------------------------------------
+def cpu_baseline(N, Re, seed):
+    from oracle import ns3d_oracle as O
+
+    cores = os.cpu_count() or 1
+    os.environ["NS3D_ORACLE_THREADS"] = str(cores)
+    U, F, dt = workload(N, Re, seed)
+    g = O.Grid(N, N, N)
+    t0 = time.perf_counter()
+    U = O.rk3_ssp(g, U, F, dt, Re)  # warm-up (plans, page faults)
+    t1 = time.perf_counter()
+    k = max(1, min(50, int(15.0 / max(t1 - t0, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        U = O.rk3_ssp(g, U, F, dt, Re)
+    el = time.perf_counter() - t0
+    return {"value": k / el, "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"{k} RK3 steps of the {N}^3 Kolmogorov workload (oracle: numpy + "
+                      f"scipy.fft pocketfft, workers={cores}) after 1 warm-up step, {el:.1f} s"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank, local, pg):
+    import torch
+
+    from ns3dperiodic_b200 import Solver
+
+    N, Re = args.N, args.Re
+    U0, F0, dt = workload(N, Re, args.seed + rank)
+    nc, Sc, Sr = sizes(N)
+    S = Solver(N, N, N)
+    stream = torch.cuda.Stream()
+    S.set_stream(stream)
+    U = S.to_device(U0)
+    F = S.to_device(F0)
+    torch.cuda.synchronize()
+    S.set_forcing(F)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            S.rk3_ssp(U, dt, Re)
+    barrier(pg)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        for _ in range(args.steps):
+            S.rk3_ssp(U, dt, Re)
+        ev1.record(stream)
+    ev1.synchronize()
+    ms_local = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    barrier(pg)
+    ms = max_over_ranks(ms_local, pg)
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+
+    # per-pass timing (CUDA events on the launching stream), dominant kernel
+    names = ["inv_x", "inv_y", "z", "fwd_y", "fwd_x"]
+    alg = [9 * Sc, 15 * Sc, 12 * Sc, 6 * Sc, 9 * Sc]  # algorithmic bytes per launch
+    with torch.cuda.stream(stream):
+        pm = S.profile_passes(U, dt, Re, reps=20)
+    dom = max(range(5), key=lambda i: pm[i])
+    peak, peak_src = peaks()
+    achieved = alg[dom] / (pm[dom] * 1e-3) / 1e9
+    kname = {0: "inv_x_kernel", 1: "inv_y_kernel", 2: "z_kernel", 3: "fwd_y_kernel",
+             4: "fwd_x_kernel"}[dom]
+    traffic = traffic_from_profiles(kname, N)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": traffic, "peak_source": peak_src,
+                "alg_bytes_per_launch": alg[dom], "ms_per_launch": round(pm[dom], 5),
+                "pass_ms": {n: round(t, 5) for n, t in zip(names, pm)},
+                "pass_frac": {n: round(a / (t * 1e-3) / 1e9 / peak, 4)
+                              for n, a, t in zip(names, alg, pm)}}
+
+    # e2e through the public API with host buffers
+    K = args.e2e_steps or args.steps
+    hU = [torch.from_numpy(u).pin_memory() for u in U0]
+    hF = [torch.from_numpy(f).pin_memory() for f in F0]
+    outU = [torch.empty_like(h).pin_memory() for h in hU]
+    Ue = S.zeros()
+    Fe = S.zeros()
+    barrier(pg)
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for d, h in zip(Ue + Fe, hU + hF):
+            d.copy_(h, non_blocking=True)
+        stream.synchronize()
+        S.set_forcing(Fe)
+        diag = None
+        for _ in range(K):
+            S.rk3_ssp(Ue, dt, Re)
+            diag = S.diagnostics(Ue)  # energy, dissipation, max|div| read back each step
+        for h, d in zip(outU, Ue):
+            h.copy_(d, non_blocking=True)
+        stream.synchronize()
+    el = time.perf_counter() - t0
+    el = max_over_ranks(el, pg)
+    e2e = {"value": round(world * K / el, 3), "unit": "steps/s",
+           "h2d_bytes_per_step": round(6 * Sc / K, 1),
+           "d2h_bytes_per_step": round(24 + 3 * Sc / K, 1),
+           "steps": K,
+           "protocol": "pinned host state+forcing -> device, K x (ns3d_rk3_step + "
+                       "ns3d_diagnostics read-back), final state -> host; wall clock"}
+    S.close()
+    p3l = 159 * Sc + 18 * Sr
+    line = {
+        "metric": f"RK3 steps/s (Kolmogorov {N}^3 FP64)",
+        "value": round(value, 3),
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"kolmogorov_{N}^3_fp64", "N": N, "Re": Re, "dt": dt,
+                   "forcing": "sin(4y) x", "perturbation": "seeded 1e-3, |k|^-2 on 1<=|k|<=8",
+                   "parallelism": f"replicas x{world}",
+                   "l2": f"working set {(24 * Sc) / 1e6:.0f} MB (state + scratch) > 126 MB L2",
+                   "mpts_steps_per_s": round(value * N ** 3 / 1e6, 1),
+                   "p3l_bytes_per_step": p3l,
+                   "p3l_gbs": round(p3l / (ms_step * 1e-3) / 1e9, 1),
+                   "p3l_frac": round(p3l / (ms_step * 1e-3) / 1e9 / peak, 4),
+                   "diag_last": diag},
+        "roofline": roofline,
+        "e2e": e2e,
+        "gpu_launches": 15 * args.steps,
+        "clocks": clocks,
+    }
+    return line
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CUDA build
+# ---------------------------------------------------------------------------
+def run_reference(args, world, rank, local, pg):
+    from oracle import ref_lib
+
+    if rank != 0:
+        return None
+    if not ref_lib.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libns3d_ref.so not built "
+                                                    "(needs the reference tree to compile)"}
+    N, Re = args.N, args.Re
+    U0, F0, dt = workload(N, Re, args.seed)
+    nc, Sc, Sr = sizes(N)
+    sampler = ClockSampler(local)
+    with ref_lib.RefSolver(N, N, N) as R:
+        R.set_u(U0)
+        R.set_f(F0)
+        R.rk3(args.warmup, dt, Re)
+        sampler.start()
+        time.sleep(0.3)
+        ms = R.time_rk3(args.steps, dt, Re)
+        clocks = sampler.stop()
+        value = args.steps / (ms / 1e3)
+        K = args.e2e_steps or args.steps
+        t0 = time.perf_counter()
+        R.set_u(U0)
+        R.set_f(F0)
+        for _ in range(K):
+            R.rk3(1, dt, Re)
+            R.diag()
+        R.get_u()
+        el = time.perf_counter() - t0
+    p3l = 159 * Sc + 18 * Sr
+    return {
+        "impl": "reference",
+        "metric": f"RK3 steps/s (Kolmogorov {N}^3 FP64)",
+        "value": round(value, 3),
+        "unit": "steps/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"kolmogorov_{N}^3_fp64", "N": N, "Re": Re, "dt": dt,
+                   "reference": "unmodified reference CUDA sources (RK3_SSP, cuFFT D2Z/Z2D) "
+                                "built for sm_100a, legacy default stream",
+                   "p3l_gbs": round(p3l / (ms / args.steps * 1e-3) / 1e9, 1)},
+        "e2e": {"value": round(K / el, 3), "unit": "steps/s",
+                "h2d_bytes_per_step": round(6 * Sc / K, 1),
+                "d2h_bytes_per_step": round(16 + 3 * Sc / K, 1), "steps": K,
+                "protocol": "host state+forcing -> device, K x (RK3_SSP + the main loop's "
+                            "energy/dissipation diagnostics), final state -> host; wall clock"},
+        "clocks": clocks,
+    }
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, world, rank, local, pg)
+        else:
+            line = run_ours(args, world, rank, local, pg)
+            if rank == 0 and world == 1 and not args.no_cpu_baseline:
+                line["cpu_baseline"] = cpu_baseline(args.N, args.Re, args.seed)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

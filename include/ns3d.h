@@ -1,0 +1,234 @@
+/*
+ * ns3d.h - C ABI of the B200 (sm_100a) pseudo-spectral Navier-Stokes path.
+ *
+ * Drop-in for the RK3 / tangent / Krylov-matvec entry points of
+ * evstigneevnm/NS3DPeriodic.  Every velocity field is a DEVICE array in the
+ * reference's own layout: [Nx][Ny][Mz] complex doubles (interleaved re, im;
+ * cufftDoubleComplex), Mz = Nz/2 + 1, element (j,k,l) at j*Ny*Mz + k*Mz + l
+ * (Source/Macros.h:11 IN(i,j,k) with Nz = Mz).  Spectra are unnormalised
+ * (forward D2Z without scaling, inverse followed by 1/(Nx Ny Nz)), exactly as
+ * Source/math_support.cu:301-334.  Viscosity is 1/Re.
+ *
+ * The reference keeps cuFFT plans, the 2/3 scratch and the wave-number /
+ * Leray / mask tables in file-static state set up by main()
+ * (Source/NS3D_periodic.cu:1141-1272).  Here a handle owns the equivalent:
+ * its own scratch, tables computed on the fly inside the kernels, and one
+ * CUDA stream.  Handles are independent and re-entrant; one handle must not
+ * be used from two host threads at once.
+ *
+ * All functions return an ns3d_status; nothing prints or exits.  Functions
+ * that launch work are asynchronous on the handle's stream unless stated.
+ * The default stream of a handle is a blocking stream, so it is ordered with
+ * work on the legacy default stream (the reference's stream).
+ */
+#ifndef NS3D_H_
+#define NS3D_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ns3d_solver ns3d_solver;
+
+typedef struct ns3d_complex {
+  double x, y;
+} ns3d_complex;
+
+typedef enum ns3d_status {
+  NS3D_OK = 0,
+  NS3D_ERR_BAD_ARG = 1,     /* null handle/pointer, non-positive size, bad dt/Re */
+  NS3D_ERR_UNSUPPORTED = 2, /* a grid extent without a compiled FFT plan */
+  NS3D_ERR_OOM = 3,         /* device allocation failed */
+  NS3D_ERR_CUDA = 4,        /* a CUDA launch or API call failed (see ns3d_last_error) */
+  NS3D_ERR_NONFINITE = 5,   /* a diagnostic reduction met NaN/Inf */
+  NS3D_ERR_TIMEOUT = 6      /* a bounded device wait gave up */
+} ns3d_status;
+
+/* ----------------------------------------------------------------------- */
+/* lifetime                                                                 */
+/* ----------------------------------------------------------------------- */
+
+/* Creates a solver for an Nx x Ny x Nz grid on a box Lx x Ly x Lz, on the
+ * current CUDA device.  Replaces cufftPlan3d + init_fft_plans
+ * (Source/math_support.h:15), the host table builders build_*
+ * (Source/math_support.h:49-58, called with Mz as Nz at
+ * Source/NS3D_periodic.cu:1153-1161) and init_dealiasing
+ * (Source/advection_2_3.h:40).  Supported extents: ns3d_supported_extent(). */
+ns3d_status ns3d_create(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                        ns3d_solver** out);
+
+/* Releases the handle.  Replaces clean_dealiasing (Source/advection_2_3.h:42). */
+ns3d_status ns3d_destroy(ns3d_solver* h);
+
+/* 1 if n has a compiled FFT plan (8, 16, 24, 32, 48, 64, 96, 128, 192, 256,
+ * 384, 512), else 0.  Host only. */
+int ns3d_supported_extent(int n);
+
+/* Uses `stream` (a cudaStream_t, may be 0 for the legacy default stream) for
+ * every later launch of this handle. */
+ns3d_status ns3d_set_stream(ns3d_solver* h, void* stream);
+
+/* Blocks until the handle's stream is idle. */
+ns3d_status ns3d_synchronize(ns3d_solver* h);
+
+/* Human-readable text of the last error on this handle ("" if none). */
+const char* ns3d_last_error(const ns3d_solver* h);
+const char* ns3d_status_string(ns3d_status s);
+
+/* Device bytes the handle holds (scratch + tables). */
+size_t ns3d_device_bytes(const ns3d_solver* h);
+
+/* ----------------------------------------------------------------------- */
+/* forcing                                                                  */
+/* ----------------------------------------------------------------------- */
+
+/* Captures the body force f_hat (3 device fields, reference layout) used by
+ * every later explicit step and RHS evaluation.  The reference passes
+ * fx_hat_d.. to each call (Source/RK_time_step.h:26); the handle instead
+ * scans the field once (synchronously) and keeps it as a sparse list of its
+ * non-zero modes when there are at most 4096 of them, else references the
+ * caller's arrays, which must then stay alive and unchanged.  Null pointers
+ * clear the forcing. */
+ns3d_status ns3d_set_forcing(ns3d_solver* h, const ns3d_complex* fx, const ns3d_complex* fy,
+                             const ns3d_complex* fz);
+
+/* Number of non-zero forcing modes kept (-1: dense forcing referenced). */
+int ns3d_forcing_modes(const ns3d_solver* h);
+
+/* ----------------------------------------------------------------------- */
+/* time stepping: Source/RK_time_step.h                                     */
+/* ----------------------------------------------------------------------- */
+
+/* One Shu-Osher SSP-RK3 step in place: RK3_SSP (Source/RK_time_step.h:26,
+ * Source/RK_time_step.cu:310-327).  The reference's scratch arguments
+ * (u_1..u_3, Q, div, tables) are owned by the handle. */
+ns3d_status ns3d_rk3_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                          double dt, double Re);
+
+/* nsteps RK3 steps in place, replayed from one captured CUDA graph (the time
+ * loop of Source/NS3D_periodic.cu:1303-1315 without diagnostics). */
+ns3d_status ns3d_rk3_steps(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                           double dt, double Re, int nsteps);
+
+/* One explicit Euler stage u <- u + dt L(u): single_time_step
+ * (Source/RK_time_step.h:19, Source/RK_time_step.cu:248-263). */
+ns3d_status ns3d_euler_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                            double dt, double Re);
+
+/* rhs = -P.Q(u) - |k|^2/Re u + f: return_RHS (Source/RK_time_step.h:34,
+ * Source/RK_time_step.cu:231-245).  rhs must not alias u. */
+ns3d_status ns3d_rhs(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                     const ns3d_complex* uz, ns3d_complex* rx, ns3d_complex* ry, ns3d_complex* rz,
+                     double Re);
+
+/* Qhat = FFT[(Mu.grad)(Mu)] with Re(Qhat)=0, Qhat(0)=0:
+ * calculate_convolution_2p3 (Source/advection_2_3.h:44). */
+ns3d_status ns3d_convolution(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                             const ns3d_complex* uz, ns3d_complex* Qx, ns3d_complex* Qy,
+                             ns3d_complex* Qz);
+
+/* Qhat = FFT[(Mv.grad)(Mu) + (Mu.grad)(Mv)], Re(Qhat)=0, Qhat(0)=0:
+ * calculate_convolution_2p3_UV (Source/advection_2_3.h:46). */
+ns3d_status ns3d_convolution_uv(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                const ns3d_complex* uz, const ns3d_complex* vx,
+                                const ns3d_complex* vy, const ns3d_complex* vz, ns3d_complex* Qx,
+                                ns3d_complex* Qy, ns3d_complex* Qz);
+
+/* ----------------------------------------------------------------------- */
+/* tangent (Jacobian-vector) steppers                                       */
+/* ----------------------------------------------------------------------- */
+
+/* One tangent step: Heun on v about an RK3 base step of u, both in place:
+ * RK3_SSP_UV (Source/RK_time_step.h:31, Source/RK_time_step.cu:342-355). */
+ns3d_status ns3d_jvp_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                          ns3d_complex* vx, ns3d_complex* vy, ns3d_complex* vz, double dt,
+                          double Re);
+
+/* nsteps tangent steps (the Timesteps_period loop of
+ * NSCallMatrixVector_exponential, Source/NS3D_periodic.cu:444-470). */
+ns3d_status ns3d_jvp_steps(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                           ns3d_complex* vx, ns3d_complex* vy, ns3d_complex* vz, double dt,
+                           double Re, int nsteps);
+
+/* v <- J(u) v = -P.B(u,v) - |k|^2/Re v in place: RK3_SSP_UV_RHS
+ * (Source/RK_time_step.h:28, Source/RK_time_step.cu:330-338). */
+ns3d_status ns3d_linearised_rhs(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                const ns3d_complex* uz, ns3d_complex* vx, ns3d_complex* vy,
+                                ns3d_complex* vz, double Re);
+
+/* v <- (v - dt P.B(u,v)) / (1 + dt |k|^2/Re) in place: single_time_step_iUV_RHS
+ * (Source/RK_time_step.h:23, Source/RK_time_step.cu:296-306). */
+ns3d_status ns3d_implicit_tangent_step(ns3d_solver* h, const ns3d_complex* ux,
+                                       const ns3d_complex* uy, const ns3d_complex* uz,
+                                       ns3d_complex* vx, ns3d_complex* vy, ns3d_complex* vz,
+                                       double dt, double Re);
+
+/* ----------------------------------------------------------------------- */
+/* Krylov adapters: Source/NS3D_periodic.cu:173-385                          */
+/* ----------------------------------------------------------------------- */
+
+/* Length of a reduced Krylov vector: 3*(Nx*Ny*Mz - 1). */
+int64_t ns3d_krylov_length(const ns3d_solver* h);
+
+/* vec = [Im vx(1..), Im vy(1..), Im vz(1..)]: A_vector_from_velocities_reduced_kernel
+ * (Source/NS3D_periodic.cu:271-284).  vec is a device array of doubles. */
+ns3d_status ns3d_pack_reduced(ns3d_solver* h, const ns3d_complex* vx, const ns3d_complex* vy,
+                              const ns3d_complex* vz, double* vec);
+
+/* v = i*vec, Re := 0, mode 0 := 0: velocities_from_A_vector_reduced_kernel
+ * (Source/NS3D_periodic.cu:173-200). */
+ns3d_status ns3d_unpack_reduced(ns3d_solver* h, const double* vec, ns3d_complex* vx,
+                                ns3d_complex* vy, ns3d_complex* vz);
+
+/* vec_out = J(u) vec_in - vec_in/tau on reduced vectors (device arrays):
+ * NSCallMatrixVector_reduced (tau <= 0) and
+ * NSCallMatrixVector_reduced_Newton_Globalization (tau > 0),
+ * Source/NS3D_periodic.cu:340-385. */
+ns3d_status ns3d_matvec_reduced(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                const ns3d_complex* uz, const double* vec_in, double* vec_out,
+                                double Re, double tau);
+
+/* ----------------------------------------------------------------------- */
+/* diagnostics (Source/math_support.cu:720-806, Source/divergence.cu:8-31)    */
+/* ----------------------------------------------------------------------- */
+
+/* Synchronous.  energy = sum 0.5 (uy^2 + uz^2) dx dy over the physical grid
+ * (get_kinetic_energy), dissipation = the reference's central-difference
+ * sum (get_dissipation), div_max = max |i k . u_hat| (solve_divergence with
+ * dt = 1).  Returns NS3D_ERR_NONFINITE if any of them is not finite.  Any
+ * output pointer may be null. */
+ns3d_status ns3d_diagnostics(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                             const ns3d_complex* uz, double* energy, double* dissipation,
+                             double* div_max);
+
+/* Times the five pass kernels of one RHS evaluation (the first RK3 stage:
+ * inv_x, inv_y, z, fwd_y, fwd_x; u is read, handle scratch is written) with
+ * CUDA events on the handle's stream, `reps` times after one warm-up, and
+ * stores the mean milliseconds per launch in ms[0..4].  Synchronous.  No
+ * reference counterpart: it serves the roofline report. */
+ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                const ns3d_complex* uz, double dt, double Re, int reps,
+                                double* ms);
+
+/* ----------------------------------------------------------------------- */
+/* host-only helpers (no GPU needed)                                        */
+/* ----------------------------------------------------------------------- */
+
+/* The 2/3 mask as a kz cut-off per (x, y) column: mode (j,k,l) is kept iff
+ * l < qcut[j*Ny + k] (and (j,k,l) != 0), evaluated with the arithmetic of
+ * build_mask_matrix (Source/math_support.cu:471-519) called with Mz as Nz.
+ * Returns NS3D_ERR_BAD_ARG if the mask is not a kz-prefix in some column. */
+ns3d_status ns3d_mask_cutoff(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                             uint16_t* qcut);
+
+/* Twiddle table tw[2e] = cos(2 pi e/N), tw[2e+1] = sin(2 pi e/N), e < N. */
+ns3d_status ns3d_twiddles(int N, double* tw);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NS3D_H_ */

@@ -1,0 +1,108 @@
+"""ctypes binding of libns3d_b200.so (the C ABI declared in include/ns3d.h).
+
+The CUDA library is the product path; there is no fallback.  If the shared
+library is missing or fails to load, importing any compute entry point
+raises :class:`Ns3dLibraryError`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libns3d_b200.so")
+
+STATUS = {
+    0: "ok",
+    1: "bad argument",
+    2: "unsupported grid extent",
+    3: "out of device memory",
+    4: "CUDA error",
+    5: "non-finite value",
+    6: "device wait timed out",
+}
+
+# every symbol include/ns3d.h declares
+EXPORTS = (
+    "ns3d_create", "ns3d_destroy", "ns3d_supported_extent", "ns3d_set_stream",
+    "ns3d_synchronize", "ns3d_last_error", "ns3d_status_string", "ns3d_device_bytes",
+    "ns3d_set_forcing", "ns3d_forcing_modes", "ns3d_rk3_step", "ns3d_rk3_steps",
+    "ns3d_euler_step", "ns3d_rhs", "ns3d_convolution", "ns3d_convolution_uv",
+    "ns3d_jvp_step", "ns3d_jvp_steps", "ns3d_linearised_rhs", "ns3d_implicit_tangent_step",
+    "ns3d_krylov_length", "ns3d_pack_reduced", "ns3d_unpack_reduced", "ns3d_matvec_reduced",
+    "ns3d_diagnostics", "ns3d_profile_passes", "ns3d_mask_cutoff", "ns3d_twiddles",
+)
+
+
+class Ns3dLibraryError(RuntimeError):
+    pass
+
+
+class Ns3dError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        msg = f"{where}: {STATUS.get(status, status)}"
+        if detail:
+            msg += f" ({detail})"
+        super().__init__(msg)
+
+
+_lib = None
+
+c_int, c_double, c_void_p, c_int64, c_size_t = (ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
+                                                ctypes.c_int64, ctypes.c_size_t)
+_P = c_void_p
+
+
+def _sig(lib):
+    S = {
+        "ns3d_create": ([c_int, c_int, c_int, c_double, c_double, c_double,
+                         ctypes.POINTER(c_void_p)], c_int),
+        "ns3d_destroy": ([_P], c_int),
+        "ns3d_supported_extent": ([c_int], c_int),
+        "ns3d_set_stream": ([_P, _P], c_int),
+        "ns3d_synchronize": ([_P], c_int),
+        "ns3d_last_error": ([_P], ctypes.c_char_p),
+        "ns3d_status_string": ([c_int], ctypes.c_char_p),
+        "ns3d_device_bytes": ([_P], c_size_t),
+        "ns3d_set_forcing": ([_P, _P, _P, _P], c_int),
+        "ns3d_forcing_modes": ([_P], c_int),
+        "ns3d_rk3_step": ([_P, _P, _P, _P, c_double, c_double], c_int),
+        "ns3d_rk3_steps": ([_P, _P, _P, _P, c_double, c_double, c_int], c_int),
+        "ns3d_euler_step": ([_P, _P, _P, _P, c_double, c_double], c_int),
+        "ns3d_rhs": ([_P] + [_P] * 6 + [c_double], c_int),
+        "ns3d_convolution": ([_P] + [_P] * 6, c_int),
+        "ns3d_convolution_uv": ([_P] + [_P] * 9, c_int),
+        "ns3d_jvp_step": ([_P] + [_P] * 6 + [c_double, c_double], c_int),
+        "ns3d_jvp_steps": ([_P] + [_P] * 6 + [c_double, c_double, c_int], c_int),
+        "ns3d_linearised_rhs": ([_P] + [_P] * 6 + [c_double], c_int),
+        "ns3d_implicit_tangent_step": ([_P] + [_P] * 6 + [c_double, c_double], c_int),
+        "ns3d_krylov_length": ([_P], c_int64),
+        "ns3d_pack_reduced": ([_P] + [_P] * 3 + [_P], c_int),
+        "ns3d_unpack_reduced": ([_P, _P] + [_P] * 3, c_int),
+        "ns3d_matvec_reduced": ([_P] + [_P] * 3 + [_P, _P, c_double, c_double], c_int),
+        "ns3d_diagnostics": ([_P] + [_P] * 3 + [_P, _P, _P], c_int),
+        "ns3d_profile_passes": ([_P] + [_P] * 3 + [c_double, c_double, c_int, _P], c_int),
+        "ns3d_mask_cutoff": ([c_int, c_int, c_int, c_double, c_double, c_double, _P], c_int),
+        "ns3d_twiddles": ([c_int, _P], c_int),
+    }
+    for name, (args, res) in S.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+
+
+def lib():
+    """The loaded CUDA library (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise Ns3dLibraryError(
+                f"{LIB_PATH} is missing: build it with `python -m ns3dperiodic_b200.build`")
+        try:
+            l = ctypes.CDLL(LIB_PATH)
+        except OSError as e:  # pragma: no cover
+            raise Ns3dLibraryError(f"cannot load {LIB_PATH}: {e}") from e
+        _sig(l)
+        _lib = l
+    return _lib

@@ -1,0 +1,25 @@
+// Concrete launch entry points of the pass kernels.  Each group lives in its
+// own translation unit (k_xy.cu, k_z.cu, k_fwdx.cu) so the per-extent
+// template instantiations compile in parallel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "passes.cuh"
+
+namespace ns3d {
+
+bool extent_supported(int n);
+
+cudaError_t run_inv_x(const InvXArgs<3>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_x(const InvXArgs<6>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_y(const InvYArgs<3>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_y(const InvYArgs<6>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_z(const ZArgs<3>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_z(const ZArgs<6>& a, const PassGeom& g, cudaStream_t st);
+// mode: UpdateMode; combine: out = ca*un + cb*base
+cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs& a, const PassGeom& g,
+                      cudaStream_t st);
+
+}  // namespace ns3d

@@ -1,0 +1,307 @@
+// FP64 line-FFT engine for sm_100a.
+//
+// One line of N complex points is owned by T = N/P threads of ONE warp (or of
+// the whole CTA when T > 32); thread t keeps the P points at positions
+// t + T*s (s = 0..P-1) in registers.  The transform is Stockham autosort
+// (Govindaraju et al., "High performance discrete Fourier transforms on
+// graphics processors", SC 2008): a sequence of radix-R stages, each thread
+// doing P/R register butterflies per stage, with the data re-distributed
+// between stages through a padded shared-memory line buffer.  Input and
+// output both use the "position t + T*s" distribution, so the first stage
+// reads straight from global memory and the last stage writes straight to it.
+//
+// Small DFTs (R = 2, 3, 4 and the composites 6, 8, 12, 16 built by a
+// two-factor Cooley-Tukey split) run fully in registers with compile-time
+// twiddles.  Stage twiddles come from a per-CTA shared-memory table
+// tw[e] = (cos 2*pi*e/N, sin 2*pi*e/N), e in [0, N).
+//
+// DIR = +1 is the inverse (e^{+i}) transform, DIR = -1 the forward one; both
+// unnormalised.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <utility>
+
+namespace ns3d {
+
+// ---------------------------------------------------------------------------
+// complex helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * (DIR * i)
+template <int DIR>
+__device__ __forceinline__ double2 cmul_i(double2 a) {
+  return DIR > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+// ---------------------------------------------------------------------------
+// compile-time twiddles: cos/sin of 2*pi*a/48 for the angles small DFTs use
+// (multiples of 22.5 and 30 degrees)
+// ---------------------------------------------------------------------------
+constexpr double kC225 = 0.92387953251128675613;  // cos(pi/8)
+constexpr double kS225 = 0.38268343236508977173;  // sin(pi/8)
+constexpr double kR3H = 0.86602540378443864676;   // sqrt(3)/2
+constexpr double kR12 = 0.70710678118654752440;   // sqrt(1/2)
+
+__host__ __device__ constexpr double cos_quarter(int a) {  // a in [0, 12], unit 7.5 deg
+  return a == 0 ? 1.0 : a == 3 ? kC225 : a == 4 ? kR3H : a == 6 ? kR12 : a == 8 ? 0.5
+       : a == 9 ? kS225 : a == 12 ? 0.0 : -2.0;  // -2: angle not representable
+}
+__host__ __device__ constexpr double cos48(int a) {
+  return (a = ((a % 48) + 48) % 48, a <= 12 ? cos_quarter(a)
+          : a <= 24 ? -cos_quarter(24 - a) : a <= 36 ? -cos_quarter(a - 24) : cos_quarter(48 - a));
+}
+__host__ __device__ constexpr double sin48(int a) { return cos48(a - 12); }
+
+// v * exp(DIR * 2*pi*i * E / R)
+template <int R, int E, int DIR>
+__device__ __forceinline__ double2 rot(double2 v) {
+  constexpr int a = ((E % R) * (48 / R)) % 48;
+  static_assert(48 % R == 0, "radix must divide 48");
+  static_assert(cos48(a) > -1.5 || a % 12 == 0, "angle not in table");
+  if constexpr (a == 0) {
+    return v;
+  } else if constexpr (a == 24) {
+    return make_double2(-v.x, -v.y);
+  } else if constexpr (a == 12) {
+    return cmul_i<DIR>(v);
+  } else if constexpr (a == 36) {
+    return cmul_i<-DIR>(v);
+  } else {
+    constexpr double c = cos48(a);
+    constexpr double s = DIR * sin48(a);
+    return make_double2(v.x * c - v.y * s, v.x * s + v.y * c);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// small DFTs in registers: V[k] = sum_r v[r] exp(DIR*2*pi*i*r*k/R)
+// ---------------------------------------------------------------------------
+template <int R, int DIR>
+struct DFT;
+
+template <int DIR>
+struct DFT<1, DIR> {
+  __device__ __forceinline__ static void run(double2*) {}
+};
+
+template <int DIR>
+struct DFT<2, DIR> {
+  __device__ __forceinline__ static void run(double2* v) {
+    double2 a = cadd(v[0], v[1]);
+    v[1] = csub(v[0], v[1]);
+    v[0] = a;
+  }
+};
+
+template <int DIR>
+struct DFT<3, DIR> {
+  __device__ __forceinline__ static void run(double2* v) {
+    double2 t = cadd(v[1], v[2]);
+    double2 d = cmul_i<DIR>(cscale(csub(v[1], v[2]), kR3H));
+    double2 m = make_double2(v[0].x - 0.5 * t.x, v[0].y - 0.5 * t.y);
+    v[0] = cadd(v[0], t);
+    v[1] = cadd(m, d);
+    v[2] = csub(m, d);
+  }
+};
+
+template <int DIR>
+struct DFT<4, DIR> {
+  __device__ __forceinline__ static void run(double2* v) {
+    double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    double2 b0 = cadd(v[1], v[3]), b1 = cmul_i<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(a0, b0);
+    v[2] = csub(a0, b0);
+    v[1] = cadd(a1, b1);
+    v[3] = csub(a1, b1);
+  }
+};
+
+// Two-factor Cooley-Tukey: R = A*B, n = B*n1 + n2, k = k1 + A*k2.
+template <int A, int B, int DIR>
+struct DFT_CT {
+  static constexpr int R = A * B;
+  __device__ __forceinline__ static void run(double2* v) {
+    double2 y[R];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) {
+      double2 t[A];
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) t[n1] = v[B * n1 + n2];
+      DFT<A, DIR>::run(t);
+#pragma unroll
+      for (int k1 = 0; k1 < A; ++k1) y[n2 * A + k1] = t[k1];
+    }
+    twiddle_all(y, std::make_integer_sequence<int, A * B>{});
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) {
+      double2 t[B];
+#pragma unroll
+      for (int n2 = 0; n2 < B; ++n2) t[n2] = y[n2 * A + k1];
+      DFT<B, DIR>::run(t);
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = t[k2];
+    }
+  }
+  template <int... I>
+  __device__ __forceinline__ static void twiddle_all(double2* y, std::integer_sequence<int, I...>) {
+    ((y[I] = rot<R, (I / A) * (I % A), DIR>(y[I])), ...);
+  }
+};
+
+template <int DIR>
+struct DFT<6, DIR> : DFT_CT<2, 3, DIR> {};
+template <int DIR>
+struct DFT<8, DIR> : DFT_CT<2, 4, DIR> {};
+template <int DIR>
+struct DFT<12, DIR> : DFT_CT<4, 3, DIR> {};
+template <int DIR>
+struct DFT<16, DIR> : DFT_CT<4, 4, DIR> {};
+
+// ---------------------------------------------------------------------------
+// synchronisation of the threads that own a line
+// ---------------------------------------------------------------------------
+template <int T>
+__device__ __forceinline__ void line_sync() {
+  if constexpr (T <= 32) {
+    __syncwarp();
+  } else {
+    __syncthreads();
+  }
+}
+
+// shared-memory line buffer index with one pad slot every PADW entries
+template <int PADW>
+__device__ __forceinline__ int spad(int p) {
+  return p + p / PADW;
+}
+template <int N, int PADW>
+constexpr int line_buf_len() {
+  return N + N / PADW + 1;
+}
+
+// ---------------------------------------------------------------------------
+// Stockham stages
+// ---------------------------------------------------------------------------
+template <int N, int T, int DIR, int PADW, int NS, int R, int... Rest>
+struct Stages {
+  static constexpr int P = N / T;
+  static constexpr int U = P / R;
+  static_assert(P % R == 0, "radix must divide the points per thread");
+
+  __device__ __forceinline__ static void run(double2 (&x)[P], int t, double2* sbuf,
+                                             const double2* __restrict__ tw) {
+    constexpr bool last = sizeof...(Rest) == 0;
+    static_assert(!last || NS * R == N, "radices must multiply to N");
+    if constexpr (!last) line_sync<T>();  // previous readers of sbuf are done
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int b = t + T * u;
+      double2 v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = x[u + r * U];
+      if constexpr (NS > 1) {
+        const int jm = b % NS;
+        constexpr int step = N / (NS * R);
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const double2 w = tw[jm * r * step];
+          v[r] = cmul(v[r], make_double2(w.x, DIR * w.y));
+        }
+      }
+      DFT<R, DIR>::run(v);
+      if constexpr (last) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) x[u + k * U] = v[k];
+      } else {
+        const int base = (b / NS) * NS * R + (b % NS);
+#pragma unroll
+        for (int k = 0; k < R; ++k) sbuf[spad<PADW>(base + k * NS)] = v[k];
+      }
+    }
+    if constexpr (!last) {
+      line_sync<T>();
+#pragma unroll
+      for (int s = 0; s < P; ++s) x[s] = sbuf[spad<PADW>(t + T * s)];
+      Stages<N, T, DIR, PADW, NS * R, Rest...>::run(x, t, sbuf, tw);
+    }
+  }
+};
+
+// Radix plans: Plan<N, P>::Rs... multiply to N and each divides P.
+template <int... Rs>
+struct RadixList {};
+
+template <int N, int P>
+struct Plan;
+template <> struct Plan<8, 8> { using L = RadixList<8>; };
+template <> struct Plan<8, 4> { using L = RadixList<4, 2>; };
+template <> struct Plan<24, 6> { using L = RadixList<6, 2, 2>; };
+template <> struct Plan<32, 4> { using L = RadixList<4, 4, 2>; };
+template <> struct Plan<48, 6> { using L = RadixList<6, 2, 2, 2>; };
+template <> struct Plan<64, 4> { using L = RadixList<4, 4, 4>; };
+template <> struct Plan<96, 6> { using L = RadixList<6, 2, 2, 2, 2>; };
+template <> struct Plan<128, 4> { using L = RadixList<4, 4, 4, 2>; };
+template <> struct Plan<192, 6> { using L = RadixList<6, 2, 2, 2, 2, 2>; };
+template <> struct Plan<256, 4> { using L = RadixList<4, 4, 4, 4>; };
+template <> struct Plan<384, 6> { using L = RadixList<6, 2, 2, 2, 2, 2, 2>; };
+template <> struct Plan<512, 4> { using L = RadixList<4, 4, 4, 4, 2>; };
+template <> struct Plan<16, 4> { using L = RadixList<4, 4>; };
+template <> struct Plan<16, 8> { using L = RadixList<8, 2>; };
+template <> struct Plan<16, 16> { using L = RadixList<16>; };
+template <> struct Plan<24, 12> { using L = RadixList<12, 2>; };
+template <> struct Plan<32, 8> { using L = RadixList<8, 4>; };
+template <> struct Plan<32, 16> { using L = RadixList<16, 2>; };
+template <> struct Plan<48, 12> { using L = RadixList<12, 4>; };
+template <> struct Plan<64, 8> { using L = RadixList<8, 8>; };
+template <> struct Plan<64, 16> { using L = RadixList<16, 4>; };
+template <> struct Plan<96, 12> { using L = RadixList<6, 4, 4>; };
+template <> struct Plan<128, 8> { using L = RadixList<8, 4, 4>; };
+template <> struct Plan<128, 16> { using L = RadixList<16, 8>; };
+template <> struct Plan<192, 12> { using L = RadixList<12, 4, 4>; };
+template <> struct Plan<256, 8> { using L = RadixList<8, 8, 4>; };
+template <> struct Plan<256, 16> { using L = RadixList<16, 16>; };
+template <> struct Plan<384, 12> { using L = RadixList<6, 4, 4, 4>; };
+template <> struct Plan<512, 8> { using L = RadixList<8, 8, 8>; };
+template <> struct Plan<512, 16> { using L = RadixList<16, 16, 2>; };
+
+template <int N, int T, int DIR, int PADW, typename L>
+struct RunPlan;
+template <int N, int T, int DIR, int PADW, int... Rs>
+struct RunPlan<N, T, DIR, PADW, RadixList<Rs...>> {
+  __device__ __forceinline__ static void run(double2 (&x)[N / T], int t, double2* sbuf,
+                                             const double2* __restrict__ tw) {
+    Stages<N, T, DIR, PADW, 1, Rs...>::run(x, t, sbuf, tw);
+  }
+};
+
+// First radix of a plan (the stride of the first exchange; used for padding).
+template <typename L>
+struct FirstRadix;
+template <int R0, int... Rs>
+struct FirstRadix<RadixList<R0, Rs...>> {
+  static constexpr int value = R0;
+};
+
+template <int N, int P>
+struct LineFFT {
+  static constexpr int T = N / P;
+  using L = typename Plan<N, P>::L;
+  static constexpr int PADW = FirstRadix<L>::value < 4 ? 4 : FirstRadix<L>::value;
+  static constexpr int BUF = line_buf_len<N, PADW>();
+  template <int DIR>
+  __device__ __forceinline__ static void run(double2 (&x)[P], int t, double2* sbuf,
+                                             const double2* __restrict__ tw) {
+    RunPlan<N, T, DIR, PADW, L>::run(x, t, sbuf, tw);
+  }
+};
+
+}  // namespace ns3d

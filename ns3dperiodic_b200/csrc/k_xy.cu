@@ -1,0 +1,25 @@
+// x and y pass instantiations (inverse x/y with lazy derivatives, forward y).
+#include "dispatch.h"
+#include "launch.cuh"
+
+namespace ns3d {
+
+bool extent_supported(int n) { return extent_supported_inline(n); }
+
+cudaError_t run_inv_x(const InvXArgs<3>& a, const PassGeom& g, cudaStream_t st) {
+  return launch_inv_x<3>(a, g, st);
+}
+cudaError_t run_inv_x(const InvXArgs<6>& a, const PassGeom& g, cudaStream_t st) {
+  return launch_inv_x<6>(a, g, st);
+}
+cudaError_t run_inv_y(const InvYArgs<3>& a, const PassGeom& g, cudaStream_t st) {
+  return launch_inv_y<3>(a, g, st);
+}
+cudaError_t run_inv_y(const InvYArgs<6>& a, const PassGeom& g, cudaStream_t st) {
+  return launch_inv_y<6>(a, g, st);
+}
+cudaError_t run_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream_t st) {
+  return launch_fwd_y(a, g, st);
+}
+
+}  // namespace ns3d

@@ -1,0 +1,132 @@
+// Per-extent dispatch of the pass kernels (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "passes.cuh"
+
+namespace ns3d {
+
+// Extents with compiled plans.
+#define NS3D_FOR_EACH_EXTENT(X) \
+  X(8) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
+
+// Points per thread: x/y passes that hold one or two lines per thread, and
+// the z / fwd_x passes that hold several fields per thread at once.
+constexpr int p_xy(int n) { return n % 3 == 0 ? 12 : 8; }
+constexpr int p_z(int n) { return n % 3 == 0 ? 12 : 8; }
+// the tangent z pass keeps u, v and the three products live: fewer points
+constexpr int p_zuv(int n) { return n % 3 == 0 ? 6 : 4; }
+
+inline bool extent_supported_inline(int n) {
+  switch (n) {
+#define NS3D_CASE(N) case N:
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    return true;
+    default:
+      return false;
+  }
+}
+
+template <int N, int P>
+constexpr int lines_per_cta_xy() {
+  return LaneMap<N / P>::LPC;
+}
+template <int N, int P>
+constexpr int lines_per_cta_z() {
+  return ZLaneMap<N / P>::LPC;
+}
+
+inline unsigned blocks_for(long long lines, int lpc) { return (unsigned)((lines + lpc - 1) / lpc); }
+
+template <int NF>
+cudaError_t launch_inv_x(const InvXArgs<NF>& a, const PassGeom& g, cudaStream_t st) {
+  const long long lines = (long long)g.Ny * g.Mz;
+  switch (g.Nx) {
+#define NS3D_CASE(N)                                                               \
+  case N: {                                                                        \
+    constexpr int P = p_xy(N);                                                     \
+    inv_x_kernel<N, P, NF><<<blocks_for(lines, lines_per_cta_xy<N, P>()),         \
+                             kWarpsPerCta * 32, 0, st>>>(a, g);                    \
+    return cudaGetLastError();                                                     \
+  }
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <int NF>
+cudaError_t launch_inv_y(const InvYArgs<NF>& a, const PassGeom& g, cudaStream_t st) {
+  const long long lines = (long long)g.Nx * g.Mz;
+  switch (g.Ny) {
+#define NS3D_CASE(N)                                                               \
+  case N: {                                                                        \
+    constexpr int P = p_xy(N);                                                     \
+    inv_y_kernel<N, P, NF><<<blocks_for(lines, lines_per_cta_xy<N, P>()),         \
+                             kWarpsPerCta * 32, 0, st>>>(a, g);                    \
+    return cudaGetLastError();                                                     \
+  }
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <bool UV>
+cudaError_t launch_z(const ZArgs<UV ? 6 : 3>& a, const PassGeom& g, cudaStream_t st) {
+  const long long lines = (long long)g.Nx * g.Ny;
+  switch (g.Nz) {
+#define NS3D_CASE(N)                                                               \
+  case N: {                                                                        \
+    constexpr int P = UV ? p_zuv(N) : p_z(N);                                      \
+    z_kernel<N, P, UV><<<blocks_for(lines, lines_per_cta_z<N, P>()),              \
+                         kWarpsPerCta * 32, 0, st>>>(a, g);                        \
+    return cudaGetLastError();                                                     \
+  }
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <int MODE, bool COMBINE>
+cudaError_t launch_fwd_x(const FwdXArgs& a, const PassGeom& g, cudaStream_t st) {
+  const long long lines = (long long)g.Ny * g.Mz;
+  switch (g.Nx) {
+#define NS3D_CASE(N)                                                               \
+  case N: {                                                                        \
+    constexpr int P = p_z(N);                                                      \
+    fwd_x_kernel<N, P, MODE, COMBINE><<<blocks_for(lines, lines_per_cta_xy<N, P>()), \
+                                        kWarpsPerCta * 32, 0, st>>>(a, g);         \
+    return cudaGetLastError();                                                     \
+  }
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+inline cudaError_t launch_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream_t st) {
+  const long long lines = (long long)g.Nx * g.Mz;
+  switch (g.Ny) {
+#define NS3D_CASE(N)                                                               \
+  case N: {                                                                        \
+    constexpr int P = p_xy(N);                                                     \
+    fwd_y_kernel<N, P><<<blocks_for(lines, lines_per_cta_xy<N, P>()),             \
+                         kWarpsPerCta * 32, 0, st>>>(a, g);                        \
+    return cudaGetLastError();                                                     \
+  }
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace ns3d

@@ -1,0 +1,753 @@
+// Host side of the C ABI (include/ns3d.h): handle, scratch, RHS pipelines and
+// the steppers of Source/RK_time_step.cu rebuilt on the fused pass kernels.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ns3d.h"
+#include "aux_kernels.cuh"
+#include "dispatch.h"
+
+using ns3d::FwdXArgs;
+using ns3d::FwdYArgs;
+using ns3d::InvXArgs;
+using ns3d::InvYArgs;
+using ns3d::PassGeom;
+using ns3d::ZArgs;
+
+namespace {
+
+constexpr int kForcingCap = 4096;
+constexpr int kDiagBlocks = 592;  // 4 x 148 SMs
+constexpr int kDiagThreads = 256;
+
+}  // namespace
+
+struct ns3d_solver {
+  int Nx = 0, Ny = 0, Nz = 0, Mz = 0;
+  double Lx = 0, Ly = 0, Lz = 0;
+  size_t nc = 0;  // complex points per field
+  int device = 0;
+  PassGeom geom{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // tables
+  uint16_t* qcut = nullptr;
+  double2* tw[3] = {};
+  // scratch: base pool (21 fields) and tangent pool (18 fields, lazily)
+  double2* pool_base = nullptr;
+  double2* pool_uv = nullptr;
+  double2* A[6] = {};
+  double2* B[6] = {};
+  double2* C[6] = {};
+  double2* D[6] = {};
+  double2* E[6] = {};
+  double2* u1[3] = {};
+  double2* u2[3] = {};
+  double2* v1[3] = {};
+  // forcing
+  int* f_count = nullptr;
+  int* f_idx = nullptr;
+  double2* f_val = nullptr;
+  int f_nnz = 0;
+  const double2* f_dense[3] = {};
+  // diagnostics
+  double* diag_partial = nullptr;
+  double* diag_out = nullptr;
+  // cached RK3 step graph
+  cudaGraphExec_t rk3_exec = nullptr;
+  const void* rk3_key[3] = {};
+  double rk3_dt = 0.0, rk3_Re = 0.0;
+  cudaStream_t rk3_stream = nullptr;
+  int f_version = 0, rk3_fversion = -1;
+  bool graphs_off = false;
+  size_t bytes = 0;
+  std::string err;
+};
+
+namespace {
+
+ns3d_status fail(ns3d_solver* h, ns3d_status s, const std::string& msg) {
+  if (h) h->err = msg;
+  return s;
+}
+
+ns3d_status cuda_fail(ns3d_solver* h, cudaError_t e, const char* where) {
+  return fail(h, e == cudaErrorMemoryAllocation ? NS3D_ERR_OOM : NS3D_ERR_CUDA,
+              std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define NS3D_CHECK(h, call, where)                 \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, where); \
+  } while (0)
+
+void build_twiddles(int N, std::vector<double2>& out) {
+  out.resize(N);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int e = 0; e < N; ++e) {
+    // exact symmetric values where they exist, long double elsewhere
+    long double a = two_pi * (long double)e / (long double)N;
+    double c = (double)cosl(a), s = (double)sinl(a);
+    if ((4 * e) % N == 0) {
+      const int q = (4 * e) / N;  // multiples of 90 degrees
+      c = q == 0 ? 1.0 : q == 2 ? -1.0 : 0.0;
+      s = q == 1 ? 1.0 : q == 3 ? -1.0 : 0.0;
+    }
+    out[e] = make_double2(c, s);
+  }
+}
+
+// build_mask_matrix (Source/math_support.cu:471-519) evaluated as main()
+// calls it: Nz slot = Mz, so kzMax = 2*Mz*PI/Lz.  Returns false if the kept
+// modes of some (j,k) column are not a prefix in l.
+bool build_mask_cutoff(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                       uint16_t* qcut) {
+  const double PI = 3.141592653589793238462643383279502884197169399375105820974944592307816406;
+  const int Mz = Nz / 2 + 1;
+  volatile double kxMax = 2 * Nx * PI / Lx;
+  volatile double kyMax = 2 * Ny * PI / Ly;
+  volatile double kzMax = 2 * Mz * PI / Lz;
+  for (int j = 0; j < Nx; ++j) {
+    const int m = j >= Nx / 2 ? j - Nx : j;
+    for (int k = 0; k < Ny; ++k) {
+      const int n = k >= Ny / 2 ? k - Ny : k;
+      int cut = 0;
+      bool ended = false;
+      for (int l = 0; l < Mz; ++l) {
+        const int q = l;
+        volatile double kx = m * 2 * PI / Lx;
+        volatile double ky = n * 2 * PI / Ly;
+        volatile double kz = q * 2 * PI / Lz;
+        volatile double tx = kx * kx / (kxMax * kxMax);
+        volatile double ty = ky * ky / (kyMax * kyMax);
+        volatile double tz = kz * kz / (kzMax * kzMax);
+        volatile double s2 = tx + ty;
+        s2 = s2 + tz;
+        const double sphere2 = std::sqrt((double)s2);
+        const bool keep = sphere2 < 2.0 / 3.0;
+        if (keep) {
+          if (ended) return false;
+          ++cut;
+        } else {
+          ended = true;
+        }
+      }
+      qcut[j * Ny + k] = (uint16_t)cut;
+    }
+  }
+  return true;
+}
+
+bool valid_extents(int Nx, int Ny, int Nz) {
+  return ns3d::extent_supported(Nx) && ns3d::extent_supported(Ny) && ns3d::extent_supported(Nz);
+}
+
+ns3d_status ensure_uv_pool(ns3d_solver* h) {
+  if (h->pool_uv) return NS3D_OK;
+  const size_t bytes = sizeof(double2) * h->nc * 18;
+  NS3D_CHECK(h, cudaMalloc(&h->pool_uv, bytes), "cudaMalloc(tangent scratch)");
+  h->bytes += bytes;
+  double2* p = h->pool_uv;
+  for (int i = 3; i < 6; ++i) {
+    h->A[i] = p; p += h->nc;
+    h->B[i] = p; p += h->nc;
+    h->C[i] = p; p += h->nc;
+    h->D[i] = p; p += h->nc;
+    h->E[i] = p; p += h->nc;
+  }
+  for (int i = 0; i < 3; ++i) { h->v1[i] = p; p += h->nc; }
+  return NS3D_OK;
+}
+
+// inv_x -> inv_y -> z -> fwd_y: leaves the y,z-transformed products in A[0..2].
+ns3d_status conv_front(ns3d_solver* h, const double2* const u[3], const double2* const v[3]) {
+  const PassGeom& g = h->geom;
+  cudaStream_t st = h->stream;
+  if (!v) {
+    InvXArgs<3> ax{};
+    InvYArgs<3> ay{};
+    ZArgs<3> az{};
+    for (int i = 0; i < 3; ++i) {
+      ax.in[i] = u[i]; ax.A[i] = h->A[i]; ax.B[i] = h->B[i];
+      ay.A[i] = h->A[i]; ay.B[i] = h->B[i];
+      ay.C[i] = h->C[i]; ay.D[i] = h->D[i]; ay.E[i] = h->E[i];
+      az.C[i] = h->C[i]; az.D[i] = h->D[i]; az.E[i] = h->E[i];
+      az.Qh[i] = h->A[i];
+    }
+    ax.qcut = h->qcut; ax.tw = h->tw[0];
+    ay.tw = h->tw[1];
+    az.tw = h->tw[2];
+    NS3D_CHECK(h, ns3d::run_inv_x(ax, g, st), "inv_x");
+    NS3D_CHECK(h, ns3d::run_inv_y(ay, g, st), "inv_y");
+    NS3D_CHECK(h, ns3d::run_z(az, g, st), "z");
+  } else {
+    ns3d_status s = ensure_uv_pool(h);
+    if (s != NS3D_OK) return s;
+    InvXArgs<6> ax{};
+    InvYArgs<6> ay{};
+    ZArgs<6> az{};
+    for (int i = 0; i < 6; ++i) {
+      ax.in[i] = i < 3 ? u[i] : v[i - 3];
+      ax.A[i] = h->A[i]; ax.B[i] = h->B[i];
+      ay.A[i] = h->A[i]; ay.B[i] = h->B[i];
+      ay.C[i] = h->C[i]; ay.D[i] = h->D[i]; ay.E[i] = h->E[i];
+      az.C[i] = h->C[i]; az.D[i] = h->D[i]; az.E[i] = h->E[i];
+    }
+    for (int i = 0; i < 3; ++i) az.Qh[i] = h->A[i];
+    ax.qcut = h->qcut; ax.tw = h->tw[0];
+    ay.tw = h->tw[1];
+    az.tw = h->tw[2];
+    NS3D_CHECK(h, ns3d::run_inv_x(ax, g, st), "inv_x(uv)");
+    NS3D_CHECK(h, ns3d::run_inv_y(ay, g, st), "inv_y(uv)");
+    NS3D_CHECK(h, ns3d::run_z(az, g, st), "z(uv)");
+  }
+  FwdYArgs fy{};
+  for (int i = 0; i < 3; ++i) fy.Q[i] = h->A[i];
+  fy.tw = h->tw[1];
+  NS3D_CHECK(h, ns3d::run_fwd_y(fy, g, st), "fwd_y");
+  return NS3D_OK;
+}
+
+// fwd_x + pointwise update on the products left by conv_front.
+ns3d_status finish(ns3d_solver* h, int mode, bool forcing, const double2* const us[3],
+                   double2* const out[3], const double2* const un[3], double ca, double cb,
+                   double dt, double Re) {
+  FwdXArgs a{};
+  for (int i = 0; i < 3; ++i) {
+    a.Qh[i] = h->A[i];
+    a.us[i] = us ? us[i] : nullptr;
+    a.un[i] = un ? un[i] : nullptr;
+    a.out[i] = out[i];
+    a.fd[i] = (forcing && h->f_dense[0]) ? h->f_dense[i] : nullptr;
+  }
+  a.fidx = h->f_idx;
+  a.fval = h->f_val;
+  a.fnnz = (forcing && !h->f_dense[0]) ? h->f_nnz : 0;
+  a.dt = dt;
+  a.Re = Re;
+  a.ca = ca;
+  a.cb = cb;
+  a.tw = h->tw[0];
+  NS3D_CHECK(h, ns3d::run_fwd_x(mode, un != nullptr, a, h->geom, h->stream), "fwd_x");
+  return NS3D_OK;
+}
+
+#define NS3D_TRY(expr)                 \
+  do {                                 \
+    ns3d_status s_ = (expr);           \
+    if (s_ != NS3D_OK) return s_;      \
+  } while (0)
+
+// RK3_SSP (Source/RK_time_step.cu:310-327) with every stage fused:
+//   u1 = u + dt L(u); u2 = 3/4 u + 1/4 (u1 + dt L(u1)); u = 1/3 u + 2/3 (u2 + dt L(u2))
+ns3d_status rk3_launches(ns3d_solver* h, double2* const u[3], double dt, double Re) {
+  const double2* uc[3] = {u[0], u[1], u[2]};
+  const double2* u1c[3] = {h->u1[0], h->u1[1], h->u1[2]};
+  const double2* u2c[3] = {h->u2[0], h->u2[1], h->u2[2]};
+  NS3D_TRY(conv_front(h, uc, nullptr));
+  NS3D_TRY(finish(h, ns3d::kExplicit, true, uc, h->u1, nullptr, 0.0, 1.0, dt, Re));
+  NS3D_TRY(conv_front(h, u1c, nullptr));
+  NS3D_TRY(finish(h, ns3d::kExplicit, true, u1c, h->u2, uc, 3.0 / 4.0, 1.0 / 4.0, dt, Re));
+  NS3D_TRY(conv_front(h, u2c, nullptr));
+  NS3D_TRY(finish(h, ns3d::kExplicit, true, u2c, u, uc, 1.0 / 3.0, 2.0 / 3.0, dt, Re));
+  return NS3D_OK;
+}
+
+bool args_ok3(const void* a, const void* b, const void* c) { return a && b && c; }
+
+ns3d_status check_handle(ns3d_solver* h) {
+  if (!h) return NS3D_ERR_BAD_ARG;
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+  h->err.clear();
+  return NS3D_OK;
+}
+
+ns3d_status check_step(ns3d_solver* h, double dt, double Re) {
+  if (!(Re > 0.0) || !std::isfinite(Re) || !std::isfinite(dt))
+    return fail(h, NS3D_ERR_BAD_ARG, "dt must be finite and Re > 0");
+  return NS3D_OK;
+}
+
+void drop_graph(ns3d_solver* h) {
+  if (h->rk3_exec) cudaGraphExecDestroy(h->rk3_exec);
+  h->rk3_exec = nullptr;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int ns3d_supported_extent(int n) { return ns3d::extent_supported(n) ? 1 : 0; }
+
+const char* ns3d_status_string(ns3d_status s) {
+  switch (s) {
+    case NS3D_OK: return "ok";
+    case NS3D_ERR_BAD_ARG: return "bad argument";
+    case NS3D_ERR_UNSUPPORTED: return "unsupported grid extent";
+    case NS3D_ERR_OOM: return "out of device memory";
+    case NS3D_ERR_CUDA: return "CUDA error";
+    case NS3D_ERR_NONFINITE: return "non-finite value";
+    case NS3D_ERR_TIMEOUT: return "device wait timed out";
+  }
+  return "unknown status";
+}
+
+const char* ns3d_last_error(const ns3d_solver* h) { return h ? h->err.c_str() : ""; }
+
+size_t ns3d_device_bytes(const ns3d_solver* h) { return h ? h->bytes : 0; }
+
+ns3d_status ns3d_mask_cutoff(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                             uint16_t* qcut) {
+  if (Nx <= 0 || Ny <= 0 || Nz <= 0 || !qcut || !(Lx > 0) || !(Ly > 0) || !(Lz > 0))
+    return NS3D_ERR_BAD_ARG;
+  return build_mask_cutoff(Nx, Ny, Nz, Lx, Ly, Lz, qcut) ? NS3D_OK : NS3D_ERR_BAD_ARG;
+}
+
+ns3d_status ns3d_twiddles(int N, double* tw) {
+  if (N <= 0 || !tw) return NS3D_ERR_BAD_ARG;
+  std::vector<double2> t;
+  build_twiddles(N, t);
+  std::memcpy(tw, t.data(), sizeof(double2) * N);
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_create(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                        ns3d_solver** out) {
+  if (!out) return NS3D_ERR_BAD_ARG;
+  *out = nullptr;
+  if (Nx <= 0 || Ny <= 0 || Nz <= 0 || !(Lx > 0) || !(Ly > 0) || !(Lz > 0))
+    return NS3D_ERR_BAD_ARG;
+  if (!valid_extents(Nx, Ny, Nz)) return NS3D_ERR_UNSUPPORTED;
+  ns3d_solver* h = new ns3d_solver();
+  h->Nx = Nx; h->Ny = Ny; h->Nz = Nz; h->Mz = Nz / 2 + 1;
+  h->Lx = Lx; h->Ly = Ly; h->Lz = Lz;
+  h->nc = (size_t)Nx * Ny * h->Mz;
+  cudaGetDevice(&h->device);
+  h->geom.Nx = Nx; h->geom.Ny = Ny; h->geom.Nz = Nz; h->geom.Mz = h->Mz;
+  // 2.0*M_PI/L as in build_Nabla_Wavenumbers (Source/math_support.cu:398-413)
+  h->geom.kfx = 2.0 * M_PI / Lx;
+  h->geom.kfy = 2.0 * M_PI / Ly;
+  h->geom.kfz = 2.0 * M_PI / Lz;
+  h->geom.inv_vol = 1.0 / (1.0 * Nx * Ny * Nz);
+
+  auto bail = [&](ns3d_status s) {
+    ns3d_destroy(h);
+    return s;
+  };
+  std::vector<uint16_t> qc((size_t)Nx * Ny);
+  if (!build_mask_cutoff(Nx, Ny, Nz, Lx, Ly, Lz, qc.data())) return bail(NS3D_ERR_BAD_ARG);
+  cudaError_t e;
+  if ((e = cudaStreamCreate(&h->stream)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
+  h->own_stream = true;
+  if ((e = cudaMalloc(&h->qcut, sizeof(uint16_t) * qc.size())) != cudaSuccess)
+    return bail(NS3D_ERR_OOM);
+  cudaMemcpy(h->qcut, qc.data(), sizeof(uint16_t) * qc.size(), cudaMemcpyHostToDevice);
+  const int ext[3] = {Nx, Ny, Nz};
+  for (int d = 0; d < 3; ++d) {
+    std::vector<double2> t;
+    build_twiddles(ext[d], t);
+    if (cudaMalloc(&h->tw[d], sizeof(double2) * t.size()) != cudaSuccess) return bail(NS3D_ERR_OOM);
+    cudaMemcpy(h->tw[d], t.data(), sizeof(double2) * t.size(), cudaMemcpyHostToDevice);
+  }
+  const size_t base_bytes = sizeof(double2) * h->nc * 21;
+  if (cudaMalloc(&h->pool_base, base_bytes) != cudaSuccess) return bail(NS3D_ERR_OOM);
+  h->bytes = base_bytes + sizeof(uint16_t) * qc.size() + sizeof(double2) * (Nx + Ny + Nz);
+  double2* p = h->pool_base;
+  for (int i = 0; i < 3; ++i) {
+    h->A[i] = p; p += h->nc;
+    h->B[i] = p; p += h->nc;
+    h->C[i] = p; p += h->nc;
+    h->D[i] = p; p += h->nc;
+    h->E[i] = p; p += h->nc;
+    h->u1[i] = p; p += h->nc;
+    h->u2[i] = p; p += h->nc;
+  }
+  if (cudaMalloc(&h->f_count, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&h->f_idx, sizeof(int) * kForcingCap) != cudaSuccess ||
+      cudaMalloc(&h->f_val, sizeof(double2) * 3 * kForcingCap) != cudaSuccess ||
+      cudaMalloc(&h->diag_partial, sizeof(double) * 3 * kDiagBlocks) != cudaSuccess ||
+      cudaMalloc(&h->diag_out, sizeof(double) * 3) != cudaSuccess)
+    return bail(NS3D_ERR_OOM);
+  if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(NS3D_ERR_CUDA);
+  *out = h;
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_destroy(ns3d_solver* h) {
+  if (!h) return NS3D_ERR_BAD_ARG;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  drop_graph(h);
+  cudaFree(h->qcut);
+  for (auto* t : h->tw) cudaFree(t);
+  cudaFree(h->pool_base);
+  cudaFree(h->pool_uv);
+  cudaFree(h->f_count);
+  cudaFree(h->f_idx);
+  cudaFree(h->f_val);
+  cudaFree(h->diag_partial);
+  cudaFree(h->diag_out);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_set_stream(ns3d_solver* h, void* stream) {
+  NS3D_TRY(check_handle(h));
+  if (h->own_stream && h->stream) {
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+  }
+  h->own_stream = false;
+  h->stream = (cudaStream_t)stream;
+  drop_graph(h);
+  h->graphs_off = false;
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_synchronize(ns3d_solver* h) {
+  NS3D_TRY(check_handle(h));
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_set_forcing(ns3d_solver* h, const ns3d_complex* fx, const ns3d_complex* fy,
+                             const ns3d_complex* fz) {
+  NS3D_TRY(check_handle(h));
+  h->f_version++;
+  h->f_dense[0] = h->f_dense[1] = h->f_dense[2] = nullptr;
+  h->f_nnz = 0;
+  if (!fx && !fy && !fz) return NS3D_OK;
+  if (!args_ok3(fx, fy, fz)) return fail(h, NS3D_ERR_BAD_ARG, "forcing needs 3 components");
+  NS3D_CHECK(h, cudaMemsetAsync(h->f_count, 0, sizeof(int), h->stream), "memset");
+  ns3d::forcing_scan_kernel<<<592, 256, 0, h->stream>>>(
+      (const double2*)fx, (const double2*)fy, (const double2*)fz, (long long)h->nc, kForcingCap,
+      h->f_count, h->f_idx, h->f_val);
+  NS3D_CHECK(h, cudaGetLastError(), "forcing_scan");
+  int count = 0;
+  NS3D_CHECK(h, cudaMemcpyAsync(&count, h->f_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream),
+             "forcing count");
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "forcing sync");
+  if (count > kForcingCap) {
+    h->f_dense[0] = (const double2*)fx;
+    h->f_dense[1] = (const double2*)fy;
+    h->f_dense[2] = (const double2*)fz;
+  } else {
+    h->f_nnz = count;
+  }
+  return NS3D_OK;
+}
+
+int ns3d_forcing_modes(const ns3d_solver* h) {
+  if (!h) return 0;
+  return h->f_dense[0] ? -1 : h->f_nnz;
+}
+
+ns3d_status ns3d_rk3_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                          double dt, double Re) {
+  return ns3d_rk3_steps(h, ux, uy, uz, dt, Re, 1);
+}
+
+ns3d_status ns3d_rk3_steps(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                           double dt, double Re, int nsteps) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, dt, Re));
+  if (!args_ok3(ux, uy, uz) || nsteps < 0) return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  double2* u[3] = {(double2*)ux, (double2*)uy, (double2*)uz};
+  if (nsteps == 0) return NS3D_OK;
+  // The legacy default stream cannot be captured: launch directly there.
+  if (h->stream == nullptr) {
+    for (int s = 0; s < nsteps; ++s) NS3D_TRY(rk3_launches(h, u, dt, Re));
+    return NS3D_OK;
+  }
+  const bool hit = h->rk3_exec && h->rk3_key[0] == ux && h->rk3_key[1] == uy &&
+                   h->rk3_key[2] == uz && h->rk3_dt == dt && h->rk3_Re == Re &&
+                   h->rk3_stream == h->stream && h->rk3_fversion == h->f_version;
+  if (!hit && !h->graphs_off) {
+    drop_graph(h);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      ns3d_status s = rk3_launches(h, u, dt, Re);
+      e = cudaStreamEndCapture(h->stream, &graph);
+      if (s != NS3D_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return s;
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&h->rk3_exec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+    }
+    if (e != cudaSuccess) {
+      // capture not possible on this stream: launch directly from now on
+      cudaGetLastError();
+      h->rk3_exec = nullptr;
+      h->graphs_off = true;
+    } else {
+      h->rk3_key[0] = ux; h->rk3_key[1] = uy; h->rk3_key[2] = uz;
+      h->rk3_dt = dt; h->rk3_Re = Re; h->rk3_stream = h->stream;
+      h->rk3_fversion = h->f_version;
+    }
+  }
+  if (h->graphs_off) {
+    for (int s = 0; s < nsteps; ++s) NS3D_TRY(rk3_launches(h, u, dt, Re));
+    return NS3D_OK;
+  }
+  for (int s = 0; s < nsteps; ++s)
+    NS3D_CHECK(h, cudaGraphLaunch(h->rk3_exec, h->stream), "graph launch");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_euler_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                            double dt, double Re) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, dt, Re));
+  if (!args_ok3(ux, uy, uz)) return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  double2* u[3] = {(double2*)ux, (double2*)uy, (double2*)uz};
+  const double2* uc[3] = {u[0], u[1], u[2]};
+  NS3D_TRY(conv_front(h, uc, nullptr));
+  return finish(h, ns3d::kExplicit, true, uc, u, nullptr, 0.0, 1.0, dt, Re);
+}
+
+ns3d_status ns3d_rhs(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                     const ns3d_complex* uz, ns3d_complex* rx, ns3d_complex* ry, ns3d_complex* rz,
+                     double Re) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, 0.0, Re));
+  if (!args_ok3(ux, uy, uz) || !args_ok3(rx, ry, rz))
+    return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  const double2* uc[3] = {(const double2*)ux, (const double2*)uy, (const double2*)uz};
+  double2* r[3] = {(double2*)rx, (double2*)ry, (double2*)rz};
+  NS3D_TRY(conv_front(h, uc, nullptr));
+  return finish(h, ns3d::kRhs, true, uc, r, nullptr, 0.0, 1.0, 0.0, Re);
+}
+
+ns3d_status ns3d_convolution(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                             const ns3d_complex* uz, ns3d_complex* Qx, ns3d_complex* Qy,
+                             ns3d_complex* Qz) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(ux, uy, uz) || !args_ok3(Qx, Qy, Qz))
+    return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  const double2* uc[3] = {(const double2*)ux, (const double2*)uy, (const double2*)uz};
+  double2* q[3] = {(double2*)Qx, (double2*)Qy, (double2*)Qz};
+  NS3D_TRY(conv_front(h, uc, nullptr));
+  return finish(h, ns3d::kConvOut, false, nullptr, q, nullptr, 0.0, 1.0, 0.0, 1.0);
+}
+
+ns3d_status ns3d_convolution_uv(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                const ns3d_complex* uz, const ns3d_complex* vx,
+                                const ns3d_complex* vy, const ns3d_complex* vz, ns3d_complex* Qx,
+                                ns3d_complex* Qy, ns3d_complex* Qz) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(ux, uy, uz) || !args_ok3(vx, vy, vz) || !args_ok3(Qx, Qy, Qz))
+    return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  const double2* uc[3] = {(const double2*)ux, (const double2*)uy, (const double2*)uz};
+  const double2* vc[3] = {(const double2*)vx, (const double2*)vy, (const double2*)vz};
+  double2* q[3] = {(double2*)Qx, (double2*)Qy, (double2*)Qz};
+  NS3D_TRY(conv_front(h, uc, vc));
+  return finish(h, ns3d::kConvOut, false, nullptr, q, nullptr, 0.0, 1.0, 0.0, 1.0);
+}
+
+ns3d_status ns3d_jvp_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                          ns3d_complex* vx, ns3d_complex* vy, ns3d_complex* vz, double dt,
+                          double Re) {
+  return ns3d_jvp_steps(h, ux, uy, uz, vx, vy, vz, dt, Re, 1);
+}
+
+// RK3_SSP_UV (Source/RK_time_step.cu:342-355):
+//   v1 = v + dt J(u) v; u <- RK3(u); v = 1/2 v + 1/2 (v1 + dt J(u_new) v1)
+ns3d_status ns3d_jvp_steps(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                           ns3d_complex* vx, ns3d_complex* vy, ns3d_complex* vz, double dt,
+                           double Re, int nsteps) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, dt, Re));
+  if (!args_ok3(ux, uy, uz) || !args_ok3(vx, vy, vz) || nsteps < 0)
+    return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  NS3D_TRY(ensure_uv_pool(h));
+  double2* u[3] = {(double2*)ux, (double2*)uy, (double2*)uz};
+  double2* v[3] = {(double2*)vx, (double2*)vy, (double2*)vz};
+  const double2* uc[3] = {u[0], u[1], u[2]};
+  const double2* vc[3] = {v[0], v[1], v[2]};
+  const double2* v1c[3] = {h->v1[0], h->v1[1], h->v1[2]};
+  for (int s = 0; s < nsteps; ++s) {
+    NS3D_TRY(conv_front(h, uc, vc));
+    NS3D_TRY(finish(h, ns3d::kExplicit, false, vc, h->v1, nullptr, 0.0, 1.0, dt, Re));
+    NS3D_TRY(rk3_launches(h, u, dt, Re));
+    NS3D_TRY(conv_front(h, uc, v1c));
+    NS3D_TRY(finish(h, ns3d::kExplicit, false, v1c, v, vc, 0.5, 0.5, dt, Re));
+  }
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_linearised_rhs(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                const ns3d_complex* uz, ns3d_complex* vx, ns3d_complex* vy,
+                                ns3d_complex* vz, double Re) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, 0.0, Re));
+  if (!args_ok3(ux, uy, uz) || !args_ok3(vx, vy, vz))
+    return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  const double2* uc[3] = {(const double2*)ux, (const double2*)uy, (const double2*)uz};
+  double2* v[3] = {(double2*)vx, (double2*)vy, (double2*)vz};
+  const double2* vc[3] = {v[0], v[1], v[2]};
+  NS3D_TRY(conv_front(h, uc, vc));
+  return finish(h, ns3d::kRhs, false, vc, v, nullptr, 0.0, 1.0, 0.0, Re);
+}
+
+ns3d_status ns3d_implicit_tangent_step(ns3d_solver* h, const ns3d_complex* ux,
+                                       const ns3d_complex* uy, const ns3d_complex* uz,
+                                       ns3d_complex* vx, ns3d_complex* vy, ns3d_complex* vz,
+                                       double dt, double Re) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, dt, Re));
+  if (!args_ok3(ux, uy, uz) || !args_ok3(vx, vy, vz))
+    return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  const double2* uc[3] = {(const double2*)ux, (const double2*)uy, (const double2*)uz};
+  double2* v[3] = {(double2*)vx, (double2*)vy, (double2*)vz};
+  const double2* vc[3] = {v[0], v[1], v[2]};
+  NS3D_TRY(conv_front(h, uc, vc));
+  return finish(h, ns3d::kImplicit, false, vc, v, nullptr, 0.0, 1.0, dt, Re);
+}
+
+int64_t ns3d_krylov_length(const ns3d_solver* h) { return h ? 3 * ((int64_t)h->nc - 1) : 0; }
+
+ns3d_status ns3d_pack_reduced(ns3d_solver* h, const ns3d_complex* vx, const ns3d_complex* vy,
+                              const ns3d_complex* vz, double* vec) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(vx, vy, vz) || !vec) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  ns3d::pack_reduced_kernel<<<592, 256, 0, h->stream>>>(
+      (const double2*)vx, (const double2*)vy, (const double2*)vz, (long long)h->nc, vec, nullptr,
+      0.0);
+  NS3D_CHECK(h, cudaGetLastError(), "pack_reduced");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_unpack_reduced(ns3d_solver* h, const double* vec, ns3d_complex* vx,
+                                ns3d_complex* vy, ns3d_complex* vz) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(vx, vy, vz) || !vec) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  ns3d::unpack_reduced_kernel<<<592, 256, 0, h->stream>>>(vec, (long long)h->nc, (double2*)vx,
+                                                          (double2*)vy, (double2*)vz);
+  NS3D_CHECK(h, cudaGetLastError(), "unpack_reduced");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_matvec_reduced(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                const ns3d_complex* uz, const double* vec_in, double* vec_out,
+                                double Re, double tau) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, 0.0, Re));
+  if (!args_ok3(ux, uy, uz) || !vec_in || !vec_out)
+    return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  NS3D_TRY(ensure_uv_pool(h));
+  double2* v[3] = {h->v1[0], h->v1[1], h->v1[2]};
+  const double2* vc[3] = {v[0], v[1], v[2]};
+  const double2* uc[3] = {(const double2*)ux, (const double2*)uy, (const double2*)uz};
+  ns3d::unpack_reduced_kernel<<<592, 256, 0, h->stream>>>(vec_in, (long long)h->nc, v[0], v[1],
+                                                          v[2]);
+  NS3D_CHECK(h, cudaGetLastError(), "unpack_reduced");
+  NS3D_TRY(conv_front(h, uc, vc));
+  NS3D_TRY(finish(h, ns3d::kRhs, false, vc, v, nullptr, 0.0, 1.0, 0.0, Re));
+  ns3d::pack_reduced_kernel<<<592, 256, 0, h->stream>>>(v[0], v[1], v[2], (long long)h->nc,
+                                                        vec_out, tau > 0.0 ? vec_in : nullptr,
+                                                        tau > 0.0 ? 1.0 / tau : 0.0);
+  NS3D_CHECK(h, cudaGetLastError(), "pack_reduced");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_diagnostics(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                             const ns3d_complex* uz, double* energy, double* dissipation,
+                             double* div_max) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(ux, uy, uz)) return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  ns3d::DiagGeom g{};
+  g.Nx = h->Nx; g.Ny = h->Ny; g.Nz = h->Nz; g.Mz = h->Mz;
+  g.kfx = h->geom.kfx; g.kfy = h->geom.kfy; g.kfz = h->geom.kfz;
+  g.dx = h->Lx / (double)h->Nx;
+  g.dy = h->Ly / (double)h->Ny;
+  g.dz = h->Lz / (double)h->Nz;
+  g.inv_vol = h->geom.inv_vol;
+  ns3d::diag_partial_kernel<<<kDiagBlocks, kDiagThreads, 0, h->stream>>>(
+      (const double2*)ux, (const double2*)uy, (const double2*)uz, g, h->diag_partial);
+  NS3D_CHECK(h, cudaGetLastError(), "diag_partial");
+  ns3d::diag_final_kernel<<<1, 1024, 0, h->stream>>>(h->diag_partial, kDiagBlocks, h->diag_out);
+  NS3D_CHECK(h, cudaGetLastError(), "diag_final");
+  double r[3];
+  NS3D_CHECK(h, cudaMemcpyAsync(r, h->diag_out, sizeof(r), cudaMemcpyDeviceToHost, h->stream),
+             "diag copy");
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "diag sync");
+  if (energy) *energy = r[0];
+  if (dissipation) *dissipation = r[1];
+  if (div_max) *div_max = r[2];
+  if (!std::isfinite(r[0]) || !std::isfinite(r[1]) || !std::isfinite(r[2]))
+    return fail(h, NS3D_ERR_NONFINITE, "diagnostics are not finite");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                const ns3d_complex* uz, double dt, double Re, int reps,
+                                double* ms) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, dt, Re));
+  if (!args_ok3(ux, uy, uz) || !ms || reps <= 0) return fail(h, NS3D_ERR_BAD_ARG, "bad args");
+  const PassGeom& g = h->geom;
+  cudaStream_t st = h->stream;
+  const double2* u[3] = {(const double2*)ux, (const double2*)uy, (const double2*)uz};
+  InvXArgs<3> ax{};
+  InvYArgs<3> ay{};
+  ZArgs<3> az{};
+  FwdYArgs fy{};
+  FwdXArgs fx{};
+  for (int i = 0; i < 3; ++i) {
+    ax.in[i] = u[i]; ax.A[i] = h->A[i]; ax.B[i] = h->B[i];
+    ay.A[i] = h->A[i]; ay.B[i] = h->B[i];
+    ay.C[i] = h->C[i]; ay.D[i] = h->D[i]; ay.E[i] = h->E[i];
+    az.C[i] = h->C[i]; az.D[i] = h->D[i]; az.E[i] = h->E[i];
+    az.Qh[i] = h->A[i];
+    fy.Q[i] = h->A[i];
+    fx.Qh[i] = h->A[i]; fx.us[i] = u[i]; fx.out[i] = h->u1[i];
+    fx.fd[i] = h->f_dense[0] ? h->f_dense[i] : nullptr;
+  }
+  ax.qcut = h->qcut; ax.tw = h->tw[0];
+  ay.tw = h->tw[1]; az.tw = h->tw[2]; fy.tw = h->tw[1]; fx.tw = h->tw[0];
+  fx.fidx = h->f_idx; fx.fval = h->f_val; fx.fnnz = h->f_dense[0] ? 0 : h->f_nnz;
+  fx.dt = dt; fx.Re = Re; fx.ca = 0.0; fx.cb = 1.0;
+  cudaEvent_t ev[6];
+  for (auto& e : ev) cudaEventCreate(&e);
+  double acc[5] = {0, 0, 0, 0, 0};
+  cudaError_t err = cudaSuccess;
+  for (int r = 0; r <= reps && err == cudaSuccess; ++r) {
+    cudaEventRecord(ev[0], st);
+    if ((err = ns3d::run_inv_x(ax, g, st)) != cudaSuccess) break;
+    cudaEventRecord(ev[1], st);
+    if ((err = ns3d::run_inv_y(ay, g, st)) != cudaSuccess) break;
+    cudaEventRecord(ev[2], st);
+    if ((err = ns3d::run_z(az, g, st)) != cudaSuccess) break;
+    cudaEventRecord(ev[3], st);
+    if ((err = ns3d::run_fwd_y(fy, g, st)) != cudaSuccess) break;
+    cudaEventRecord(ev[4], st);
+    if ((err = ns3d::run_fwd_x(ns3d::kExplicit, false, fx, g, st)) != cudaSuccess) break;
+    cudaEventRecord(ev[5], st);
+    if ((err = cudaEventSynchronize(ev[5])) != cudaSuccess) break;
+    if (r == 0) continue;  // warm-up
+    for (int k = 0; k < 5; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (err != cudaSuccess) return cuda_fail(h, err, "profile_passes");
+  for (int k = 0; k < 5; ++k) ms[k] = acc[k] / reps;
+  return NS3D_OK;
+}
+
+}  // extern "C"

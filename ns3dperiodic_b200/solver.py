@@ -1,0 +1,238 @@
+"""Python host mirror of the reference's time-stepping interface.
+
+Method names follow Source/RK_time_step.h, Source/advection_2_3.h and the
+Krylov adapters of Source/NS3D_periodic.cu; each call goes through the C ABI
+(include/ns3d.h) into the sm_100a kernels.  Fields are CUDA complex128
+tensors of shape (Nx, Ny, Nz//2+1) in the reference layout; torch only
+provides device memory and streams.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Sequence
+
+from ._lib import Ns3dError, lib
+
+_PI2 = 2.0 * math.pi
+
+
+def _ptr(t) -> int:
+    return int(t.data_ptr())
+
+
+class Solver:
+    """One ns3d_solver handle (scratch, tables, stream) on one CUDA device."""
+
+    def __init__(self, Nx: int, Ny: int, Nz: int, Lx: float = _PI2, Ly: float = _PI2,
+                 Lz: float = _PI2, device=None):
+        import torch
+
+        self._torch = torch
+        dev = torch.device(device if device is not None else "cuda")
+        if dev.type != "cuda":
+            raise ValueError("the solver runs on CUDA devices only")
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)
+        self.Mz = self.Nz // 2 + 1
+        self.Lx, self.Ly, self.Lz = float(Lx), float(Ly), float(Lz)
+        self._L = lib()
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            torch.cuda.init()
+            rc = self._L.ns3d_create(self.Nx, self.Ny, self.Nz, self.Lx, self.Ly, self.Lz,
+                                     ctypes.byref(h))
+        if rc != 0:
+            raise Ns3dError(rc, "ns3d_create")
+        self._h = h
+        self._forcing = None  # keeps dense forcing tensors alive
+
+    # -- plumbing ---------------------------------------------------------
+    @property
+    def shape(self):
+        return (self.Nx, self.Ny, self.Mz)
+
+    def _check(self, rc: int, where: str):
+        if rc != 0:
+            detail = self._L.ns3d_last_error(self._h)
+            raise Ns3dError(rc, where, detail.decode() if detail else "")
+
+    def _fields(self, F: Sequence, name: str):
+        torch = self._torch
+        if len(F) != 3:
+            raise ValueError(f"{name}: need 3 components")
+        for f in F:
+            if (not isinstance(f, torch.Tensor) or f.dtype != torch.complex128
+                    or f.device != self.device or tuple(f.shape) != self.shape
+                    or not f.is_contiguous()):
+                raise ValueError(f"{name}: expected contiguous complex128 {self.shape} tensors "
+                                 f"on {self.device}")
+        return [_ptr(f) for f in F]
+
+    def zeros(self):
+        t = self._torch
+        return [t.zeros(self.shape, dtype=t.complex128, device=self.device) for _ in range(3)]
+
+    def to_device(self, F):
+        t = self._torch
+        return [t.as_tensor(f).to(device=self.device, dtype=t.complex128).contiguous() for f in F]
+
+    def synchronize(self):
+        self._check(self._L.ns3d_synchronize(self._h), "ns3d_synchronize")
+
+    def set_stream(self, stream):
+        """Use a torch.cuda.Stream (or raw handle int) for later launches."""
+        raw = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        self._check(self._L.ns3d_set_stream(self._h, ctypes.c_void_p(raw)), "ns3d_set_stream")
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._L.ns3d_device_bytes(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._L.ns3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- forcing ----------------------------------------------------------
+    def set_forcing(self, F):
+        if F is None:
+            self._check(self._L.ns3d_set_forcing(self._h, None, None, None), "set_forcing")
+            self._forcing = None
+            return
+        p = self._fields(F, "forcing")
+        self._check(self._L.ns3d_set_forcing(self._h, *p), "ns3d_set_forcing")
+        self._forcing = list(F)
+
+    @property
+    def forcing_modes(self) -> int:
+        return int(self._L.ns3d_forcing_modes(self._h))
+
+    # -- Source/RK_time_step.h --------------------------------------------
+    def rk3_ssp(self, U, dt: float, Re: float, nsteps: int = 1):
+        """RK3_SSP in place, nsteps times (CUDA-graph replay)."""
+        p = self._fields(U, "U")
+        self._check(self._L.ns3d_rk3_steps(self._h, *p, dt, Re, int(nsteps)), "ns3d_rk3_steps")
+        return U
+
+    def single_time_step(self, U, dt: float, Re: float):
+        p = self._fields(U, "U")
+        self._check(self._L.ns3d_euler_step(self._h, *p, dt, Re), "ns3d_euler_step")
+        return U
+
+    def return_rhs(self, U, Re: float, out=None):
+        out = out if out is not None else self.zeros()
+        p = self._fields(U, "U")
+        q = self._fields(out, "out")
+        self._check(self._L.ns3d_rhs(self._h, *p, *q, Re), "ns3d_rhs")
+        return out
+
+    def rk3_ssp_uv(self, U, V, dt: float, Re: float, nsteps: int = 1):
+        """RK3_SSP_UV: tangent V and base U advanced in place."""
+        p = self._fields(U, "U")
+        q = self._fields(V, "V")
+        self._check(self._L.ns3d_jvp_steps(self._h, *p, *q, dt, Re, int(nsteps)),
+                    "ns3d_jvp_steps")
+        return U, V
+
+    def rk3_ssp_uv_rhs(self, U, V, Re: float):
+        """RK3_SSP_UV_RHS: V <- J(U) V in place."""
+        p = self._fields(U, "U")
+        q = self._fields(V, "V")
+        self._check(self._L.ns3d_linearised_rhs(self._h, *p, *q, Re), "ns3d_linearised_rhs")
+        return V
+
+    def single_time_step_iuv_rhs(self, U, V, dt: float, Re: float):
+        p = self._fields(U, "U")
+        q = self._fields(V, "V")
+        self._check(self._L.ns3d_implicit_tangent_step(self._h, *p, *q, dt, Re),
+                    "ns3d_implicit_tangent_step")
+        return V
+
+    # -- Source/advection_2_3.h -------------------------------------------
+    def calculate_convolution_2p3(self, U, out=None):
+        out = out if out is not None else self.zeros()
+        self._check(self._L.ns3d_convolution(self._h, *self._fields(U, "U"),
+                                             *self._fields(out, "out")), "ns3d_convolution")
+        return out
+
+    def calculate_convolution_2p3_uv(self, U, V, out=None):
+        out = out if out is not None else self.zeros()
+        self._check(self._L.ns3d_convolution_uv(self._h, *self._fields(U, "U"),
+                                                *self._fields(V, "V"),
+                                                *self._fields(out, "out")),
+                    "ns3d_convolution_uv")
+        return out
+
+    # -- Krylov adapters (Source/NS3D_periodic.cu:173-385) ------------------
+    @property
+    def krylov_length(self) -> int:
+        return int(self._L.ns3d_krylov_length(self._h))
+
+    def _vec(self, v, name):
+        t = self._torch
+        if (v.dtype != t.float64 or v.device != self.device or v.numel() != self.krylov_length
+                or not v.is_contiguous()):
+            raise ValueError(f"{name}: expected contiguous float64 vector of length "
+                             f"{self.krylov_length} on {self.device}")
+        return _ptr(v)
+
+    def pack_reduced(self, V, out=None):
+        t = self._torch
+        out = out if out is not None else t.empty(self.krylov_length, dtype=t.float64,
+                                                  device=self.device)
+        self._check(self._L.ns3d_pack_reduced(self._h, *self._fields(V, "V"),
+                                              self._vec(out, "out")), "ns3d_pack_reduced")
+        return out
+
+    def unpack_reduced(self, vec, out=None):
+        out = out if out is not None else self.zeros()
+        self._check(self._L.ns3d_unpack_reduced(self._h, self._vec(vec, "vec"),
+                                                *self._fields(out, "out")),
+                    "ns3d_unpack_reduced")
+        return out
+
+    def matvec_reduced(self, U, vec_in, Re: float, tau: float = 0.0, out=None):
+        """NSCallMatrixVector_reduced (tau <= 0) / _Newton_Globalization (tau > 0)."""
+        t = self._torch
+        out = out if out is not None else t.empty_like(vec_in)
+        self._check(self._L.ns3d_matvec_reduced(self._h, *self._fields(U, "U"),
+                                                self._vec(vec_in, "vec_in"),
+                                                self._vec(out, "vec_out"), Re, tau),
+                    "ns3d_matvec_reduced")
+        return out
+
+    # -- diagnostics --------------------------------------------------------
+    def diagnostics(self, U):
+        """(energy, dissipation, max|div|) as the reference main loop reports them."""
+        e, d, dv = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self._L.ns3d_diagnostics(self._h, *self._fields(U, "U"), ctypes.byref(e),
+                                             ctypes.byref(d), ctypes.byref(dv)),
+                    "ns3d_diagnostics")
+        return e.value, d.value, dv.value
+
+
+    def profile_passes(self, U, dt: float, Re: float, reps: int = 10):
+        """Mean ms per launch of (inv_x, inv_y, z, fwd_y, fwd_x), CUDA events."""
+        ms = (ctypes.c_double * 5)()
+        self._check(self._L.ns3d_profile_passes(self._h, *self._fields(U, "U"), dt, Re,
+                                                int(reps), ms), "ns3d_profile_passes")
+        return list(ms)
+
+
+def supported_extent(n: int) -> bool:
+    return bool(lib().ns3d_supported_extent(int(n)))
