@@ -214,6 +214,36 @@ ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns
                                 double* ms);
 
 /* ----------------------------------------------------------------------- */
+/* allocation-free nonlinear term                                           */
+/* ----------------------------------------------------------------------- */
+
+/* Largest grid the allocation-free entry point accepts, as complex points
+ * per field (Nx * Ny * (Nz/2+1)); 64^3 fits.  The fixed scratch behind it is
+ * NS3D_NOALLOC_SCRATCH_BYTES of device memory. */
+#define NS3D_NOALLOC_MAX_POINTS 135168
+#define NS3D_NOALLOC_SCRATCH_BYTES 33005568
+
+/* No counterpart in the reference (which allocates its scratch in
+ * init_dealiasing).  Same result as ns3d_convolution, but without a handle and
+ * without allocating device memory: for callers that reserve all device
+ * memory up front in their own pool, that keep no handle between calls, or
+ * that cannot afford the synchronisation of cudaMalloc/cudaFree.  The
+ * scratch is a fixed array compiled into the library (about 33 MB per GPU,
+ * held from the first call on a device until the process exits).  The first
+ * call on each device looks up that array's device address and uploads the
+ * grid's twiddle and mask tables; make that first call before capturing the
+ * stream.  Later calls with the same grid reuse the tables.  All calls on a
+ * device share the array, so calls that overlap on the GPU race: serialise
+ * them (one stream, one host thread).  Runs on `stream` (cudaStream_t, 0 for
+ * the legacy default stream) on the current device.  Returns
+ * NS3D_ERR_BAD_ARG when Nx*Ny*(Nz/2+1) > NS3D_NOALLOC_MAX_POINTS (nothing is
+ * launched), NS3D_ERR_UNSUPPORTED for an extent without a compiled plan. */
+ns3d_status ns3d_convolution_noalloc(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                                     const ns3d_complex* ux, const ns3d_complex* uy,
+                                     const ns3d_complex* uz, ns3d_complex* Qx, ns3d_complex* Qy,
+                                     ns3d_complex* Qz, void* stream);
+
+/* ----------------------------------------------------------------------- */
 /* host-only helpers (no GPU needed)                                        */
 /* ----------------------------------------------------------------------- */
 

@@ -31,6 +31,7 @@ EXPORTS = (
     "ns3d_jvp_step", "ns3d_jvp_steps", "ns3d_linearised_rhs", "ns3d_implicit_tangent_step",
     "ns3d_krylov_length", "ns3d_pack_reduced", "ns3d_unpack_reduced", "ns3d_matvec_reduced",
     "ns3d_diagnostics", "ns3d_profile_passes", "ns3d_mask_cutoff", "ns3d_twiddles",
+    "ns3d_convolution_noalloc",
 )
 
 
@@ -85,6 +86,8 @@ def _sig(lib):
         "ns3d_profile_passes": ([_P] + [_P] * 3 + [c_double, c_double, c_int, _P], c_int),
         "ns3d_mask_cutoff": ([c_int, c_int, c_int, c_double, c_double, c_double, _P], c_int),
         "ns3d_twiddles": ([c_int, _P], c_int),
+        "ns3d_convolution_noalloc": ([c_int, c_int, c_int, c_double, c_double, c_double]
+                                     + [_P] * 6 + [_P], c_int),
     }
     for name, (args, res) in S.items():
         f = getattr(lib, name)

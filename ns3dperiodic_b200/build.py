@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(ROOT, "_build", "obj")
 LIB = os.path.join(HERE, "libns3d_b200.so")
 
-SOURCES = ["k_xy.cu", "k_z.cu", "k_fwdx.cu", "aux_kernels.cu", "solver.cu"]
+SOURCES = ["k_xy.cu", "k_z.cu", "k_fwdx.cu", "aux_kernels.cu", "solver.cu", "noalloc.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
