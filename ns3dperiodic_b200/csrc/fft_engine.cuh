@@ -209,11 +209,12 @@ struct Stages {
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = x[u + r * U];
       if constexpr (NS > 1) {
+        // stage table [r-1][jm] = exp(2 pi i jm r / (NS R)): consecutive lanes
+        // read consecutive entries
         const int jm = b % NS;
-        constexpr int step = N / (NS * R);
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          const double2 w = tw[jm * r * step];
+          const double2 w = tw[(r - 1) * NS + jm];
           v[r] = cmul(v[r], make_double2(w.x, DIR * w.y));
         }
       }
@@ -231,7 +232,8 @@ struct Stages {
       line_sync<T>();
 #pragma unroll
       for (int s = 0; s < P; ++s) x[s] = sbuf[spad<PADW>(t + T * s)];
-      Stages<N, T, DIR, PADW, NS * R, Rest...>::run(x, t, sbuf, tw);
+      Stages<N, T, DIR, PADW, NS * R, Rest...>::run(x, t, sbuf,
+                                                    NS > 1 ? tw + (R - 1) * NS : tw);
     }
   }
 };
@@ -291,12 +293,46 @@ struct FirstRadix<RadixList<R0, Rs...>> {
   static constexpr int value = R0;
 };
 
+// Per-stage twiddle tables of a plan, stage after stage (stages with NS > 1):
+// entry (r-1)*NS + jm of a stage = exp(2 pi i jm r step / N), step = N/(NS R).
+template <int N, int NS, typename L>
+struct StageTw;
+template <int N, int NS>
+struct StageTw<N, NS, RadixList<>> {
+  static constexpr int len = 0;
+  __device__ __forceinline__ static void fill(double2*, const double2* __restrict__) {}
+};
+template <int N, int NS, int R, int... Rest>
+struct StageTw<N, NS, RadixList<R, Rest...>> {
+  static constexpr int own = NS > 1 ? (R - 1) * NS : 0;
+  using Next = StageTw<N, NS * R, RadixList<Rest...>>;
+  static constexpr int len = own + Next::len;
+  __device__ __forceinline__ static void fill(double2* tws, const double2* __restrict__ tw_g) {
+    if constexpr (NS > 1) {
+      constexpr int step = N / (NS * R);
+      for (int e = threadIdx.x; e < own; e += blockDim.x) {
+        const int r = e / NS + 1, jm = e - (r - 1) * NS;
+        tws[e] = tw_g[jm * r * step];
+      }
+    }
+    Next::fill(tws + own, tw_g);
+  }
+};
+
 template <int N, int P>
 struct LineFFT {
   static constexpr int T = N / P;
   using L = typename Plan<N, P>::L;
   static constexpr int PADW = FirstRadix<L>::value < 4 ? 4 : FirstRadix<L>::value;
   static constexpr int BUF = line_buf_len<N, PADW>();
+  // shared-memory twiddle words the plan needs (N - first radix), at least 1
+  static constexpr int TWLEN = StageTw<N, 1, L>::len > 0 ? StageTw<N, 1, L>::len : 1;
+  // fills the per-stage table from the global table tw_g[e] = exp(2 pi i e / N);
+  // ends with a CTA barrier
+  __device__ __forceinline__ static void load_tw(double2* tws, const double2* __restrict__ tw_g) {
+    StageTw<N, 1, L>::fill(tws, tw_g);
+    __syncthreads();
+  }
   template <int DIR>
   __device__ __forceinline__ static void run(double2 (&x)[P], int t, double2* sbuf,
                                              const double2* __restrict__ tw) {

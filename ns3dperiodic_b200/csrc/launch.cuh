@@ -8,13 +8,28 @@
 namespace ns3d {
 
 // Extents with compiled plans.
+#ifndef NS3D_FOR_EACH_EXTENT
 #define NS3D_FOR_EACH_EXTENT(X) \
   X(8) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
+#endif
+
+// Points per thread of power-of-two extents, per pass family.
+#ifndef NS3D_PXY
+#define NS3D_PXY 16
+#endif
+#ifndef NS3D_PZ
+#define NS3D_PZ 8
+#endif
+#ifndef NS3D_PFX
+#define NS3D_PFX 16
+#endif
 
 // Points per thread: x/y passes that hold one or two lines per thread, and
 // the z / fwd_x passes that hold several fields per thread at once.
-constexpr int p_xy(int n) { return n % 3 == 0 ? 12 : 8; }
-constexpr int p_z(int n) { return n % 3 == 0 ? 12 : 8; }
+constexpr int p_pow2(int n, int p) { return p > n ? n : p; }
+constexpr int p_xy(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PXY); }
+constexpr int p_z(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PZ); }
+constexpr int p_fx(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PFX); }
 // the tangent z pass keeps u, v and the three products live: fewer points
 constexpr int p_zuv(int n) { return n % 3 == 0 ? 6 : 4; }
 
@@ -100,7 +115,7 @@ cudaError_t launch_fwd_x(const FwdXArgs& a, const PassGeom& g, cudaStream_t st) 
   switch (g.Nx) {
 #define NS3D_CASE(N)                                                               \
   case N: {                                                                        \
-    constexpr int P = p_z(N);                                                      \
+    constexpr int P = p_fx(N);                                                     \
     fwd_x_kernel<N, P, MODE, COMBINE><<<blocks_for(lines, lines_per_cta_xy<N, P>()), \
                                         kWarpsPerCta * 32, 0, st>>>(a, g);         \
     return cudaGetLastError();                                                     \

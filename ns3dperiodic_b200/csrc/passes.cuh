@@ -26,9 +26,18 @@ namespace ns3d {
 
 constexpr int kWarpsPerCta = 4;
 // Minimum resident CTAs per SM requested from ptxas (caps registers/thread).
-constexpr int kMinCtasXY = 3;
-constexpr int kMinCtasZ = 2;
-constexpr int kMinCtasFwdX = 3;
+#ifndef NS3D_MINCTA_XY
+#define NS3D_MINCTA_XY 2
+#endif
+#ifndef NS3D_MINCTA_Z
+#define NS3D_MINCTA_Z 2
+#endif
+#ifndef NS3D_MINCTA_FX
+#define NS3D_MINCTA_FX 2
+#endif
+constexpr int kMinCtasXY = NS3D_MINCTA_XY;
+constexpr int kMinCtasZ = NS3D_MINCTA_Z;
+constexpr int kMinCtasFwdX = NS3D_MINCTA_FX;
 
 struct PassGeom {
   int Nx, Ny, Nz, Mz;
@@ -39,12 +48,6 @@ struct PassGeom {
 // signed wavenumber index: j < N/2 -> j, else j - N (x and y; the Nyquist
 // index N/2 is stored as -N/2, Source/math_support.cu:354-357)
 __device__ __forceinline__ int signed_idx(int j, int n) { return j < (n >> 1) ? j : j - n; }
-
-template <int N>
-__device__ __forceinline__ void load_twiddles(double2* tw_s, const double2* __restrict__ tw_g) {
-  for (int e = threadIdx.x; e < N; e += blockDim.x) tw_s[e] = tw_g[e];
-  __syncthreads();
-}
 
 // Thread -> (line slot, t) for passes whose batch index is contiguous in
 // memory: lanes with the same t and consecutive lines are adjacent, so a warp
@@ -82,9 +85,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasXY) inv_x_kernel(In
   using F = LineFFT<NX, P>;
   constexpr int T = F::T;
   using LM = LaneMap<T>;
-  __shared__ double2 tw_s[NX];
+  __shared__ double2 tw_s[F::TWLEN];
   __shared__ double2 sbuf_all[LM::LPC][F::BUF];
-  load_twiddles<NX>(tw_s, a.tw);
+  F::load_tw(tw_s, a.tw);
   int li, t;
   LM::get(li, t);
   const int nlines = g.Ny * g.Mz;
@@ -102,25 +105,31 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasXY) inv_x_kernel(In
   }
 #pragma unroll 1
   for (int f = 0; f < NF; ++f) {
-    double2 va[P], vb[P];
+    // X then i kx X, one transform at a time: the second read of the line hits
+    // L1/L2, and only one line of P points is live in registers
+    double2 v[P];
 #pragma unroll
     for (int s = 0; s < P; ++s) {
       const int x = t + T * s;
-      double2 v = make_double2(0.0, 0.0);
-      if ((keep >> s) & 1u) v = __ldg(a.in[f] + (size_t)x * nlines + Lc);
+      v[s] = ((keep >> s) & 1u) ? __ldg(a.in[f] + (size_t)x * nlines + Lc) : make_double2(0.0, 0.0);
+    }
+    F::template run<+1>(v, t, sbuf, tw_s);
+    if (valid) {
+#pragma unroll
+      for (int s = 0; s < P; ++s) a.A[f][(size_t)(t + T * s) * nlines + L] = v[s];
+    }
+#pragma unroll
+    for (int s = 0; s < P; ++s) {
+      const int x = t + T * s;
+      const double2 u =
+          ((keep >> s) & 1u) ? __ldg(a.in[f] + (size_t)x * nlines + Lc) : make_double2(0.0, 0.0);
       const double kx = g.kfx * (double)signed_idx(x, NX);
-      va[s] = v;
-      vb[s] = make_double2(-v.y * kx, v.x * kx);  // i kx v (build_ders_device)
+      v[s] = make_double2(-u.y * kx, u.x * kx);  // i kx u (build_ders_device)
     }
-    F::template run<+1>(va, t, sbuf, tw_s);
+    F::template run<+1>(v, t, sbuf, tw_s);
     if (valid) {
 #pragma unroll
-      for (int s = 0; s < P; ++s) a.A[f][(size_t)(t + T * s) * nlines + L] = va[s];
-    }
-    F::template run<+1>(vb, t, sbuf, tw_s);
-    if (valid) {
-#pragma unroll
-      for (int s = 0; s < P; ++s) a.B[f][(size_t)(t + T * s) * nlines + L] = vb[s];
+      for (int s = 0; s < P; ++s) a.B[f][(size_t)(t + T * s) * nlines + L] = v[s];
     }
   }
 }
@@ -143,9 +152,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasXY) inv_y_kernel(In
   using F = LineFFT<NY, P>;
   constexpr int T = F::T;
   using LM = LaneMap<T>;
-  __shared__ double2 tw_s[NY];
+  __shared__ double2 tw_s[F::TWLEN];
   __shared__ double2 sbuf_all[LM::LPC][F::BUF];
-  load_twiddles<NY>(tw_s, a.tw);
+  F::load_tw(tw_s, a.tw);
   int li, t;
   LM::get(li, t);
   const int nb = g.Nx * g.Mz;
@@ -158,31 +167,32 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasXY) inv_y_kernel(In
   double2* sbuf = sbuf_all[li];
 #pragma unroll 1
   for (int f = 0; f < NF; ++f) {
-    double2 va[P], vd[P];
+    double2 v[P];
+#pragma unroll
+    for (int s = 0; s < P; ++s) v[s] = __ldg(a.A[f] + base + (size_t)(t + T * s) * stride);
+    F::template run<+1>(v, t, sbuf, tw_s);
+    if (valid) {
+#pragma unroll
+      for (int s = 0; s < P; ++s) a.C[f][base + (size_t)(t + T * s) * stride] = v[s];
+    }
 #pragma unroll
     for (int s = 0; s < P; ++s) {
       const int y = t + T * s;
-      const double2 v = __ldg(a.A[f] + base + (size_t)y * stride);
+      const double2 u = __ldg(a.A[f] + base + (size_t)y * stride);
       const double ky = g.kfy * (double)signed_idx(y, NY);
-      va[s] = v;
-      vd[s] = make_double2(-v.y * ky, v.x * ky);
+      v[s] = make_double2(-u.y * ky, u.x * ky);
     }
-    F::template run<+1>(va, t, sbuf, tw_s);
+    F::template run<+1>(v, t, sbuf, tw_s);
     if (valid) {
 #pragma unroll
-      for (int s = 0; s < P; ++s) a.C[f][base + (size_t)(t + T * s) * stride] = va[s];
-    }
-    F::template run<+1>(vd, t, sbuf, tw_s);
-    if (valid) {
-#pragma unroll
-      for (int s = 0; s < P; ++s) a.D[f][base + (size_t)(t + T * s) * stride] = vd[s];
+      for (int s = 0; s < P; ++s) a.D[f][base + (size_t)(t + T * s) * stride] = v[s];
     }
 #pragma unroll
-    for (int s = 0; s < P; ++s) va[s] = __ldg(a.B[f] + base + (size_t)(t + T * s) * stride);
-    F::template run<+1>(va, t, sbuf, tw_s);
+    for (int s = 0; s < P; ++s) v[s] = __ldg(a.B[f] + base + (size_t)(t + T * s) * stride);
+    F::template run<+1>(v, t, sbuf, tw_s);
     if (valid) {
 #pragma unroll
-      for (int s = 0; s < P; ++s) a.E[f][base + (size_t)(t + T * s) * stride] = va[s];
+      for (int s = 0; s < P; ++s) a.E[f][base + (size_t)(t + T * s) * stride] = v[s];
     }
   }
 }
@@ -308,9 +318,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
   using F = LineFFT<NZ, P>;
   constexpr int T = F::T;
   using LM = ZLaneMap<T>;
-  __shared__ double2 tw_s[NZ];
+  __shared__ double2 tw_s[F::TWLEN];
   __shared__ double2 sbuf_all[LM::LPC][F::BUF];
-  load_twiddles<NZ>(tw_s, a.tw);
+  F::load_tw(tw_s, a.tw);
   int li, t;
   LM::get(li, t);
   const int nb = g.Nx * g.Ny;
@@ -323,22 +333,40 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
   double2 w[P];
   double ux[P], uy[P], uz[P], q0[P], q1[P], q2[P];
   if constexpr (!UV) {
+    // Q_z first, so at most five real lines (u_x, u_y, u_z and two products)
+    // are live at any time.
     // (u_x, u_y)
     load_pair<NZ, P, false, false>(w, a.C[0], a.C[1], base, t, kfz);
     F::template run<+1>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { ux[s] = w[s].x * sc; uy[s] = w[s].y * sc; }
-    // (u_z, d_z u_x)
-    load_pair<NZ, P, false, true>(w, a.C[2], a.C[0], base, t, kfz);
+    // (u_z, d_z u_z) from one field
+    load_pair<NZ, P, false, true>(w, a.C[2], a.C[2], base, t, kfz);
     F::template run<+1>(w, t, sbuf, tw_s);
 #pragma unroll
-    for (int s = 0; s < P; ++s) { uz[s] = w[s].x * sc; q0[s] = w[s].y * sc; }
-    // (d_z u_y, d_z u_z)
-    load_pair<NZ, P, true, true>(w, a.C[1], a.C[2], base, t, kfz);
+    for (int s = 0; s < P; ++s) { uz[s] = w[s].x * sc; q2[s] = w[s].y * sc; }
+    // Q_z = u_x d_x u_z + u_y d_y u_z + u_z d_z u_z  (calc_vels_nabla_vels)
+    load_pair<NZ, P, false, false>(w, a.E[2], a.D[2], base, t, kfz);
     F::template run<+1>(w, t, sbuf, tw_s);
 #pragma unroll
-    for (int s = 0; s < P; ++s) { q1[s] = w[s].x * sc; q2[s] = w[s].y * sc; }
-    // Q_i = u_x d_x u_i + u_y d_y u_i + u_z d_z u_i  (calc_vels_nabla_vels)
+    for (int s = 0; s < P; ++s)
+      q2[s] = ux[s] * (w[s].x * sc) + uy[s] * (w[s].y * sc) + uz[s] * q2[s];
+    // R2C of Q_z alone
+#pragma unroll
+    for (int s = 0; s < P; ++s) w[s] = make_double2(q2[s], 0.0);
+    F::template run<-1>(w, t, sbuf, tw_s);
+    if (valid) {
+#pragma unroll
+      for (int s = 0; s < P; ++s) {
+        const int k = t + T * s;
+        if (k <= NZ / 2) a.Qh[2][base + k] = w[s];
+      }
+    }
+    // (d_z u_x, d_z u_y)
+    load_pair<NZ, P, true, true>(w, a.C[0], a.C[1], base, t, kfz);
+    F::template run<+1>(w, t, sbuf, tw_s);
+#pragma unroll
+    for (int s = 0; s < P; ++s) { q0[s] = w[s].x * sc; q1[s] = w[s].y * sc; }
     load_pair<NZ, P, false, false>(w, a.E[0], a.D[0], base, t, kfz);
     F::template run<+1>(w, t, sbuf, tw_s);
 #pragma unroll
@@ -349,11 +377,12 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
 #pragma unroll
     for (int s = 0; s < P; ++s)
       q1[s] = ux[s] * (w[s].x * sc) + uy[s] * (w[s].y * sc) + uz[s] * q1[s];
-    load_pair<NZ, P, false, false>(w, a.E[2], a.D[2], base, t, kfz);
-    F::template run<+1>(w, t, sbuf, tw_s);
+    // R2C of (Q_x, Q_y) packed
 #pragma unroll
-    for (int s = 0; s < P; ++s)
-      q2[s] = ux[s] * (w[s].x * sc) + uy[s] * (w[s].y * sc) + uz[s] * q2[s];
+    for (int s = 0; s < P; ++s) w[s] = make_double2(q0[s], q1[s]);
+    F::template run<-1>(w, t, sbuf, tw_s);
+    store_pair_spectrum<NZ, P>(w, sbuf, t, a.Qh[0], a.Qh[1], base, valid);
+    return;
   } else {
     // B(u,v)_i = (v.grad) u_i + (u.grad) v_i; fields 0..2 are u, 3..5 are v
     double vx[P], vy[P], vz[P];
@@ -403,9 +432,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasXY) fwd_y_kernel(Fw
   using F = LineFFT<NY, P>;
   constexpr int T = F::T;
   using LM = LaneMap<T>;
-  __shared__ double2 tw_s[NY];
+  __shared__ double2 tw_s[F::TWLEN];
   __shared__ double2 sbuf_all[LM::LPC][F::BUF];
-  load_twiddles<NY>(tw_s, a.tw);
+  F::load_tw(tw_s, a.tw);
   int li, t;
   LM::get(li, t);
   const int nb = g.Nx * g.Mz;
@@ -457,9 +486,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasFwdX) fwd_x_kernel(
   using F = LineFFT<NX, P>;
   constexpr int T = F::T;
   using LM = LaneMap<T>;
-  __shared__ double2 tw_s[NX];
+  __shared__ double2 tw_s[F::TWLEN];
   __shared__ double2 sbuf_all[LM::LPC][F::BUF];
-  load_twiddles<NX>(tw_s, a.tw);
+  F::load_tw(tw_s, a.tw);
   int li, t;
   LM::get(li, t);
   const int nlines = g.Ny * g.Mz;
@@ -468,12 +497,17 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasFwdX) fwd_x_kernel(
   const int Lc = valid ? L : 0;
   const int y = Lc / g.Mz, z = Lc - y * g.Mz;
   double2* sbuf = sbuf_all[li];
-  double2 q[3][P];
+  // Re(Qh) is set to zero (set_to_zero_real), so only the imaginary part of
+  // each transformed component is kept
+  double qi[3][P];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
+    double2 v[P];
 #pragma unroll
-    for (int s = 0; s < P; ++s) q[c][s] = __ldg(a.Qh[c] + (size_t)(t + T * s) * nlines + Lc);
-    F::template run<-1>(q[c], t, sbuf, tw_s);
+    for (int s = 0; s < P; ++s) v[s] = __ldg(a.Qh[c] + (size_t)(t + T * s) * nlines + Lc);
+    F::template run<-1>(v, t, sbuf, tw_s);
+#pragma unroll
+    for (int s = 0; s < P; ++s) qi[c][s] = v[s].y;
   }
   if (!valid) return;
   if constexpr (MODE == kConvOut) {
@@ -483,7 +517,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasFwdX) fwd_x_kernel(
       const size_t idx = (size_t)x * nlines + L;
       const bool origin = (x == 0) && (L == 0);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) a.out[c][idx] = make_double2(0.0, origin ? 0.0 : q[c][s].y);
+      for (int c = 0; c < 3; ++c) a.out[c][idx] = make_double2(0.0, origin ? 0.0 : qi[c][s]);
     }
     return;
   }
@@ -498,9 +532,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasFwdX) fwd_x_kernel(
     const double kk = kx * kx + ky * ky + kz * kz;
     // set_to_zero_real: Re(Qh) = 0 everywhere, Qh(0,0,0) = 0
     const bool origin = (x == 0) && (L == 0);
-    const double Q0 = origin ? 0.0 : q[0][s].y;
-    const double Q1 = origin ? 0.0 : q[1][s].y;
-    const double Q2 = origin ? 0.0 : q[2][s].y;
+    const double Q0 = origin ? 0.0 : qi[0][s];
+    const double Q1 = origin ? 0.0 : qi[1][s];
+    const double Q2 = origin ? 0.0 : qi[2][s];
     // AM.Q - Q with AM_ij = k_i k_j / |k|^2 (0 at k = 0); imaginary part only
     const double kq = kk > 0.0 ? (kx * Q0 + ky * Q1 + kz * Q2) / kk : 0.0;
     const double p[3] = {kx * kq - Q0, ky * kq - Q1, kz * kq - Q2};
