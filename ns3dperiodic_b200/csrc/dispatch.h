@@ -18,6 +18,10 @@ cudaError_t run_inv_y(const InvYArgs<6>& a, const PassGeom& g, cudaStream_t st);
 cudaError_t run_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream_t st);
 cudaError_t run_z(const ZArgs<3>& a, const PassGeom& g, cudaStream_t st);
 cudaError_t run_z(const ZArgs<6>& a, const PassGeom& g, cudaStream_t st);
+// Launch attributes of the pipelined passes for this geometry on the current
+// device; called when a handle is created (outside any stream capture).
+cudaError_t prepare_xy(const PassGeom& g);
+cudaError_t prepare_fwdx(const PassGeom& g);
 // mode: UpdateMode; combine: out = ca*un + cb*base
 cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs& a, const PassGeom& g,
                       cudaStream_t st);

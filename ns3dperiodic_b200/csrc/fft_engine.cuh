@@ -191,6 +191,12 @@ constexpr int line_buf_len() {
 // ---------------------------------------------------------------------------
 // Stockham stages
 // ---------------------------------------------------------------------------
+// Radix > 4 stages: read w, w^2, w^4, w^8 and compose the other twiddle
+// powers (1), or read every power from the table (0).
+#ifndef NS3D_TW_COMPOSE
+#define NS3D_TW_COMPOSE 1
+#endif
+constexpr bool kComposeTwiddles = NS3D_TW_COMPOSE != 0;
 template <int N, int T, int DIR, int PADW, int NS, int R, int... Rest>
 struct Stages {
   static constexpr int P = N / T;
@@ -209,14 +215,23 @@ struct Stages {
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = x[u + r * U];
       if constexpr (NS > 1) {
-        // stage table [r-1][jm] = exp(2 pi i jm r / (NS R)): consecutive lanes
-        // read consecutive entries
+        // stage table [r-1][jm] = w^r, w = exp(2 pi i jm / (NS R)); consecutive
+        // lanes read consecutive entries.  For R > 4 only w, w^2, w^4, w^8 are
+        // read and the other powers composed (at most 3 products deep).
         const int jm = b % NS;
+        double2 W[R];
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          const double2 w = tw[(r - 1) * NS + jm];
-          v[r] = cmul(v[r], make_double2(w.x, DIR * w.y));
+          if (!kComposeTwiddles || R <= 4 || r == 1 || r == 2 || r == 4 || r == 8) {
+            W[r] = tw[(r - 1) * NS + jm];
+          } else {
+            // r = hi + lo with hi the largest of 8, 4, 2 below r (lo >= 1)
+            const int hi = r > 8 ? 8 : (r > 4 ? 4 : 2);
+            W[r] = cmul(W[hi], W[r - hi]);
+          }
         }
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], make_double2(W[r].x, DIR * W[r].y));
       }
       DFT<R, DIR>::run(v);
       if constexpr (last) {

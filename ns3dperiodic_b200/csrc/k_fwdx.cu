@@ -21,4 +21,14 @@ cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs& a, const PassGeom&
   }
 }
 
+cudaError_t prepare_fwdx(const PassGeom& g) {
+  const FwdXArgs a{};
+  cudaError_t e;
+  if ((e = launch_fwd_x<kExplicit, false>(a, g, nullptr, true)) != cudaSuccess) return e;
+  if ((e = launch_fwd_x<kExplicit, true>(a, g, nullptr, true)) != cudaSuccess) return e;
+  if ((e = launch_fwd_x<kRhs, false>(a, g, nullptr, true)) != cudaSuccess) return e;
+  if ((e = launch_fwd_x<kImplicit, false>(a, g, nullptr, true)) != cudaSuccess) return e;
+  return launch_fwd_x<kConvOut, false>(a, g, nullptr, true);
+}
+
 }  // namespace ns3d

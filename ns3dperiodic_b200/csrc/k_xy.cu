@@ -22,4 +22,13 @@ cudaError_t run_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream_t st) {
   return launch_fwd_y(a, g, st);
 }
 
+cudaError_t prepare_xy(const PassGeom& g) {
+  cudaError_t e;
+  if ((e = launch_inv_x<3>(InvXArgs<3>{}, g, nullptr, true)) != cudaSuccess) return e;
+  if ((e = launch_inv_x<6>(InvXArgs<6>{}, g, nullptr, true)) != cudaSuccess) return e;
+  if ((e = launch_inv_y<3>(InvYArgs<3>{}, g, nullptr, true)) != cudaSuccess) return e;
+  if ((e = launch_inv_y<6>(InvYArgs<6>{}, g, nullptr, true)) != cudaSuccess) return e;
+  return launch_fwd_y(FwdYArgs{}, g, nullptr, true);
+}
+
 }  // namespace ns3d

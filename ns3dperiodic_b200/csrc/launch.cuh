@@ -55,16 +55,46 @@ constexpr int lines_per_cta_z() {
 
 inline unsigned blocks_for(long long lines, int lpc) { return (unsigned)((lines + lpc - 1) / lpc); }
 
+// Persistent grid for a pipelined pass: set the dynamic shared-memory
+// attribute and query the resident CTAs per SM once per kernel instantiation
+// (Tag) and device; grid = min(groups, SMs x resident CTAs).
+template <int KIND, int N, int P, int X>
+struct KTag {};
+
+template <typename Tag, typename Kern>
+inline unsigned persistent_grid(Kern kern, size_t smem, long long groups) {
+  static int per_sm[64] = {};
+  static int sms[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  dev &= 63;
+  if (per_sm[dev] == 0) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem);
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    sms[dev] = n > 0 ? n : 1;
+    per_sm[dev] = occ > 0 ? occ : 1;
+  }
+  const long long cap = NS3D_SCHED == 0 ? groups : (long long)sms[dev] * per_sm[dev];
+  return (unsigned)(groups < cap ? (groups > 0 ? groups : 1) : cap);
+}
+
 template <int NF>
-cudaError_t launch_inv_x(const InvXArgs<NF>& a, const PassGeom& g, cudaStream_t st) {
+cudaError_t launch_inv_x(const InvXArgs<NF>& a, const PassGeom& g, cudaStream_t st,
+                         bool prepare_only = false) {
   const long long lines = (long long)g.Ny * g.Mz;
   switch (g.Nx) {
-#define NS3D_CASE(N)                                                               \
-  case N: {                                                                        \
-    constexpr int P = p_xy(N);                                                     \
-    inv_x_kernel<N, P, NF><<<blocks_for(lines, lines_per_cta_xy<N, P>()),         \
-                             kWarpsPerCta * 32, 0, st>>>(a, g);                    \
-    return cudaGetLastError();                                                     \
+#define NS3D_CASE(N)                                                                    \
+  case N: {                                                                             \
+    constexpr int P = p_xy(N);                                                          \
+    using S = PassSmem<N, P>;                                                           \
+    const unsigned grid = persistent_grid<KTag<0, N, P, NF>>(                           \
+        inv_x_kernel<N, P, NF>, S::BYTES, (lines + S::LPC - 1) / S::LPC);                \
+    if (prepare_only) return cudaGetLastError();                                        \
+    inv_x_kernel<N, P, NF><<<grid, kThreads, S::BYTES, st>>>(a, g);                      \
+    return cudaGetLastError();                                                          \
   }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE
@@ -74,15 +104,19 @@ cudaError_t launch_inv_x(const InvXArgs<NF>& a, const PassGeom& g, cudaStream_t 
 }
 
 template <int NF>
-cudaError_t launch_inv_y(const InvYArgs<NF>& a, const PassGeom& g, cudaStream_t st) {
+cudaError_t launch_inv_y(const InvYArgs<NF>& a, const PassGeom& g, cudaStream_t st,
+                         bool prepare_only = false) {
   const long long lines = (long long)g.Nx * g.Mz;
   switch (g.Ny) {
-#define NS3D_CASE(N)                                                               \
-  case N: {                                                                        \
-    constexpr int P = p_xy(N);                                                     \
-    inv_y_kernel<N, P, NF><<<blocks_for(lines, lines_per_cta_xy<N, P>()),         \
-                             kWarpsPerCta * 32, 0, st>>>(a, g);                    \
-    return cudaGetLastError();                                                     \
+#define NS3D_CASE(N)                                                                    \
+  case N: {                                                                             \
+    constexpr int P = p_xy(N);                                                          \
+    using S = PassSmem<N, P>;                                                           \
+    const unsigned grid = persistent_grid<KTag<1, N, P, NF>>(                           \
+        inv_y_kernel<N, P, NF>, S::BYTES, (lines + S::LPC - 1) / S::LPC);                \
+    if (prepare_only) return cudaGetLastError();                                        \
+    inv_y_kernel<N, P, NF><<<grid, kThreads, S::BYTES, st>>>(a, g);                      \
+    return cudaGetLastError();                                                          \
   }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE
@@ -110,15 +144,19 @@ cudaError_t launch_z(const ZArgs<UV ? 6 : 3>& a, const PassGeom& g, cudaStream_t
 }
 
 template <int MODE, bool COMBINE>
-cudaError_t launch_fwd_x(const FwdXArgs& a, const PassGeom& g, cudaStream_t st) {
+cudaError_t launch_fwd_x(const FwdXArgs& a, const PassGeom& g, cudaStream_t st,
+                         bool prepare_only = false) {
   const long long lines = (long long)g.Ny * g.Mz;
   switch (g.Nx) {
-#define NS3D_CASE(N)                                                               \
-  case N: {                                                                        \
-    constexpr int P = p_fx(N);                                                     \
-    fwd_x_kernel<N, P, MODE, COMBINE><<<blocks_for(lines, lines_per_cta_xy<N, P>()), \
-                                        kWarpsPerCta * 32, 0, st>>>(a, g);         \
-    return cudaGetLastError();                                                     \
+#define NS3D_CASE(N)                                                                    \
+  case N: {                                                                             \
+    constexpr int P = p_fx(N);                                                          \
+    using S = PassSmem<N, P>;                                                           \
+    const unsigned grid = persistent_grid<KTag<2 + 2 * MODE + (COMBINE ? 1 : 0), N, P, 0>>( \
+        fwd_x_kernel<N, P, MODE, COMBINE>, S::BYTES, (lines + S::LPC - 1) / S::LPC);     \
+    if (prepare_only) return cudaGetLastError();                                        \
+    fwd_x_kernel<N, P, MODE, COMBINE><<<grid, kThreads, S::BYTES, st>>>(a, g);           \
+    return cudaGetLastError();                                                          \
   }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE
@@ -127,15 +165,19 @@ cudaError_t launch_fwd_x(const FwdXArgs& a, const PassGeom& g, cudaStream_t st) 
   }
 }
 
-inline cudaError_t launch_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream_t st) {
+inline cudaError_t launch_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream_t st,
+                                bool prepare_only = false) {
   const long long lines = (long long)g.Nx * g.Mz;
   switch (g.Ny) {
-#define NS3D_CASE(N)                                                               \
-  case N: {                                                                        \
-    constexpr int P = p_xy(N);                                                     \
-    fwd_y_kernel<N, P><<<blocks_for(lines, lines_per_cta_xy<N, P>()),             \
-                         kWarpsPerCta * 32, 0, st>>>(a, g);                        \
-    return cudaGetLastError();                                                     \
+#define NS3D_CASE(N)                                                                    \
+  case N: {                                                                             \
+    constexpr int P = p_xy(N);                                                          \
+    using S = PassSmem<N, P>;                                                           \
+    const unsigned grid = persistent_grid<KTag<20, N, P, 0>>(                           \
+        fwd_y_kernel<N, P>, S::BYTES, (lines + S::LPC - 1) / S::LPC);                    \
+    if (prepare_only) return cudaGetLastError();                                        \
+    fwd_y_kernel<N, P><<<grid, kThreads, S::BYTES, st>>>(a, g);                          \
+    return cudaGetLastError();                                                          \
   }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE

@@ -68,6 +68,103 @@ struct LaneMap {
   }
 };
 
+
+// ---------------------------------------------------------------------------
+// Persistent, software-pipelined x / y passes.  Each CTA walks groups of LPC
+// lines (grid = resident CTAs); every thread owns a private double buffer in
+// shared memory and, while the current line of field f is transformed,
+// prefetches with cp.async the P samples it will need for the next unit (the
+// next field of the same lines, or the first field of the next group).
+// ---------------------------------------------------------------------------
+constexpr int kThreads = kWarpsPerCta * 32;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred = true) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = pred ? 16 : 0;  // 0: nothing is read, the slot is zero-filled
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Copies the P samples t + T*s (s < P) of one line into a private slot:
+// slot[s*kThreads] <- src[base + (t + T*s) * stride], skipping (zero-filling)
+// the samples whose bit in `keep` is clear.
+template <int P, int T>
+__device__ __forceinline__ void issue_line(double2* slot, const double2* __restrict__ src,
+                                           size_t base, size_t stride, int t,
+                                           uint32_t keep = 0xffffffffu) {
+#pragma unroll
+  for (int s = 0; s < P; ++s)
+    cp_async16(slot + s * kThreads, src + base + (size_t)(t + T * s) * stride, (keep >> s) & 1u);
+}
+
+// Smallest line-buffer stride >= len whose residue mod 8 (16-byte slots; one
+// shared-memory wavefront is 8 slots) is `target`, 0 meaning any.
+constexpr int line_stride(int len, int target) {
+  return target == 0 ? len : (len % 8 == target % 8 ? len : line_stride(len + 1, target));
+}
+// LaneMap puts LPW lines side by side in a quarter warp: give each its own
+// 16-byte slots.
+template <int T>
+constexpr int xy_stride_target() {
+  constexpr int lpw = T <= 32 ? 32 / T : 1;
+  constexpr int per_phase = lpw < 8 ? lpw : 8;
+  return per_phase <= 1 ? 0 : 8 / per_phase;
+}
+
+
+// Work distribution of the pipelined passes over groups of lines:
+//   NS3D_SCHED 0: one group per CTA (grid = groups; the hardware scheduler
+//                 keeps the resident CTAs on a window of neighbouring groups),
+//   NS3D_SCHED 1: persistent CTAs, groups dealt round robin,
+//   NS3D_SCHED 2: persistent CTAs, one contiguous range of groups each.
+#ifndef NS3D_SCHED
+#define NS3D_SCHED 0
+#endif
+struct GroupRange {
+  int grp, end, step;
+};
+__device__ __forceinline__ GroupRange group_range(int groups) {
+  if (NS3D_SCHED == 2) {
+    return {(int)(((long long)blockIdx.x * groups) / gridDim.x),
+            (int)(((long long)(blockIdx.x + 1) * groups) / gridDim.x), 1};
+  }
+  return {(int)blockIdx.x, groups, (int)gridDim.x};
+}
+
+// Dynamic shared memory of a pipelined pass, in double2 words.
+template <int N, int P>
+struct PassSmem {
+  using F = LineFFT<N, P>;
+  using LM = LaneMap<F::T>;
+  static constexpr int LPC = LM::LPC;
+  static constexpr int STRIDE = line_stride(F::BUF, xy_stride_target<F::T>());
+  static constexpr int TW = 0;
+  static constexpr int SBUF = F::TWLEN;
+  static constexpr int PF = SBUF + LPC * STRIDE;
+  static constexpr int WORDS = PF + 2 * P * kThreads;
+  static constexpr size_t BYTES = (size_t)WORDS * sizeof(double2);
+  static_assert(BYTES <= 227 * 1024, "shared memory per CTA");
+};
+
+template <int NX>
+__device__ __forceinline__ uint32_t mask_bits(const uint16_t* __restrict__ qcut, int Ny, int y,
+                                              int z, int L, bool valid, int t, int T, int P) {
+  uint32_t keep = 0;
+  for (int s = 0; s < P; ++s) {
+    const int x = t + T * s;
+    const bool k = valid && z < (int)__ldg(qcut + x * Ny + y) && !(x == 0 && L == 0);
+    keep |= (uint32_t)k << s;
+  }
+  return keep;
+}
+
 // ---------------------------------------------------------------------------
 // inv_x: lines along x, batch L = y*Mz + z (contiguous), NF = 3 or 6 fields
 // ---------------------------------------------------------------------------
@@ -81,57 +178,86 @@ struct InvXArgs {
 };
 
 template <int NX, int P, int NF>
-__global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasXY) inv_x_kernel(InvXArgs<NF> a, PassGeom g) {
-  using F = LineFFT<NX, P>;
+__global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF> a, PassGeom g) {
+  using S = PassSmem<NX, P>;
+  using F = typename S::F;
+  using LM = typename S::LM;
   constexpr int T = F::T;
-  using LM = LaneMap<T>;
-  __shared__ double2 tw_s[F::TWLEN];
-  __shared__ double2 sbuf_all[LM::LPC][F::BUF];
-  F::load_tw(tw_s, a.tw);
+  extern __shared__ double2 dsm[];
+  F::load_tw(dsm + S::TW, a.tw);
+  const double2* tw_s = dsm + S::TW;
   int li, t;
   LM::get(li, t);
+  double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
+  double2* pf = dsm + S::PF + threadIdx.x;
   const int nlines = g.Ny * g.Mz;
-  const int L = blockIdx.x * LM::LPC + li;
-  const bool valid = L < nlines;
-  const int Lc = valid ? L : 0;
-  const int y = Lc / g.Mz, z = Lc - y * g.Mz;
-  double2* sbuf = sbuf_all[li];
-  uint32_t keep = 0;  // bit s: mode (t + T s, y, z) survives the 2/3 mask
-#pragma unroll
-  for (int s = 0; s < P; ++s) {
-    const int x = t + T * s;
-    const bool k = valid && z < (int)__ldg(a.qcut + x * g.Ny + y) && !(x == 0 && Lc == 0);
-    keep |= (uint32_t)k << s;
+  const int groups = (nlines + LM::LPC - 1) / LM::LPC;
+  // each CTA takes a contiguous range of groups, so neighbouring lines (which
+  // share partially covered 32-byte sectors) are handled back to back
+  const GroupRange gr = group_range(groups);
+  const int g_end = gr.end;
+  int grp = gr.grp;
+  if (grp >= g_end) return;  // uniform across the CTA
+  uint32_t keep;             // bit s: mode (t + T s, y, z) survives the 2/3 mask
+  {
+    const int L = grp * LM::LPC + li;
+    const bool valid = L < nlines;
+    const int Lc = valid ? L : 0;
+    const int y = Lc / g.Mz, z = Lc - y * g.Mz;
+    keep = mask_bits<NX>(a.qcut, g.Ny, y, z, Lc, valid, t, T, P);
+    issue_line<P, T>(pf, a.in[0], (size_t)Lc, (size_t)nlines, t, keep);
+    cp_async_commit();
   }
-#pragma unroll 1
-  for (int f = 0; f < NF; ++f) {
-    // X then i kx X, one transform at a time: the second read of the line hits
-    // L1/L2, and only one line of P points is live in registers
-    double2 v[P];
-#pragma unroll
-    for (int s = 0; s < P; ++s) {
-      const int x = t + T * s;
-      v[s] = ((keep >> s) & 1u) ? __ldg(a.in[f] + (size_t)x * nlines + Lc) : make_double2(0.0, 0.0);
+  int ub = 0;
+  for (; grp < g_end; grp += gr.step) {
+    const int L = grp * LM::LPC + li;
+    const bool valid = L < nlines;
+    const int Lc = valid ? L : 0;
+    const int gn = grp + gr.step;
+    const int Ln = gn * LM::LPC + li;
+    const bool validn = Ln < nlines;
+    const int Lnc = validn ? Ln : 0;
+    uint32_t keep_next = 0;
+    if (gn < g_end) {
+      const int yn = Lnc / g.Mz, zn = Lnc - yn * g.Mz;
+      keep_next = mask_bits<NX>(a.qcut, g.Ny, yn, zn, Lnc, validn, t, T, P);
     }
-    F::template run<+1>(v, t, sbuf, tw_s);
-    if (valid) {
 #pragma unroll
-      for (int s = 0; s < P; ++s) a.A[f][(size_t)(t + T * s) * nlines + L] = v[s];
-    }
+    for (int f = 0; f < NF; ++f) {
+      const double2* cur = pf + ub * (P * kThreads);
+      double2* nxt = pf + (ub ^ 1) * (P * kThreads);
+      if (f + 1 < NF) {
+        issue_line<P, T>(nxt, a.in[f + 1], (size_t)Lc, (size_t)nlines, t, keep);
+      } else if (gn < g_end) {
+        issue_line<P, T>(nxt, a.in[0], (size_t)Lnc, (size_t)nlines, t, keep_next);
+      }
+      cp_async_commit();
+      cp_async_wait<1>();
+      // X (masked) then i kx X, both from the prefetched samples
+      double2 v[P];
 #pragma unroll
-    for (int s = 0; s < P; ++s) {
-      const int x = t + T * s;
-      const double2 u =
-          ((keep >> s) & 1u) ? __ldg(a.in[f] + (size_t)x * nlines + Lc) : make_double2(0.0, 0.0);
-      const double kx = g.kfx * (double)signed_idx(x, NX);
-      v[s] = make_double2(-u.y * kx, u.x * kx);  // i kx u (build_ders_device)
-    }
-    F::template run<+1>(v, t, sbuf, tw_s);
-    if (valid) {
+      for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
+      F::template run<+1>(v, t, sbuf, tw_s);
+      if (valid) {
 #pragma unroll
-      for (int s = 0; s < P; ++s) a.B[f][(size_t)(t + T * s) * nlines + L] = v[s];
+        for (int s = 0; s < P; ++s) a.A[f][(size_t)(t + T * s) * nlines + L] = v[s];
+      }
+#pragma unroll
+      for (int s = 0; s < P; ++s) {
+        const double2 u = cur[s * kThreads];
+        const double kx = g.kfx * (double)signed_idx(t + T * s, NX);
+        v[s] = make_double2(-u.y * kx, u.x * kx);  // i kx u (build_ders_device)
+      }
+      F::template run<+1>(v, t, sbuf, tw_s);
+      if (valid) {
+#pragma unroll
+        for (int s = 0; s < P; ++s) a.B[f][(size_t)(t + T * s) * nlines + L] = v[s];
+      }
+      ub ^= 1;
     }
+    keep = keep_next;
   }
+  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -148,53 +274,93 @@ struct InvYArgs {
 };
 
 template <int NY, int P, int NF>
-__global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasXY) inv_y_kernel(InvYArgs<NF> a, PassGeom g) {
-  using F = LineFFT<NY, P>;
+__global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF> a, PassGeom g) {
+  using S = PassSmem<NY, P>;
+  using F = typename S::F;
+  using LM = typename S::LM;
   constexpr int T = F::T;
-  using LM = LaneMap<T>;
-  __shared__ double2 tw_s[F::TWLEN];
-  __shared__ double2 sbuf_all[LM::LPC][F::BUF];
-  F::load_tw(tw_s, a.tw);
+  extern __shared__ double2 dsm[];
+  F::load_tw(dsm + S::TW, a.tw);
+  const double2* tw_s = dsm + S::TW;
   int li, t;
   LM::get(li, t);
+  double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
+  double2* pf = dsm + S::PF + threadIdx.x;
   const int nb = g.Nx * g.Mz;
-  const int b = blockIdx.x * LM::LPC + li;
-  const bool valid = b < nb;
-  const int bc = valid ? b : 0;
-  const int x = bc / g.Mz, z = bc - x * g.Mz;
-  const size_t base = (size_t)x * g.Ny * g.Mz + z;
-  const int stride = g.Mz;
-  double2* sbuf = sbuf_all[li];
-#pragma unroll 1
-  for (int f = 0; f < NF; ++f) {
-    double2 v[P];
+  const int groups = (nb + LM::LPC - 1) / LM::LPC;
+  const size_t stride = (size_t)g.Mz;
+  const GroupRange gr = group_range(groups);
+  const int g_end = gr.end;
+  int grp = gr.grp;
+  if (grp >= g_end) return;
+  auto line_base = [&](int gidx) -> size_t {
+    const int b = gidx * LM::LPC + li;
+    const int bc = b < nb ? b : 0;
+    const int x = bc / g.Mz, z = bc - x * g.Mz;
+    return (size_t)x * g.Ny * g.Mz + z;
+  };
+  issue_line<P, T>(pf, a.A[0], line_base(grp), stride, t);
+  cp_async_commit();
+  int ub = 0;
+  for (; grp < g_end; grp += gr.step) {
+    const bool valid = grp * LM::LPC + li < nb;
+    const size_t base = line_base(grp);
+    const int gn = grp + gr.step;
+    const size_t basen = line_base(gn < g_end ? gn : grp);
 #pragma unroll
-    for (int s = 0; s < P; ++s) v[s] = __ldg(a.A[f] + base + (size_t)(t + T * s) * stride);
-    F::template run<+1>(v, t, sbuf, tw_s);
-    if (valid) {
+    for (int f = 0; f < NF; ++f) {
+      // unit A[f] -> C[f] = IFFT_y A, D[f] = IFFT_y(i ky A)
+      {
+        const double2* cur = pf + ub * (P * kThreads);
+        double2* nxt = pf + (ub ^ 1) * (P * kThreads);
+        issue_line<P, T>(nxt, a.B[f], base, stride, t);
+        cp_async_commit();
+        cp_async_wait<1>();
+        double2 v[P];
 #pragma unroll
-      for (int s = 0; s < P; ++s) a.C[f][base + (size_t)(t + T * s) * stride] = v[s];
-    }
+        for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
+        F::template run<+1>(v, t, sbuf, tw_s);
+        if (valid) {
 #pragma unroll
-    for (int s = 0; s < P; ++s) {
-      const int y = t + T * s;
-      const double2 u = __ldg(a.A[f] + base + (size_t)y * stride);
-      const double ky = g.kfy * (double)signed_idx(y, NY);
-      v[s] = make_double2(-u.y * ky, u.x * ky);
-    }
-    F::template run<+1>(v, t, sbuf, tw_s);
-    if (valid) {
+          for (int s = 0; s < P; ++s) a.C[f][base + (size_t)(t + T * s) * stride] = v[s];
+        }
 #pragma unroll
-      for (int s = 0; s < P; ++s) a.D[f][base + (size_t)(t + T * s) * stride] = v[s];
-    }
+        for (int s = 0; s < P; ++s) {
+          const double2 u = cur[s * kThreads];
+          const double ky = g.kfy * (double)signed_idx(t + T * s, NY);
+          v[s] = make_double2(-u.y * ky, u.x * ky);
+        }
+        F::template run<+1>(v, t, sbuf, tw_s);
+        if (valid) {
 #pragma unroll
-    for (int s = 0; s < P; ++s) v[s] = __ldg(a.B[f] + base + (size_t)(t + T * s) * stride);
-    F::template run<+1>(v, t, sbuf, tw_s);
-    if (valid) {
+          for (int s = 0; s < P; ++s) a.D[f][base + (size_t)(t + T * s) * stride] = v[s];
+        }
+        ub ^= 1;
+      }
+      // unit B[f] -> E[f] = IFFT_y B
+      {
+        const double2* cur = pf + ub * (P * kThreads);
+        double2* nxt = pf + (ub ^ 1) * (P * kThreads);
+        if (f + 1 < NF) {
+          issue_line<P, T>(nxt, a.A[f + 1], base, stride, t);
+        } else if (gn < g_end) {
+          issue_line<P, T>(nxt, a.A[0], basen, stride, t);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();
+        double2 v[P];
 #pragma unroll
-      for (int s = 0; s < P; ++s) a.E[f][base + (size_t)(t + T * s) * stride] = v[s];
+        for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
+        F::template run<+1>(v, t, sbuf, tw_s);
+        if (valid) {
+#pragma unroll
+          for (int s = 0; s < P; ++s) a.E[f][base + (size_t)(t + T * s) * stride] = v[s];
+        }
+        ub ^= 1;
+      }
     }
   }
+  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -428,34 +594,62 @@ struct FwdYArgs {
 };
 
 template <int NY, int P>
-__global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasXY) fwd_y_kernel(FwdYArgs a, PassGeom g) {
-  using F = LineFFT<NY, P>;
+__global__ void __launch_bounds__(kThreads, kMinCtasXY) fwd_y_kernel(FwdYArgs a, PassGeom g) {
+  using S = PassSmem<NY, P>;
+  using F = typename S::F;
+  using LM = typename S::LM;
   constexpr int T = F::T;
-  using LM = LaneMap<T>;
-  __shared__ double2 tw_s[F::TWLEN];
-  __shared__ double2 sbuf_all[LM::LPC][F::BUF];
-  F::load_tw(tw_s, a.tw);
+  extern __shared__ double2 dsm[];
+  F::load_tw(dsm + S::TW, a.tw);
+  const double2* tw_s = dsm + S::TW;
   int li, t;
   LM::get(li, t);
+  double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
+  double2* pf = dsm + S::PF + threadIdx.x;
   const int nb = g.Nx * g.Mz;
-  const int b = blockIdx.x * LM::LPC + li;
-  const bool valid = b < nb;
-  const int bc = valid ? b : 0;
-  const int x = bc / g.Mz, z = bc - x * g.Mz;
-  const size_t base = (size_t)x * g.Ny * g.Mz + z;
-  const int stride = g.Mz;
-  double2* sbuf = sbuf_all[li];
-#pragma unroll 1
-  for (int f = 0; f < 3; ++f) {
-    double2 v[P];
+  const int groups = (nb + LM::LPC - 1) / LM::LPC;
+  const size_t stride = (size_t)g.Mz;
+  const GroupRange gr = group_range(groups);
+  const int g_end = gr.end;
+  int grp = gr.grp;
+  if (grp >= g_end) return;
+  auto line_base = [&](int gidx) -> size_t {
+    const int b = gidx * LM::LPC + li;
+    const int bc = b < nb ? b : 0;
+    const int x = bc / g.Mz, z = bc - x * g.Mz;
+    return (size_t)x * g.Ny * g.Mz + z;
+  };
+  issue_line<P, T>(pf, a.Q[0], line_base(grp), stride, t);
+  cp_async_commit();
+  int ub = 0;
+  for (; grp < g_end; grp += gr.step) {
+    const bool valid = grp * LM::LPC + li < nb;
+    const size_t base = line_base(grp);
+    const int gn = grp + gr.step;
+    const size_t basen = line_base(gn < g_end ? gn : grp);
 #pragma unroll
-    for (int s = 0; s < P; ++s) v[s] = a.Q[f][base + (size_t)(t + T * s) * stride];
-    F::template run<-1>(v, t, sbuf, tw_s);
-    if (valid) {
+    for (int f = 0; f < 3; ++f) {
+      const double2* cur = pf + ub * (P * kThreads);
+      double2* nxt = pf + (ub ^ 1) * (P * kThreads);
+      if (f + 1 < 3) {
+        issue_line<P, T>(nxt, a.Q[f + 1], base, stride, t);
+      } else if (gn < g_end) {
+        issue_line<P, T>(nxt, a.Q[0], basen, stride, t);
+      }
+      cp_async_commit();
+      cp_async_wait<1>();
+      double2 v[P];
 #pragma unroll
-      for (int s = 0; s < P; ++s) a.Q[f][base + (size_t)(t + T * s) * stride] = v[s];
+      for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
+      F::template run<-1>(v, t, sbuf, tw_s);
+      if (valid) {
+#pragma unroll
+        for (int s = 0; s < P; ++s) a.Q[f][base + (size_t)(t + T * s) * stride] = v[s];
+      }
+      ub ^= 1;
     }
   }
+  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -481,33 +675,38 @@ struct FwdXArgs {
   const double2* tw;
 };
 
+// One line of the forward x pass: FFT_x of the 3 product spectra (from the
+// prefetch slots), then the pointwise update of Source/diffusion.cu.
 template <int NX, int P, int MODE, bool COMBINE>
-__global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasFwdX) fwd_x_kernel(FwdXArgs a, PassGeom g) {
+__device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g, int t, int L,
+                                           int Lc, bool valid, double2* sbuf,
+                                           const double2* tw_s, double2* pf, int& ub,
+                                           bool more, size_t Lnc) {
+  constexpr int T = NX / P;
   using F = LineFFT<NX, P>;
-  constexpr int T = F::T;
-  using LM = LaneMap<T>;
-  __shared__ double2 tw_s[F::TWLEN];
-  __shared__ double2 sbuf_all[LM::LPC][F::BUF];
-  F::load_tw(tw_s, a.tw);
-  int li, t;
-  LM::get(li, t);
   const int nlines = g.Ny * g.Mz;
-  const int L = blockIdx.x * LM::LPC + li;
-  const bool valid = L < nlines;
-  const int Lc = valid ? L : 0;
   const int y = Lc / g.Mz, z = Lc - y * g.Mz;
-  double2* sbuf = sbuf_all[li];
   // Re(Qh) is set to zero (set_to_zero_real), so only the imaginary part of
   // each transformed component is kept
   double qi[3][P];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
+    const double2* cur = pf + ub * (P * kThreads);
+    double2* nxt = pf + (ub ^ 1) * (P * kThreads);
+    if (c + 1 < 3) {
+      issue_line<P, T>(nxt, a.Qh[c + 1], (size_t)Lc, (size_t)nlines, t);
+    } else if (more) {
+      issue_line<P, T>(nxt, a.Qh[0], Lnc, (size_t)nlines, t);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
     double2 v[P];
 #pragma unroll
-    for (int s = 0; s < P; ++s) v[s] = __ldg(a.Qh[c] + (size_t)(t + T * s) * nlines + Lc);
+    for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
     F::template run<-1>(v, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) qi[c][s] = v[s].y;
+    ub ^= 1;
   }
   if (!valid) return;
   if constexpr (MODE == kConvOut) {
@@ -573,6 +772,43 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasFwdX) fwd_x_kernel(
       a.out[c][idx] = r;
     }
   }
+}
+
+template <int NX, int P, int MODE, bool COMBINE>
+__global__ void __launch_bounds__(kThreads, kMinCtasFwdX) fwd_x_kernel(FwdXArgs a, PassGeom g) {
+  using S = PassSmem<NX, P>;
+  using F = typename S::F;
+  using LM = typename S::LM;
+  constexpr int T = F::T;
+  extern __shared__ double2 dsm[];
+  F::load_tw(dsm + S::TW, a.tw);
+  const double2* tw_s = dsm + S::TW;
+  int li, t;
+  LM::get(li, t);
+  double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
+  double2* pf = dsm + S::PF + threadIdx.x;
+  const int nlines = g.Ny * g.Mz;
+  const int groups = (nlines + LM::LPC - 1) / LM::LPC;
+  const GroupRange gr = group_range(groups);
+  const int g_end = gr.end;
+  int grp = gr.grp;
+  if (grp >= g_end) return;
+  {
+    const int L0 = grp * LM::LPC + li;
+    issue_line<P, T>(pf, a.Qh[0], (size_t)(L0 < nlines ? L0 : 0), (size_t)nlines, t);
+    cp_async_commit();
+  }
+  int ub = 0;
+  for (; grp < g_end; grp += gr.step) {
+    const int L = grp * LM::LPC + li;
+    const bool valid = L < nlines;
+    const int Lc = valid ? L : 0;
+    const int gn = grp + gr.step;
+    const int Ln = gn * LM::LPC + li;
+    const size_t Lnc = (size_t)(Ln < nlines ? Ln : 0);
+    fwd_x_line<NX, P, MODE, COMBINE>(a, g, t, L, Lc, valid, sbuf, tw_s, pf, ub, gn < g_end, Lnc);
+  }
+  cp_async_wait<0>();
 }
 
 }  // namespace ns3d

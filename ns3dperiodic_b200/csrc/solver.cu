@@ -378,6 +378,8 @@ ns3d_status ns3d_create(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
       cudaMalloc(&h->diag_partial, sizeof(double) * 3 * kDiagBlocks) != cudaSuccess ||
       cudaMalloc(&h->diag_out, sizeof(double) * 3) != cudaSuccess)
     return bail(NS3D_ERR_OOM);
+  if ((e = ns3d::prepare_xy(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
+  if ((e = ns3d::prepare_fwdx(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   *out = h;
   return NS3D_OK;
