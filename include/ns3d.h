@@ -244,6 +244,114 @@ ns3d_status ns3d_convolution_noalloc(int Nx, int Ny, int Nz, double Lx, double L
                                      ns3d_complex* Qz, void* stream);
 
 /* ----------------------------------------------------------------------- */
+/* Krylov eigen-analysis: Arnoldi factorisation and implicit restart        */
+/* (Source/Arnoldi/Arnoldi_Driver.cu, Source/Arnoldi/QR_Shifts.cpp,          */
+/*  Source/Arnoldi/Implicit_restart_Arnoldi.cu:531-563)                      */
+/* ----------------------------------------------------------------------- */
+
+typedef struct ns3d_krylov ns3d_krylov;
+
+/* Matrix-vector map out = A in on device vectors of the workspace length n;
+ * the same type as the reference's user_map_vector
+ * (Source/Arnoldi/Matrix_Vector_emulator.h:11), so its NSCall* adapters can
+ * be passed unchanged.  The map must not write `in`, and its work must be
+ * complete when it returns (or be ordered before later work on the
+ * workspace stream: same stream, or a blocking stream while the workspace
+ * runs on the legacy default stream). */
+typedef void (*ns3d_user_map_vector)(void* user, void* in, void* out);
+
+/* Workspace for Krylov vectors of length n >= 2 and bases of up to
+ * 2 <= m_max <= 200 columns on the current device: the vectors v, w and the
+ * reduction buffers of Arnoldi_driver (its vec_v_d, vec_w_d, vec_c_d,
+ * vec_h_d arguments) plus pinned host staging.  Work runs on the legacy
+ * default stream until ns3d_krylov_set_stream. */
+ns3d_status ns3d_krylov_create(int64_t n, int m_max, ns3d_krylov** out);
+ns3d_status ns3d_krylov_destroy(ns3d_krylov* kr);
+ns3d_status ns3d_krylov_set_stream(ns3d_krylov* kr, void* stream);
+const char* ns3d_krylov_last_error(const ns3d_krylov* kr);
+
+/* Arnoldi_driver (Source/Arnoldi/Arnoldi_Driver.cu:29-120): extends
+ * A V = V H + f e_k^T to m columns (k = 0 starts from f).  V: DEVICE,
+ * n x m column-major (leading dimension n); H: HOST, m x m column-major
+ * (leading dimension m; columns k+1..m-1 are overwritten whole, H(k+1,k) and
+ * for k = 0 also H(0,0) are set); f: DEVICE, length n, the residual on entry
+ * and exit.  Classical Gram-Schmidt with iterative reorthogonalisation,
+ * tolerance 5e-12, at most 13 passes per column; a column that reaches the
+ * limit is counted (ns3d_krylov_stats) and the factorisation goes on, as in
+ * the reference.  Synchronous.  NS3D_ERR_BAD_ARG when k = 0 and
+ * ||f|| < 1e-15 (the reference exits), NS3D_ERR_NONFINITE when a norm, dot
+ * product or H entry is not finite (the reference checks element 0 of v, w
+ * and f for NaN and exits). */
+ns3d_status ns3d_arnoldi(ns3d_krylov* kr, ns3d_user_map_vector Axb, void* user, double* V,
+                         double* H, double* f, int k, int m);
+
+/* Largest number of reorthogonalisation passes a column of the last
+ * ns3d_arnoldi call took, and how many columns reached the pass limit. */
+ns3d_status ns3d_krylov_stats(const ns3d_krylov* kr, int* max_passes, int* limit_hits);
+
+/* HOST ONLY (no GPU needed).  QR_shifts (Source/Arnoldi/QR_Shifts.cpp:46-72):
+ * for j = m, m-1, ... while j > k, one shifted QR step of H with the shift
+ * eig[j-1] (a double step with (H - Re)^2 + Im^2 when |Im| > 1e-15, which
+ * also consumes eig[j-2]); Q (m x m, column-major, output) accumulates the
+ * orthogonal factors, H (m x m, column-major) becomes Q^T H Q with the
+ * entries below the subdiagonal zeroed, *ko = the final j.  The Q factors
+ * are Householder QR factors with LAPACK's conventions (dgeqrf + dormqr,
+ * Source/Arnoldi/LAPACK_routines.cpp:289-345).  eig_re/eig_im: the m Ritz
+ * values in the order the shifts are taken from (select_shifts). */
+ns3d_status ns3d_qr_shifts(int k, int m, double* Q, double* H, const double* eig_re,
+                           const double* eig_im, int* ko);
+
+/* Restart update (Source/Arnoldi/Implicit_restart_Arnoldi.cu:544-563) with
+ * q = Q(:,k0), hl = H(k0,k0-1), ql = Q(m-1,k0-1):  f = hl V q + ql f;
+ * Q(:, k0..m-1) := the identity columns (in the host array, as the
+ * reference does); V = V Q in place (columns k0.. keep their values).
+ * V, f: DEVICE; Q, H: HOST m x m column-major; 1 <= k0 < m.  *f_norm (may be
+ * null) receives ||f|| before the update (the Ritz-estimate scale, :547).
+ * One pass over V.  Synchronous. */
+ns3d_status ns3d_ira_restart(ns3d_krylov* kr, double* V, double* f, double* Q, const double* H,
+                             int k0, int m, double* f_norm);
+
+/* Built-in maps for ns3d_arnoldi.  Each finishes its work before returning
+ * and, on failure, records the first non-OK status in `status` and fills
+ * `out` with NaN so the driver stops with NS3D_ERR_NONFINITE. */
+typedef struct ns3d_map_context {
+  ns3d_solver* solver;
+  ns3d_complex* ux; /* base flow (advanced in place by the exponential map) */
+  ns3d_complex* uy;
+  ns3d_complex* uz;
+  ns3d_complex* vx; /* tangent fields, scratch of the exponential map */
+  ns3d_complex* vy;
+  ns3d_complex* vz;
+  double dt, Re, tau;
+  int steps;
+  int status; /* NS3D_OK until a call fails */
+} ns3d_map_context;
+
+/* user = ns3d_map_context*: out = J(u) in - in/tau (tau <= 0: no shift) on
+ * reduced vectors: NSCallMatrixVector_reduced[_Newton_Globalization]
+ * (Source/NS3D_periodic.cu:340-385) through ns3d_matvec_reduced. */
+void ns3d_map_linearised(void* user, void* in, void* out);
+
+/* user = ns3d_map_context*: in -> v (reduced unpacking), `steps` Heun tangent
+ * steps of (u, v) with ns3d_jvp_steps, v -> out: NSCallMatrixVector_exponential
+ * (Source/NS3D_periodic.cu:444-470).  As in the reference, the base flow u
+ * advances with every call.  The reference packs with the full-length
+ * kernels of a 3*Nc vector while its IRA call passes the reduced length
+ * 3*Nc-3 (Source/NS3D_periodic.cu:1717); this map uses the reduced packing
+ * consistently. */
+void ns3d_map_exponential(void* user, void* in, void* out);
+
+/* The reference's Krylov self-test operator (user_Ax_function,
+ * Source/Arnoldi/Matrix_Vector_emulator.cu:10-36): out_i = in_{i+1} - 2 in_i
+ * + in_{i-1} with periodic indices, then out_0 = 0. */
+typedef struct ns3d_laplace_context {
+  int64_t n;
+  void* stream; /* cudaStream_t, 0 = legacy default stream */
+  int status;
+} ns3d_laplace_context;
+void ns3d_map_laplace1d(void* user, void* in, void* out);
+
+/* ----------------------------------------------------------------------- */
 /* host-only helpers (no GPU needed)                                        */
 /* ----------------------------------------------------------------------- */
 

@@ -32,7 +32,27 @@ EXPORTS = (
     "ns3d_krylov_length", "ns3d_pack_reduced", "ns3d_unpack_reduced", "ns3d_matvec_reduced",
     "ns3d_diagnostics", "ns3d_profile_passes", "ns3d_mask_cutoff", "ns3d_twiddles",
     "ns3d_convolution_noalloc",
+    "ns3d_krylov_create", "ns3d_krylov_destroy", "ns3d_krylov_set_stream",
+    "ns3d_krylov_last_error", "ns3d_arnoldi", "ns3d_krylov_stats", "ns3d_qr_shifts",
+    "ns3d_ira_restart", "ns3d_map_linearised", "ns3d_map_exponential", "ns3d_map_laplace1d",
 )
+
+# the matrix-vector callback type of ns3d_arnoldi: void (*)(void*, void*, void*)
+MAP_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
+
+
+class MapContext(ctypes.Structure):
+    """ns3d_map_context of include/ns3d.h."""
+    _fields_ = [("solver", ctypes.c_void_p),
+                ("ux", ctypes.c_void_p), ("uy", ctypes.c_void_p), ("uz", ctypes.c_void_p),
+                ("vx", ctypes.c_void_p), ("vy", ctypes.c_void_p), ("vz", ctypes.c_void_p),
+                ("dt", ctypes.c_double), ("Re", ctypes.c_double), ("tau", ctypes.c_double),
+                ("steps", ctypes.c_int), ("status", ctypes.c_int)]
+
+
+class LaplaceContext(ctypes.Structure):
+    """ns3d_laplace_context of include/ns3d.h."""
+    _fields_ = [("n", ctypes.c_int64), ("stream", ctypes.c_void_p), ("status", ctypes.c_int)]
 
 
 class Ns3dLibraryError(RuntimeError):
@@ -88,6 +108,17 @@ def _sig(lib):
         "ns3d_twiddles": ([c_int, _P], c_int),
         "ns3d_convolution_noalloc": ([c_int, c_int, c_int, c_double, c_double, c_double]
                                      + [_P] * 6 + [_P], c_int),
+        "ns3d_krylov_create": ([c_int64, c_int, ctypes.POINTER(c_void_p)], c_int),
+        "ns3d_krylov_destroy": ([_P], c_int),
+        "ns3d_krylov_set_stream": ([_P, _P], c_int),
+        "ns3d_krylov_last_error": ([_P], ctypes.c_char_p),
+        "ns3d_arnoldi": ([_P, _P, _P, _P, _P, _P, c_int, c_int], c_int),
+        "ns3d_krylov_stats": ([_P, _P, _P], c_int),
+        "ns3d_qr_shifts": ([c_int, c_int, _P, _P, _P, _P, _P], c_int),
+        "ns3d_ira_restart": ([_P, _P, _P, _P, _P, c_int, c_int, _P], c_int),
+        "ns3d_map_linearised": ([_P, _P, _P], None),
+        "ns3d_map_exponential": ([_P, _P, _P], None),
+        "ns3d_map_laplace1d": ([_P, _P, _P], None),
     }
     for name, (args, res) in S.items():
         f = getattr(lib, name)

@@ -1,0 +1,535 @@
+// Krylov eigen-analysis on the device: the Arnoldi factorisation with
+// classical Gram-Schmidt and iterative reorthogonalisation, and the
+// implicit-restart update of the basis.
+//
+// Reference behaviour followed:
+//   Arnoldi_driver       Source/Arnoldi/Arnoldi_Driver.cu:29-120
+//   restart update       Source/Arnoldi/Implicit_restart_Arnoldi.cu:544-563
+//   built-in maps        Source/NS3D_periodic.cu:340-385,444-470 and the
+//                        Krylov self-test operator
+//                        Source/Arnoldi/Matrix_Vector_emulator.cu:10-36
+//
+// The reference issues one cuBLAS call per BLAS-1/2 operation and keeps H on
+// the host.  Here each Gram-Schmidt pass is two bandwidth-bound kernels over
+// the tall-skinny basis V (n x j+1, column-major, ld n):
+//   gemv_t_partial  per-block partial dot products of up to 8 columns per
+//                   sweep, the right-hand vector re-read from L2 per sweep;
+//   reduce_cols     one block folds the partials in a fixed order
+//                   (deterministic), updates h += c and ||c|| on the device;
+//   gemv_n_sub      y = y_in - V c with c staged in shared memory.
+// Only the scalars the host must branch on (||f||, ||c||) and the Hessenberg
+// column travel to the host, through one pinned buffer per pass.
+// The restart forms V Q (first k0 columns) and the new residual
+// f = hl V q + ql f in ONE pass over V: each row of V is staged in shared
+// memory once and every output column is produced from it, in place.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "ns3d.h"
+
+struct ns3d_krylov {
+  int64_t n = 0;
+  int m_max = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;  // nullptr = legacy default stream
+  double* v = nullptr;            // n: the normalised Krylov vector handed to the map
+  double* w = nullptr;            // n: the map's output
+  double* part = nullptr;         // m_max * kMaxBlocks partial sums
+  double* small = nullptr;        // [0] norm, [1] ||c||, [2..2+m) h, [2+m..2+2m) c
+  double* qcoef = nullptr;        // m_max * (m_max + 1): the Q columns used by a restart
+  double* host = nullptr;         // pinned: mirror of `small` + staging of qcoef
+  int max_passes = 0;
+  int limit_hits = 0;
+  std::string err;
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kColTile = 8;
+constexpr int kMaxBlocks = 148 * 4;
+constexpr int kRestartThreads = 128;
+constexpr int kMaxColumns = 200;        // restart row staging: m * 1 KB of shared memory
+constexpr double kReorthTol = 5.0e-12;  // Arnoldi_Driver.cu:31
+constexpr int kPassLimitIndex = 12;     // "if(it>12) break" after the pass
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// part[c * gridDim.x + b] = sum over the rows of block b of V[c*ldv + r] x[r]
+__global__ void __launch_bounds__(kThreads) gemv_t_partial(const double* __restrict__ V,
+                                                           int64_t ldv, int ncols,
+                                                           const double* __restrict__ x,
+                                                           int64_t n, double* __restrict__ part) {
+  __shared__ double red[kColTile][kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  for (int c0 = 0; c0 < ncols; c0 += kColTile) {
+    const int nc = min(kColTile, ncols - c0);
+    const double* Vc = V + (int64_t)c0 * ldv;
+    double acc[kColTile];
+#pragma unroll
+    for (int t = 0; t < kColTile; ++t) acc[t] = 0.0;
+    for (int64_t r = (int64_t)blockIdx.x * kThreads + threadIdx.x; r < n; r += stride) {
+      const double xr = __ldg(x + r);
+#pragma unroll
+      for (int t = 0; t < kColTile; ++t)
+        if (t < nc) acc[t] = fma(__ldg(Vc + (int64_t)t * ldv + r), xr, acc[t]);
+    }
+#pragma unroll
+    for (int t = 0; t < kColTile; ++t) {
+      double s = acc[t];
+#pragma unroll
+      for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) red[t][warp] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < nc) {
+      double s = 0.0;
+#pragma unroll
+      for (int w = 0; w < kThreads / 32; ++w) s += red[threadIdx.x][w];
+      part[(int64_t)(c0 + threadIdx.x) * gridDim.x + blockIdx.x] = s;
+    }
+    __syncthreads();
+  }
+}
+
+enum ReduceMode : int {
+  kNorm = 0,        // out[0] = sqrt(sum)             (ncols == 1)
+  kStore = 1,       // out[c] = sum
+  kAccumulate = 2,  // out[c] = sum, acc[c] += sum, nrm[0] = ||out||
+};
+
+// One block: column c folded by warp (c mod 8) over the nb partials, lanes
+// strided, then a fixed shuffle tree.
+__global__ void __launch_bounds__(kThreads) reduce_cols(const double* __restrict__ part, int nb,
+                                                        int ncols, int mode, double* out,
+                                                        double* acc, double* nrm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c = warp; c < ncols; c += kThreads / 32) {
+    double s = 0.0;
+    for (int b = lane; b < nb; b += 32) s += part[(int64_t)c * nb + b];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      if (mode == kNorm) {
+        out[0] = sqrt(s);
+      } else {
+        out[c] = s;
+        if (mode == kAccumulate) acc[c] += s;
+      }
+    }
+  }
+  if (mode == kAccumulate) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int c = 0; c < ncols; ++c) s = fma(out[c], out[c], s);
+      nrm[0] = sqrt(s);
+    }
+  }
+}
+
+// v = f / ||f|| and V(:, col) = v, with ||f|| read from the device.
+__global__ void __launch_bounds__(kThreads) scale_copy(const double* __restrict__ f,
+                                                       const double* __restrict__ norm,
+                                                       double* __restrict__ v,
+                                                       double* __restrict__ vcol, int64_t n) {
+  const double inv = 1.0 / norm[0];
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  for (int64_t r = (int64_t)blockIdx.x * kThreads + threadIdx.x; r < n; r += stride) {
+    const double x = f[r] * inv;
+    v[r] = x;
+    vcol[r] = x;
+  }
+}
+
+// y_out = y_in - V(:, 0..ncols) c
+__global__ void __launch_bounds__(kThreads) gemv_n_sub(const double* __restrict__ V, int64_t ldv,
+                                                       int ncols, const double* __restrict__ c,
+                                                       const double* y_in, double* y_out,
+                                                       int64_t n) {
+  extern __shared__ double sc[];
+  for (int i = threadIdx.x; i < ncols; i += kThreads) sc[i] = c[i];
+  __syncthreads();
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  for (int64_t r = (int64_t)blockIdx.x * kThreads + threadIdx.x; r < n; r += stride) {
+    double s = 0.0;
+    int i = 0;
+    for (; i + 4 <= ncols; i += 4) {
+      const double a0 = __ldg(V + (int64_t)i * ldv + r);
+      const double a1 = __ldg(V + (int64_t)(i + 1) * ldv + r);
+      const double a2 = __ldg(V + (int64_t)(i + 2) * ldv + r);
+      const double a3 = __ldg(V + (int64_t)(i + 3) * ldv + r);
+      s = fma(a0, sc[i], s);
+      s = fma(a1, sc[i + 1], s);
+      s = fma(a2, sc[i + 2], s);
+      s = fma(a3, sc[i + 3], s);
+    }
+    for (; i < ncols; ++i) s = fma(__ldg(V + (int64_t)i * ldv + r), sc[i], s);
+    y_out[r] = y_in[r] - s;
+  }
+}
+
+// In place, per row r of V (n x m, ld n):
+//   V(r, j) = sum_c V(r, c) Q(c, j)          for j < k0
+//   f(r)    = hl * sum_c V(r, c) Q(c, k0) + ql * f(r)
+// qc holds Q(:, 0..k0) column-major (ld m); every lane of a warp reads the
+// same coefficient, so those loads are L1 broadcasts.  Each thread stages
+// its own row in shared memory (column-strided, conflict-free) before any
+// output column is written, so no block barrier is needed.
+__global__ void __launch_bounds__(kRestartThreads) restart_rows(double* V, int64_t n, int m,
+                                                                int k0,
+                                                                const double* __restrict__ qc,
+                                                                double hl, double ql, double* f) {
+  extern __shared__ double row[];  // m * kRestartThreads
+  const int t = threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * kRestartThreads;
+  for (int64_t r = (int64_t)blockIdx.x * kRestartThreads + t; r < n; r += stride) {
+    for (int c = 0; c < m; ++c) row[c * kRestartThreads + t] = V[(int64_t)c * n + r];
+    for (int j = 0; j <= k0; ++j) {
+      const double* q = qc + (size_t)j * m;
+      double s = 0.0;
+      for (int c = 0; c < m; ++c) s = fma(row[c * kRestartThreads + t], __ldg(q + c), s);
+      if (j < k0)
+        V[(int64_t)j * n + r] = s;
+      else
+        f[r] = hl * s + ql * f[r];
+    }
+  }
+}
+
+// out_i = in_{i+1} - 2 in_i + in_{i-1} (periodic), out_0 = 0
+__global__ void __launch_bounds__(kThreads) laplace1d_kernel(const double* __restrict__ in,
+                                                             double* __restrict__ out, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+    if (i == 0) {
+      out[0] = 0.0;
+      continue;
+    }
+    const int64_t ip = (i + 1 == n) ? 0 : i + 1;
+    out[i] = in[ip] - 2.0 * in[i] + in[i - 1];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+
+ns3d_status kfail(ns3d_krylov* kr, ns3d_status s, const std::string& msg) {
+  if (kr) kr->err = msg;
+  return s;
+}
+
+ns3d_status kcuda(ns3d_krylov* kr, cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return NS3D_OK;
+  return kfail(kr, e == cudaErrorMemoryAllocation ? NS3D_ERR_OOM : NS3D_ERR_CUDA,
+               std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define KR_TRY(expr)                 \
+  do {                               \
+    ns3d_status s_ = (expr);         \
+    if (s_ != NS3D_OK) return s_;    \
+  } while (0)
+#define KR_CHECK(kr, expr, where) KR_TRY(kcuda(kr, (expr), where))
+
+int blocks_for(int64_t n, int threads, int cap) {
+  const int64_t b = (n + threads - 1) / threads;
+  return (int)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+
+ns3d_status enter(ns3d_krylov* kr) {
+  if (!kr) return NS3D_ERR_BAD_ARG;
+  KR_CHECK(kr, cudaSetDevice(kr->device), "cudaSetDevice");
+  kr->err.clear();
+  return NS3D_OK;
+}
+
+// dst[0..ncols) = V(:, 0..ncols)^T x, written by reduce_cols in `mode`.
+ns3d_status dots(ns3d_krylov* kr, const double* V, int ncols, const double* x, int mode,
+                 double* out, double* acc, double* nrm) {
+  const int nb = blocks_for(kr->n, kThreads, kMaxBlocks);
+  gemv_t_partial<<<nb, kThreads, 0, kr->stream>>>(V, kr->n, ncols, x, kr->n, kr->part);
+  KR_CHECK(kr, cudaGetLastError(), "gemv_t_partial");
+  reduce_cols<<<1, kThreads, 0, kr->stream>>>(kr->part, nb, ncols, mode, out, acc, nrm);
+  KR_CHECK(kr, cudaGetLastError(), "reduce_cols");
+  return NS3D_OK;
+}
+
+ns3d_status subtract(ns3d_krylov* kr, const double* V, int ncols, const double* c,
+                     const double* y_in, double* y_out) {
+  const int nb = blocks_for(kr->n, kThreads, kMaxBlocks * 2);
+  gemv_n_sub<<<nb, kThreads, sizeof(double) * ncols, kr->stream>>>(V, kr->n, ncols, c, y_in,
+                                                                   y_out, kr->n);
+  KR_CHECK(kr, cudaGetLastError(), "gemv_n_sub");
+  return NS3D_OK;
+}
+
+// ||f|| -> small[0]; v = V(:, col) = f / ||f||.
+ns3d_status normalise_into(ns3d_krylov* kr, double* f, double* vcol) {
+  KR_TRY(dots(kr, f, 1, f, kNorm, kr->small, nullptr, nullptr));
+  scale_copy<<<blocks_for(kr->n, kThreads, kMaxBlocks * 2), kThreads, 0, kr->stream>>>(
+      f, kr->small, kr->v, vcol, kr->n);
+  KR_CHECK(kr, cudaGetLastError(), "scale_copy");
+  return NS3D_OK;
+}
+
+ns3d_status fetch(ns3d_krylov* kr, int count) {
+  KR_CHECK(kr, cudaMemcpyAsync(kr->host, kr->small, sizeof(double) * count,
+                               cudaMemcpyDeviceToHost, kr->stream),
+           "scalar copy");
+  KR_CHECK(kr, cudaStreamSynchronize(kr->stream), "scalar sync");
+  return NS3D_OK;
+}
+
+ns3d_status call_map(ns3d_krylov* kr, ns3d_user_map_vector Axb, void* user) {
+  // the map may run on any stream: v must be complete before it starts
+  KR_CHECK(kr, cudaStreamSynchronize(kr->stream), "sync before map");
+  Axb(user, kr->v, kr->w);
+  KR_CHECK(kr, cudaGetLastError(), "matrix-vector map");
+  return NS3D_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+ns3d_status ns3d_krylov_create(int64_t n, int m_max, ns3d_krylov** out) {
+  if (!out) return NS3D_ERR_BAD_ARG;
+  *out = nullptr;
+  if (n < 2 || m_max < 2 || m_max > kMaxColumns) return NS3D_ERR_BAD_ARG;
+  ns3d_krylov* kr = new ns3d_krylov();
+  kr->n = n;
+  kr->m_max = m_max;
+  cudaGetDevice(&kr->device);
+  const size_t small = 2 + 2 * (size_t)m_max;
+  const size_t qc = (size_t)m_max * (m_max + 1);
+  cudaError_t e = cudaMalloc(&kr->v, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&kr->w, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&kr->part, sizeof(double) * (size_t)m_max * kMaxBlocks);
+  if (e == cudaSuccess) e = cudaMalloc(&kr->small, sizeof(double) * small);
+  if (e == cudaSuccess) e = cudaMalloc(&kr->qcoef, sizeof(double) * qc);
+  if (e == cudaSuccess) e = cudaMallocHost(&kr->host, sizeof(double) * (small + qc));
+  if (e == cudaSuccess) e = cudaMemset(kr->v, 0, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMemset(kr->w, 0, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMemset(kr->small, 0, sizeof(double) * small);
+  if (e == cudaSuccess) {
+    const size_t smem = sizeof(double) * (size_t)m_max * kRestartThreads;
+    e = cudaFuncSetAttribute(restart_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+  }
+  if (e != cudaSuccess) {
+    ns3d_krylov_destroy(kr);
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? NS3D_ERR_OOM : NS3D_ERR_CUDA;
+  }
+  *out = kr;
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_krylov_destroy(ns3d_krylov* kr) {
+  if (!kr) return NS3D_ERR_BAD_ARG;
+  cudaSetDevice(kr->device);
+  cudaStreamSynchronize(kr->stream);
+  cudaFree(kr->v);
+  cudaFree(kr->w);
+  cudaFree(kr->part);
+  cudaFree(kr->small);
+  cudaFree(kr->qcoef);
+  cudaFreeHost(kr->host);
+  delete kr;
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_krylov_set_stream(ns3d_krylov* kr, void* stream) {
+  KR_TRY(enter(kr));
+  kr->stream = (cudaStream_t)stream;
+  return NS3D_OK;
+}
+
+const char* ns3d_krylov_last_error(const ns3d_krylov* kr) {
+  return kr ? kr->err.c_str() : "null workspace";
+}
+
+ns3d_status ns3d_krylov_stats(const ns3d_krylov* kr, int* max_passes, int* limit_hits) {
+  if (!kr) return NS3D_ERR_BAD_ARG;
+  if (max_passes) *max_passes = kr->max_passes;
+  if (limit_hits) *limit_hits = kr->limit_hits;
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_arnoldi(ns3d_krylov* kr, ns3d_user_map_vector Axb, void* user, double* V,
+                         double* H, double* f, int k, int m) {
+  KR_TRY(enter(kr));
+  if (!Axb || !V || !H || !f) return kfail(kr, NS3D_ERR_BAD_ARG, "null pointer");
+  if (m < 2 || m > kr->m_max || k < 0 || k >= m)
+    return kfail(kr, NS3D_ERR_BAD_ARG, "need 0 <= k < m <= m_max and m >= 2");
+  kr->max_passes = 0;
+  kr->limit_hits = 0;
+  const int64_t n = kr->n;
+  double* hd = kr->small + 2;      // h on the device
+  double* cd = kr->small + 2 + m;  // c on the device (k == 0 uses cd[0] as the scalar)
+  const double* hh = kr->host + 2;
+
+  if (k == 0) {
+    KR_TRY(normalise_into(kr, f, V));
+    KR_TRY(fetch(kr, 1));
+    const double beta = kr->host[0];
+    if (!std::isfinite(beta)) return kfail(kr, NS3D_ERR_NONFINITE, "||f|| is not finite");
+    if (beta < 1.0e-15)
+      return kfail(kr, NS3D_ERR_BAD_ARG, "norm of the input vector ||f|| < 1e-15");
+    KR_TRY(call_map(kr, Axb, user));
+    KR_TRY(dots(kr, kr->v, 1, kr->w, kStore, cd, nullptr, nullptr));
+    KR_TRY(subtract(kr, kr->v, 1, cd, kr->w, f));
+    KR_CHECK(kr, cudaMemcpyAsync(kr->host, cd, sizeof(double), cudaMemcpyDeviceToHost,
+                                 kr->stream), "alpha copy");
+    KR_CHECK(kr, cudaStreamSynchronize(kr->stream), "alpha sync");
+    double alpha = kr->host[0];
+    double c = 1.0;
+    int it = 0;
+    while (c > kReorthTol) {  // signed, as the reference tests it
+      ++it;
+      KR_TRY(dots(kr, kr->v, 1, f, kStore, cd, nullptr, nullptr));
+      KR_TRY(subtract(kr, kr->v, 1, cd, f, f));
+      KR_CHECK(kr, cudaMemcpyAsync(kr->host, cd, sizeof(double), cudaMemcpyDeviceToHost,
+                                   kr->stream), "c copy");
+      KR_CHECK(kr, cudaStreamSynchronize(kr->stream), "c sync");
+      c = kr->host[0];
+      alpha += c;
+      if (!std::isfinite(c)) return kfail(kr, NS3D_ERR_NONFINITE, "reorthogonalisation");
+      if (it > kPassLimitIndex) {
+        ++kr->limit_hits;
+        break;
+      }
+    }
+    if (it > kr->max_passes) kr->max_passes = it;
+    if (!std::isfinite(alpha)) return kfail(kr, NS3D_ERR_NONFINITE, "H(0,0) is not finite");
+    H[0] = alpha;
+  }
+
+  for (int j = k + 1; j < m; ++j) {
+    KR_TRY(normalise_into(kr, f, V + (int64_t)j * n));
+    KR_TRY(fetch(kr, 1));
+    const double beta = kr->host[0];
+    if (!std::isfinite(beta)) return kfail(kr, NS3D_ERR_NONFINITE, "||f|| is not finite");
+    H[j + (int64_t)(j - 1) * m] = beta;
+    KR_TRY(call_map(kr, Axb, user));
+    KR_CHECK(kr, cudaMemsetAsync(hd, 0, sizeof(double) * 2 * m, kr->stream), "h reset");
+    KR_TRY(dots(kr, V, j + 1, kr->w, kStore, hd, nullptr, nullptr));
+    KR_TRY(subtract(kr, V, j + 1, hd, kr->w, f));
+    double cn = 1.0;
+    int it = 0;
+    while (cn > kReorthTol) {
+      ++it;
+      KR_TRY(dots(kr, V, j + 1, f, kAccumulate, cd, hd, kr->small + 1));
+      KR_TRY(subtract(kr, V, j + 1, cd, f, f));
+      KR_TRY(fetch(kr, 2 + m));
+      cn = kr->host[1];
+      if (!std::isfinite(cn)) return kfail(kr, NS3D_ERR_NONFINITE, "reorthogonalisation");
+      if (it > kPassLimitIndex) {
+        ++kr->limit_hits;
+        break;
+      }
+    }
+    if (it > kr->max_passes) kr->max_passes = it;
+    for (int i = 0; i < m; ++i) {
+      const double x = i <= j ? hh[i] : 0.0;
+      if (!std::isfinite(x)) return kfail(kr, NS3D_ERR_NONFINITE, "H column is not finite");
+      H[i + (int64_t)j * m] = x;
+    }
+  }
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_ira_restart(ns3d_krylov* kr, double* V, double* f, double* Q, const double* H,
+                             int k0, int m, double* f_norm) {
+  KR_TRY(enter(kr));
+  if (!V || !f || !Q || !H) return kfail(kr, NS3D_ERR_BAD_ARG, "null pointer");
+  if (m < 2 || m > kr->m_max || k0 < 1 || k0 >= m)
+    return kfail(kr, NS3D_ERR_BAD_ARG, "need 1 <= k0 < m <= m_max");
+  const double hl = H[k0 + (int64_t)(k0 - 1) * m];
+  const double ql = Q[(m - 1) + (int64_t)(k0 - 1) * m];
+  const size_t small = 2 + 2 * (size_t)kr->m_max;
+  double* staged = kr->host + small;
+  const size_t nq = (size_t)m * (k0 + 1);
+  std::memcpy(staged, Q, sizeof(double) * nq);  // Q(:, 0..k0), column-major
+  KR_CHECK(kr, cudaMemcpyAsync(kr->qcoef, staged, sizeof(double) * nq, cudaMemcpyHostToDevice,
+                               kr->stream), "Q upload");
+  KR_TRY(dots(kr, f, 1, f, kNorm, kr->small, nullptr, nullptr));
+  const size_t smem = sizeof(double) * (size_t)m * kRestartThreads;
+  restart_rows<<<blocks_for(kr->n, kRestartThreads, 148 * 8), kRestartThreads, smem,
+                 kr->stream>>>(V, kr->n, m, k0, kr->qcoef, hl, ql, f);
+  KR_CHECK(kr, cudaGetLastError(), "restart_rows");
+  KR_TRY(fetch(kr, 1));
+  if (f_norm) *f_norm = kr->host[0];
+  for (int j = k0; j < m; ++j)
+    for (int i = 0; i < m; ++i) Q[i + (int64_t)j * m] = (i == j) ? 1.0 : 0.0;
+  if (!std::isfinite(kr->host[0])) return kfail(kr, NS3D_ERR_NONFINITE, "||f|| is not finite");
+  return NS3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// built-in matrix-vector maps
+// ---------------------------------------------------------------------------
+
+static void map_poison(ns3d_map_context* c, double* out) {
+  const int64_t n = ns3d_krylov_length(c->solver);
+  if (n > 0 && out) cudaMemset(out, 0xff, sizeof(double) * n);  // NaN: the driver stops
+}
+
+void ns3d_map_linearised(void* user, void* in, void* out) {
+  ns3d_map_context* c = static_cast<ns3d_map_context*>(user);
+  if (!c) return;
+  ns3d_status s = ns3d_matvec_reduced(c->solver, c->ux, c->uy, c->uz,
+                                      static_cast<const double*>(in), static_cast<double*>(out),
+                                      c->Re, c->tau);
+  if (s == NS3D_OK) s = ns3d_synchronize(c->solver);
+  if (s != NS3D_OK) {
+    if (c->status == NS3D_OK) c->status = s;
+    map_poison(c, static_cast<double*>(out));
+  }
+}
+
+void ns3d_map_exponential(void* user, void* in, void* out) {
+  ns3d_map_context* c = static_cast<ns3d_map_context*>(user);
+  if (!c) return;
+  ns3d_status s = ns3d_unpack_reduced(c->solver, static_cast<const double*>(in), c->vx, c->vy,
+                                      c->vz);
+  if (s == NS3D_OK)
+    s = ns3d_jvp_steps(c->solver, c->ux, c->uy, c->uz, c->vx, c->vy, c->vz, c->dt, c->Re,
+                       c->steps);
+  if (s == NS3D_OK)
+    s = ns3d_pack_reduced(c->solver, c->vx, c->vy, c->vz, static_cast<double*>(out));
+  if (s == NS3D_OK) s = ns3d_synchronize(c->solver);
+  if (s != NS3D_OK) {
+    if (c->status == NS3D_OK) c->status = s;
+    map_poison(c, static_cast<double*>(out));
+  }
+}
+
+void ns3d_map_laplace1d(void* user, void* in, void* out) {
+  ns3d_laplace_context* c = static_cast<ns3d_laplace_context*>(user);
+  if (!c) return;
+  if (c->n < 2 || !in || !out) {
+    if (c->status == NS3D_OK) c->status = NS3D_ERR_BAD_ARG;
+    return;
+  }
+  cudaStream_t st = (cudaStream_t)c->stream;
+  laplace1d_kernel<<<blocks_for(c->n, kThreads, kMaxBlocks * 2), kThreads, 0, st>>>(
+      static_cast<const double*>(in), static_cast<double*>(out), c->n);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess && c->status == NS3D_OK) c->status = NS3D_ERR_CUDA;
+}
+
+}  // extern "C"

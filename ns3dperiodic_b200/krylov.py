@@ -1,0 +1,258 @@
+"""Python host mirror of the reference's Krylov eigen-analysis.
+
+Follows Source/Arnoldi: ``Arnoldi_driver`` (Arnoldi_Driver.cu:29),
+``select_shifts`` (Select_Shifts.cpp:86), ``QR_shifts`` (QR_Shifts.cpp:46)
+and the restart loop of ``Implicit_restart_Arnoldi_GPU_data``
+(Implicit_restart_Arnoldi.cu:444-581).  The Gram-Schmidt passes and the
+restart run as sm_100a kernels behind the C ABI (include/ns3d.h); the small
+m x m Hessenberg work stays on the host, as in the reference.
+
+Storage follows the reference: the basis V is n x m column-major on the
+device, held here as a contiguous float64 CUDA tensor of shape (m, n) (row j
+is Krylov vector j, which is the same memory); H and Q are numpy (m, m)
+matrices indexed [row, col].
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import LaplaceContext, MAP_FN, MapContext, Ns3dError, lib
+
+IM_EIG_TOL = 1.0e-15  # Source/Arnoldi/Macros.h:10
+
+
+class _DeviceVector:
+    """__cuda_array_interface__ view of a raw device pointer (no ownership)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8",
+                                         "data": (int(ptr), False), "version": 3,
+                                         "strides": None}
+
+
+class Map:
+    """A matrix-vector map for :meth:`Krylov.arnoldi`: a C function pointer
+    plus the context object it receives (kept alive here)."""
+
+    def __init__(self, fn, ctx, keep=()):
+        self.fn = fn
+        self.ctx = ctx
+        self._keep = keep
+
+    @property
+    def status(self) -> int:
+        return int(self.ctx.status)
+
+    def ctx_ptr(self) -> int:
+        return ctypes.addressof(self.ctx)
+
+
+def select_shifts(H: np.ndarray, which: str = "LR"):
+    """select_shifts (Select_Shifts.cpp:86-133): eigenvalues of H sorted by
+    ``which`` ("LR" largest real part first, "LM" largest modulus first) and
+    the Ritz estimates |last component| of the unit eigenvectors (zgeev)."""
+    m = H.shape[0]
+    w, vecs = np.linalg.eig(np.asarray(H, dtype=np.complex128))
+    if which == "LR":
+        key = -w.real
+    elif which == "LM":
+        key = -np.abs(w)
+    else:
+        raise ValueError("which must be 'LR' or 'LM'")
+    order = np.argsort(key, kind="stable")
+    return w[order], np.abs(vecs[m - 1, order])
+
+
+def qr_shifts(k: int, H: np.ndarray, eigs):
+    """QR_shifts through ns3d_qr_shifts (host code of the library).
+    Returns (Q, H_new, ko)."""
+    m = H.shape[0]
+    L = lib()
+    Q = np.zeros((m, m), order="F")
+    Hf = np.asfortranarray(np.array(H, dtype=np.float64))
+    e = np.asarray(eigs, dtype=np.complex128)
+    er = np.ascontiguousarray(e.real)
+    ei = np.ascontiguousarray(e.imag)
+    ko = ctypes.c_int(0)
+    rc = L.ns3d_qr_shifts(int(k), m, Q.ctypes.data, Hf.ctypes.data, er.ctypes.data,
+                          ei.ctypes.data, ctypes.byref(ko))
+    if rc != 0:
+        raise Ns3dError(rc, "ns3d_qr_shifts")
+    return np.ascontiguousarray(Q), np.ascontiguousarray(Hf), int(ko.value)
+
+
+class Krylov:
+    """One ns3d_krylov workspace: vectors of length n, bases of up to m_max
+    columns, on one CUDA device."""
+
+    def __init__(self, n: int, m_max: int, device=None):
+        import torch
+
+        self._torch = torch
+        dev = torch.device(device if device is not None else "cuda")
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        self.n, self.m_max = int(n), int(m_max)
+        self._L = lib()
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            torch.cuda.init()
+            rc = self._L.ns3d_krylov_create(self.n, self.m_max, ctypes.byref(h))
+        if rc != 0:
+            raise Ns3dError(rc, "ns3d_krylov_create")
+        self._h = h
+        self._stream = None
+        self._views = {}
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, rc: int, where: str):
+        if rc != 0:
+            d = self._L.ns3d_krylov_last_error(self._h)
+            raise Ns3dError(rc, where, d.decode() if d else "")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.ns3d_krylov_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream=None):
+        """Run on a torch.cuda.Stream (None: the legacy default stream)."""
+        self._stream = stream
+        self._check(self._L.ns3d_krylov_set_stream(
+            self._h, ctypes.c_void_p(stream.cuda_stream if stream is not None else 0)),
+            "ns3d_krylov_set_stream")
+
+    def _view(self, ptr: int):
+        t = self._views.get(ptr)
+        if t is None:
+            t = self._torch.as_tensor(_DeviceVector(ptr, self.n), device=self.device)
+            self._views[ptr] = t
+        return t
+
+    def python_map(self, fn) -> Map:
+        """Wraps ``fn(x, y)`` (y = A x on float64 CUDA tensors of length n)."""
+        torch = self._torch
+
+        def tramp(_user, pin, pout):
+            x, y = self._view(pin), self._view(pout)
+            if self._stream is not None:
+                with torch.cuda.stream(self._stream):
+                    fn(x, y)
+                self._stream.synchronize()
+            else:
+                fn(x, y)
+                torch.cuda.current_stream(self.device).synchronize()
+
+        cfn = MAP_FN(tramp)
+        ctx = LaplaceContext()  # unused placeholder so every Map has a context
+        return Map(cfn, ctx, keep=(tramp,))
+
+    def laplace_map(self) -> Map:
+        """The reference's Krylov self-test operator (ns3d_map_laplace1d)."""
+        ctx = LaplaceContext(self.n, ctypes.c_void_p(
+            self._stream.cuda_stream if self._stream is not None else 0), 0)
+        return Map(ctypes.cast(self._L.ns3d_map_laplace1d, ctypes.c_void_p).value, ctx)
+
+    def linearised_map(self, solver, U, Re: float, tau: float = 0.0) -> Map:
+        """J(u) (minus 1/tau) on reduced vectors (ns3d_map_linearised)."""
+        p = solver._fields(U, "U")
+        ctx = MapContext(solver._h.value, p[0], p[1], p[2], 0, 0, 0, 0.0, float(Re),
+                         float(tau), 0, 0)
+        return Map(ctypes.cast(self._L.ns3d_map_linearised, ctypes.c_void_p).value, ctx,
+                   keep=(U,))
+
+    def exponential_map(self, solver, U, Vscratch, dt: float, Re: float, steps: int) -> Map:
+        """``steps`` Heun tangent steps per call (ns3d_map_exponential); U
+        advances with every call, as in the reference."""
+        p = solver._fields(U, "U")
+        q = solver._fields(Vscratch, "V")
+        ctx = MapContext(solver._h.value, p[0], p[1], p[2], q[0], q[1], q[2], float(dt),
+                         float(Re), 0.0, int(steps), 0)
+        return Map(ctypes.cast(self._L.ns3d_map_exponential, ctypes.c_void_p).value, ctx,
+                   keep=(U, Vscratch))
+
+    def _basis(self, V, m: int):
+        torch = self._torch
+        if (not isinstance(V, torch.Tensor) or V.dtype != torch.float64
+                or V.device != self.device or V.dim() != 2 or V.shape[1] != self.n
+                or V.shape[0] < m or not V.is_contiguous()):
+            raise ValueError(f"V: expected a contiguous float64 ({m}, {self.n}) tensor on "
+                             f"{self.device}")
+
+    def _vector(self, f):
+        torch = self._torch
+        if (not isinstance(f, torch.Tensor) or f.dtype != torch.float64
+                or f.device != self.device or f.numel() != self.n or not f.is_contiguous()):
+            raise ValueError(f"f: expected a contiguous float64 vector of length {self.n}")
+
+    # -- reference entry points ---------------------------------------------
+    def arnoldi(self, A: Map, V, H: np.ndarray, f, k: int, m: int) -> dict:
+        """Arnoldi_driver: extends the factorisation in place (V, f on the
+        device, H host (m, m))."""
+        self._basis(V, m)
+        self._vector(f)
+        Hf = np.asfortranarray(H[:m, :m], dtype=np.float64)
+        fn = A.fn if isinstance(A.fn, int) else ctypes.cast(A.fn, ctypes.c_void_p).value
+        rc = self._L.ns3d_arnoldi(self._h, ctypes.c_void_p(fn), ctypes.c_void_p(A.ctx_ptr()),
+                                  ctypes.c_void_p(V.data_ptr()), Hf.ctypes.data,
+                                  ctypes.c_void_p(f.data_ptr()), int(k), int(m))
+        H[:m, :m] = Hf
+        self._check(rc, "ns3d_arnoldi")
+        mp, lh = ctypes.c_int(0), ctypes.c_int(0)
+        self._L.ns3d_krylov_stats(self._h, ctypes.byref(mp), ctypes.byref(lh))
+        return {"max_passes": mp.value, "limit_hits": lh.value}
+
+    def ira_restart(self, V, f, Q: np.ndarray, H: np.ndarray, k0: int) -> float:
+        """Restart update f = hl V q + ql f, V = V Q; Q's columns k0.. are
+        reset to the identity in place.  Returns ||f|| before the update."""
+        m = Q.shape[0]
+        self._basis(V, m)
+        self._vector(f)
+        Qf = np.asfortranarray(Q, dtype=np.float64)
+        Hf = np.asfortranarray(H, dtype=np.float64)
+        fn = ctypes.c_double(0.0)
+        rc = self._L.ns3d_ira_restart(self._h, ctypes.c_void_p(V.data_ptr()),
+                                      ctypes.c_void_p(f.data_ptr()), Qf.ctypes.data,
+                                      Hf.ctypes.data, int(k0), m, ctypes.byref(fn))
+        Q[:, :] = Qf
+        self._check(rc, "ns3d_ira_restart")
+        return fn.value
+
+    def implicit_restart_arnoldi(self, A: Map, which: str = "LR", k: int = 6, m: int = 30,
+                                 tol: float = 5.0e-8, max_iter: int = 3000, seed: int = 0,
+                                 f0=None):
+        """The restart loop of Implicit_restart_Arnoldi_GPU_data
+        (Implicit_restart_Arnoldi.cu:531-581).  Returns (eigenvalues of H in
+        'which' order, Ritz-norm, iterations, V, H).  The start vector is
+        N(0, 2) from a seeded generator (the reference seeds from the clock)."""
+        torch = self._torch
+        if f0 is None:
+            g = torch.Generator(device="cpu").manual_seed(int(seed))
+            f = (torch.randn(self.n, generator=g, dtype=torch.float64) * 2.0).to(self.device)
+        else:
+            f = f0.clone()
+        V = torch.zeros((m, self.n), dtype=torch.float64, device=self.device)
+        H = np.zeros((m, m))
+        k0, it, ritz_norm = 1, 0, 1.0
+        eig = np.zeros(m, dtype=np.complex128)
+        while it < max_iter and ritz_norm > tol:
+            it += 1
+            self.arnoldi(A, V, H, f, k0 - 1, m)
+            eig, ritz = select_shifts(H, which)
+            Q, H, k0 = qr_shifts(k, H, eig)
+            if k0 < 1:
+                raise Ns3dError(1, "implicit_restart_arnoldi", "no wanted Ritz value kept")
+            fnorm = self.ira_restart(V, f, Q, H, k0)
+            ritz[:k0] *= fnorm
+            # vector_normC: max of fabsf (single precision), Products.cpp:23-31
+            ritz_norm = float(np.max(np.abs(ritz[:k0]).astype(np.float32)))
+        return eig, ritz_norm, it, V, H

@@ -1,0 +1,195 @@
+// Harness around the reference's own Krylov code (TEST INFRASTRUCTURE).
+//
+// oracle/Makefile compiles the reference's Source/Arnoldi/{Arnoldi_Driver.cu,
+// cuda_supp.cu, memory_operations.cu, Matrix_Vector_emulator.cu,
+// Products.cpp, QR_Shifts.cpp, Select_Shifts.cpp, LAPACK_routines.cpp}
+// unmodified (with oracle/c99_complex_prelude.h force-included) together with
+// this file into oracle/_ref/libarnoldi_ref.so.  This file adds only:
+//   * flat C entry points for ctypes (host arrays in, host arrays out);
+//   * the matrix-vector callbacks handed to Arnoldi_driver: the reference's
+//     own 1-D periodic Laplacian (user_Ax_function,
+//     Source/Arnoldi/Matrix_Vector_emulator.cu:27-36) and a dense matrix
+//     applied with cublasDgemv;
+//   * forwarding of the Fortran LAPACK names the reference calls (dgeqrf_,
+//     dormqr_, zgeev_, dhseqr_) to the LP64 OpenBLAS that scipy ships
+//     (exported there with a "scipy_" prefix); the image has no other LAPACK.
+// Arnoldi_driver needs a GPU; the QR-shift and shift-selection entry points
+// are host code and run anywhere the library loads.
+#include "Arnoldi_Driver.h"
+#include "QR_Shifts.h"
+#include "Select_Shifts.h"
+#include "Matrix_Vector_emulator.h"
+
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <vector>
+
+extern "C" {
+void scipy_dgeqrf_(int*, int*, double*, int*, double*, double*, int*, int*);
+void scipy_dormqr_(char*, char*, int*, int*, int*, double*, int*, double*, double*, int*,
+                   double*, int*, int*);
+void scipy_zgeev_(char*, char*, int*, double _Complex*, int*, double _Complex*,
+                  double _Complex*, int*, double _Complex*, int*, double _Complex*, int*,
+                  double _Complex*, int*);
+void scipy_dhseqr_(char*, char*, int*, int*, int*, double*, int*, double*, double*, double*,
+                   int*, double*, int*, int*);
+
+void dgeqrf_(int* M, int* N, double* A, int* LDA, double* TAU, double* WORK, int* LWORK,
+             int* INFO)
+{
+    scipy_dgeqrf_(M, N, A, LDA, TAU, WORK, LWORK, INFO);
+}
+void dormqr_(char* SIDE, char* TRANS, int* M, int* N, int* K, double* A, int* LDA, double* TAU,
+             double* C, int* LDC, double* WORK, int* LWORK, int* INFO)
+{
+    scipy_dormqr_(SIDE, TRANS, M, N, K, A, LDA, TAU, C, LDC, WORK, LWORK, INFO);
+}
+void zgeev_(char* jobvl, char* jobvr, int* n, double _Complex* a, int* lda, double _Complex* w,
+            double _Complex* vl, int* ldvl, double _Complex* vr, int* ldvr,
+            double _Complex* work, int* lwork, double _Complex* rwork, int* info)
+{
+    scipy_zgeev_(jobvl, jobvr, n, a, lda, w, vl, ldvl, vr, ldvr, work, lwork, rwork, info);
+}
+void dhseqr_(char* JOB, char* COMPZ, int* N, int* ILO, int* IHI, double* H, int* LDH, double* WR,
+             double* WI, double* Z, int* LDZ, double* WORK, int* LWORK, int* INFO)
+{
+    scipy_dhseqr_(JOB, COMPZ, N, ILO, IHI, H, LDH, WR, WI, Z, LDZ, WORK, LWORK, INFO);
+}
+}
+
+namespace {
+
+struct DenseMap {
+    cublasHandle_t handle;
+    int n;
+    double* A;  // column-major n x n on the device
+};
+
+void dense_map(void* ctx, void* in, void* out)
+{
+    DenseMap* d = static_cast<DenseMap*>(ctx);
+    const double one = 1.0, zero = 0.0;
+    cublasDgemv(d->handle, CUBLAS_OP_N, d->n, d->n, &one, d->A, d->n,
+                static_cast<double*>(in), 1, &zero, static_cast<double*>(out), 1);
+}
+
+void laplace_map(void* ctx, void* in, void* out)
+{
+    user_Ax_function(static_cast<Ax_struct*>(ctx), static_cast<real*>(in),
+                     static_cast<real*>(out));
+}
+
+// Runs Arnoldi_driver on host copies of V (n x m), H (m x m) and f (n).
+int run_arnoldi(int n, int m, int k, user_map_vector Axb, void* ctx, cublasHandle_t handle,
+                double* V, double* H, double* f)
+{
+    double *V_d = nullptr, *f_d = nullptr, *v_d = nullptr, *w_d = nullptr, *c_d = nullptr,
+           *h_d = nullptr;
+    const size_t nb = sizeof(double) * static_cast<size_t>(n);
+    if (cudaMalloc(&V_d, nb * m) != cudaSuccess) return 1;
+    cudaMalloc(&f_d, nb);
+    cudaMalloc(&v_d, nb);
+    cudaMalloc(&w_d, nb);
+    cudaMalloc(&c_d, sizeof(double) * m);
+    cudaMalloc(&h_d, sizeof(double) * m);
+    cudaMemcpy(V_d, V, nb * m, cudaMemcpyHostToDevice);
+    cudaMemcpy(f_d, f, nb, cudaMemcpyHostToDevice);
+    cudaMemset(v_d, 0, nb);
+    cudaMemset(w_d, 0, nb);
+    std::vector<double> vec_h(m, 0.0);
+    Arnoldi_driver(handle, n, Axb, ctx, V_d, H, f_d, k, m, v_d, w_d, c_d, h_d, vec_h.data());
+    cudaMemcpy(V, V_d, nb * m, cudaMemcpyDeviceToHost);
+    cudaMemcpy(f, f_d, nb, cudaMemcpyDeviceToHost);
+    const cudaError_t err = cudaDeviceSynchronize();
+    cudaFree(V_d);
+    cudaFree(f_d);
+    cudaFree(v_d);
+    cudaFree(w_d);
+    cudaFree(c_d);
+    cudaFree(h_d);
+    return err == cudaSuccess ? 0 : 2;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Arnoldi_driver (Source/Arnoldi/Arnoldi_Driver.cu:29) with the reference's
+// 1-D periodic Laplacian test operator.
+int ref_arnoldi_laplace(int n, int m, int k, double* V, double* H, double* f)
+{
+    cublasHandle_t handle;
+    if (cublasCreate(&handle) != CUBLAS_STATUS_SUCCESS) return 3;
+    Ax_struct ctx;
+    ctx.N = n;
+    const int rc = run_arnoldi(n, m, k, laplace_map, &ctx, handle, V, H, f);
+    cublasDestroy(handle);
+    return rc;
+}
+
+// Arnoldi_driver with a dense column-major n x n matrix A.
+int ref_arnoldi_dense(int n, int m, int k, const double* A, double* V, double* H, double* f)
+{
+    cublasHandle_t handle;
+    if (cublasCreate(&handle) != CUBLAS_STATUS_SUCCESS) return 3;
+    DenseMap ctx;
+    ctx.handle = handle;
+    ctx.n = n;
+    if (cudaMalloc(&ctx.A, sizeof(double) * n * static_cast<size_t>(n)) != cudaSuccess) {
+        cublasDestroy(handle);
+        return 1;
+    }
+    cudaMemcpy(ctx.A, A, sizeof(double) * n * static_cast<size_t>(n), cudaMemcpyHostToDevice);
+    const int rc = run_arnoldi(n, m, k, dense_map, &ctx, handle, V, H, f);
+    cudaFree(ctx.A);
+    cublasDestroy(handle);
+    return rc;
+}
+
+// The reference's 1-D periodic Laplacian applied once (for checking the
+// project's copy of the test operator).
+int ref_laplace_apply(int n, const double* in, double* out)
+{
+    double *a = nullptr, *b = nullptr;
+    if (cudaMalloc(&a, sizeof(double) * n) != cudaSuccess) return 1;
+    cudaMalloc(&b, sizeof(double) * n);
+    cudaMemcpy(a, in, sizeof(double) * n, cudaMemcpyHostToDevice);
+    cudaMemset(b, 0, sizeof(double) * n);
+    Ax_struct ctx;
+    ctx.N = n;
+    laplace_map(&ctx, a, b);
+    cudaMemcpy(out, b, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    const cudaError_t err = cudaDeviceSynchronize();
+    cudaFree(a);
+    cudaFree(b);
+    return err == cudaSuccess ? 0 : 2;
+}
+
+// QR_shifts (Source/Arnoldi/QR_Shifts.cpp:46-72); host only.  Q (m x m) is
+// output, H (m x m) is updated in place, eigenvalues are given as separate
+// real and imaginary arrays of length m.
+void ref_qr_shifts(int k, int m, double* Q, double* H, const double* eig_re,
+                   const double* eig_im, int* ko)
+{
+    std::vector<double _Complex> eig(m);
+    for (int i = 0; i < m; ++i) {
+        __real__ eig[i] = eig_re[i];
+        __imag__ eig[i] = eig_im[i];
+    }
+    QR_shifts(k, m, Q, H, eig.data(), ko);
+}
+
+// select_shifts (Source/Arnoldi/Select_Shifts.cpp:86-133); host only.
+void ref_select_shifts(int m, double* H, const char* which, double* eig_re, double* eig_im,
+                       double* ritz)
+{
+    std::vector<double _Complex> vecs(static_cast<size_t>(m) * m), eig(m);
+    char w[2] = {which[0], which[1]};
+    select_shifts(m, H, w, vecs.data(), eig.data(), ritz);
+    for (int i = 0; i < m; ++i) {
+        eig_re[i] = __real__ eig[i];
+        eig_im[i] = __imag__ eig[i];
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,196 @@
+"""CPU oracle for the Krylov (Arnoldi / implicit-restart) path (TEST INFRASTRUCTURE).
+
+This module is the checker, not the product.  Only ``tests/``,
+``__graft_entry__.smoke()`` and the reference legs of ``bench.py`` may import
+it.  It restates in numpy FP64, step by step, the reference's
+
+* Arnoldi factorisation with classical Gram-Schmidt and iterative
+  reorthogonalisation (Source/Arnoldi/Arnoldi_Driver.cu:29-120; tolerance
+  5e-12 at :31, at most 13 passes at :60-72 and :97-115);
+* implicit shifted QR on the Hessenberg matrix (Source/Arnoldi/QR_Shifts.cpp:
+  7-72) with the Q factor of LAPACK's Householder QR (``dgeqrf`` + ``dormqr``,
+  Source/Arnoldi/LAPACK_routines.cpp:289-345; numpy's ``qr`` is the same
+  ``dgeqrf`` factorisation);
+* shift selection (Source/Arnoldi/Select_Shifts.cpp:86-133);
+* the restart update ``f = hl V q + ql f``, ``V = V Q`` with the trailing
+  columns of Q reset to the identity
+  (Source/Arnoldi/Implicit_restart_Arnoldi.cu:544-563);
+* the 1-D periodic Laplacian test operator of the reference's Krylov
+  self-test (Source/Arnoldi/Matrix_Vector_emulator.cu:10-36).
+
+Layout follows the reference: ``V`` is n x m column-major (numpy arrays of
+shape (m, n) here, row j = column j of V, which is the same memory), ``H``
+is m x m column-major (numpy shape (m, m) indexed ``H[col, row]``; the
+helpers take and return it as a normal row/column matrix ``Hm[row, col]``).
+
+Parity status: pinned against the reference's own Krylov code built by
+oracle/Makefile into oracle/_ref/libarnoldi_ref.so (Arnoldi_driver on a B200;
+QR_shifts and select_shifts on the host with LAPACK from scipy's OpenBLAS),
+through tests/golden/make_golden_krylov.py and tests/test_krylov_oracle.py.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+ARNOLDI_TOL = 5.0e-12      # Source/Arnoldi/Arnoldi_Driver.cu:31
+MAX_PASS_INDEX = 12        # "if(it>12) break" after the pass (:64,:109)
+IM_EIG_TOL = 1.0e-15       # Source/Arnoldi/Macros.h:10
+
+
+class ArnoldiBreakdown(RuntimeError):
+    """||f|| < 1e-15 on entry with k == 0 (Arnoldi_Driver.cu:38-41)."""
+
+
+def arnoldi_driver(Axb, V: np.ndarray, H: np.ndarray, f: np.ndarray, k: int, m: int,
+                   tol: float = ARNOLDI_TOL) -> dict:
+    """Extend an Arnoldi factorisation in place (Arnoldi_Driver.cu:29-120).
+
+    ``V`` has shape (m, n) (row j is Krylov column j), ``H`` is a normal
+    (m, m) matrix ``H[row, col]``, ``f`` the residual (n,).  ``Axb(v)``
+    returns A v.  Returns statistics: reorthogonalisation passes per column
+    and the number of columns that hit the pass limit.
+    """
+    passes = []
+    failures = 0
+    if k == 0:
+        beta = float(np.sqrt(np.dot(f, f)))
+        if beta < 1.0e-15:
+            raise ArnoldiBreakdown("norm of the input vector ||f|| < 1e-15")
+        v = f * (1.0 / beta)                       # Dcopy + Dscal(1/||f||)
+        w = Axb(v)
+        alpha = float(np.dot(v, w))
+        f[:] = w - alpha * v                       # Dcopy + Daxpy(-alpha)
+        c = 1.0
+        it = 0
+        while c > tol:                             # signed c, as in :60
+            it += 1
+            c = float(np.dot(v, f))
+            f -= c * v
+            alpha += c
+            if it > MAX_PASS_INDEX:
+                failures += 1
+                break
+        passes.append(it)
+        H[0, 0] = alpha
+        V[0, :] = v
+    for j in range(k + 1, m):
+        beta = float(np.sqrt(np.dot(f, f)))
+        v = f * (1.0 / beta)
+        H[j, j - 1] = beta
+        V[j, :] = v
+        w = Axb(v)
+        Vj = V[: j + 1]
+        h = np.zeros(m)
+        h[: j + 1] = Vj @ w                        # Dgemv T, columns 0..j
+        f[:] = w - Vj.T @ h[: j + 1]               # Dgemv N, alpha=-1, beta=1
+        cn = 1.0
+        it = 0
+        while cn > tol:
+            it += 1
+            c = Vj @ f
+            f -= Vj.T @ c
+            h[: j + 1] += c
+            cn = float(np.sqrt(np.dot(c, c)))
+            if it > MAX_PASS_INDEX:
+                failures += 1
+                break
+        passes.append(it)
+        H[:, j] = h
+    return {"passes": passes, "failures": failures}
+
+
+def _householder_q(A: np.ndarray) -> np.ndarray:
+    """Q factor of LAPACK's Householder QR (dgeqrf) of a square matrix."""
+    q, _ = np.linalg.qr(A, mode="complete")
+    return q
+
+
+def _imag_exceeds(eig_im: float) -> bool:
+    # QR_step tests abs() in double (QR_Shifts.cpp:9).
+    return abs(eig_im) > IM_EIG_TOL
+
+
+def _imag_exceeds_f32(eig_im: float) -> bool:
+    # QR_shifts decrements j after testing fabsf(), i.e. in single precision
+    # (QR_Shifts.cpp:63).
+    return float(np.float32(abs(eig_im))) > IM_EIG_TOL
+
+
+def qr_step(Qacc: np.ndarray, H: np.ndarray, eig: complex) -> tuple[np.ndarray, np.ndarray]:
+    """One (double-)shift QR step (QR_Shifts.cpp:7-40); returns (Qacc Q, Q^T H Q)."""
+    m = H.shape[0]
+    er, ei = eig.real, eig.imag
+    if _imag_exceeds(ei):
+        H1 = H - er * np.eye(m)
+        H1 = H1 @ H1 + (ei * ei) * np.eye(m)
+    else:
+        H1 = H - er * np.eye(m)
+    Q = _householder_q(H1)
+    Hn = (Q.T @ H) @ Q
+    for j in range(m - 1):
+        Hn[j + 2:, j] = 0.0                        # remove noise below the subdiagonal
+    return Qacc @ Q, Hn
+
+
+def qr_shifts(k: int, m: int, H: np.ndarray, eigs) -> tuple[np.ndarray, np.ndarray, int]:
+    """QR_shifts (QR_Shifts.cpp:46-72): returns (Q, H_new, ko)."""
+    Q = np.eye(m)
+    Hn = np.array(H, dtype=np.float64, copy=True)
+    j = m
+    while j > k:
+        e = complex(eigs[j - 1])
+        Q, Hn = qr_step(Q, Hn, e)
+        j -= 2 if _imag_exceeds_f32(e.imag) else 1
+    return Q, Hn, j
+
+
+def select_shifts(m: int, H: np.ndarray, which: str = "LR") -> tuple[np.ndarray, np.ndarray]:
+    """select_shifts (Select_Shifts.cpp:86-133): eigenvalues of H sorted by
+    'which' ("LR": largest real part first, "LM": largest modulus first) and
+    the Ritz estimates |last component of each eigenvector|."""
+    w, vecs = np.linalg.eig(np.asarray(H, dtype=np.complex128))
+    if which == "LR":
+        key = -w.real
+    elif which == "LM":
+        key = -np.abs(w)
+    else:
+        key = np.zeros(m)
+    order = np.argsort(key, kind="stable")
+    # zgeev normalises each eigenvector to unit 2-norm; so does numpy.
+    ritz = np.abs(vecs[m - 1, order])
+    return w[order], ritz
+
+
+def ira_restart(V: np.ndarray, f: np.ndarray, Q: np.ndarray, H: np.ndarray, k0: int) -> float:
+    """Restart update of Implicit_restart_Arnoldi.cu:544-563, in place.
+
+    Returns ||f|| before the update (:547).  ``Q`` and ``H`` are normal
+    (m, m) matrices; the columns k0..m-1 of Q are reset to the identity, as
+    the reference does before forming V Q.
+    """
+    m = Q.shape[0]
+    fnorm = float(np.sqrt(np.dot(f, f)))
+    q = Q[:, k0].copy()
+    hl = H[k0, k0 - 1]
+    ql = Q[m - 1, k0 - 1]
+    f[:] = hl * (V.T @ q) + ql * f                 # Dgemv N: alpha=hl, beta=ql
+    Q[:, k0:] = np.eye(m)[:, k0:]
+    V[:] = (V.T @ Q).T                             # Dgemm V Q
+    return fnorm
+
+
+def laplace1d(v: np.ndarray) -> np.ndarray:
+    """The reference's Krylov test operator (Matrix_Vector_emulator.cu:10-20):
+    w_i = v_{i+1} - 2 v_i + v_{i-1} periodic, then w_0 := 0."""
+    w = np.roll(v, -1) - 2.0 * v + np.roll(v, 1)
+    w[0] = 0.0
+    return w
+
+
+def arnoldi_residual(Axb, V: np.ndarray, H: np.ndarray, f: np.ndarray, m: int) -> float:
+    """max |A V - V H - f e_m^T| relative to ||H||: the Arnoldi relation."""
+    AV = np.stack([Axb(V[j]) for j in range(m)])           # rows = columns of A V
+    VH = (V[:m].T @ H[:m, :m]).T
+    R = AV - VH
+    R[m - 1] -= f
+    return float(np.abs(R).max() / max(np.abs(H).max(), 1.0))
