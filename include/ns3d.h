@@ -192,6 +192,21 @@ ns3d_status ns3d_matvec_reduced(ns3d_solver* h, const ns3d_complex* ux, const ns
                                 double Re, double tau);
 
 /* ----------------------------------------------------------------------- */
+/* plain 3-D transforms (Source/math_support.cu:301-334)                      */
+/* ----------------------------------------------------------------------- */
+
+/* FFTN_Device: the unnormalised forward real-to-complex 3-D transform
+ * (cufftExecD2Z) of a real [Nx][Ny][Nz] device array (z fastest) into the
+ * [Nx][Ny][Mz] complex layout.  in and out must not overlap. */
+ns3d_status ns3d_fft_r2c(ns3d_solver* h, const double* in, ns3d_complex* out);
+
+/* iFFTN_Device: complex-to-real 3-D transform (cufftExecZ2D) followed by the
+ * 1/(Nx Ny Nz) scale (scale_double).  As cuFFT does, only the Hermitian part
+ * of the kz = 0 and kz = Nz/2 planes contributes.  `in` is not modified
+ * (cuFFT's Z2D may overwrite its input); the handle's scratch is used. */
+ns3d_status ns3d_fft_c2r(ns3d_solver* h, const ns3d_complex* in, double* out);
+
+/* ----------------------------------------------------------------------- */
 /* diagnostics (Source/math_support.cu:720-806, Source/divergence.cu:8-31)    */
 /* ----------------------------------------------------------------------- */
 

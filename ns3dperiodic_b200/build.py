@@ -19,8 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(ROOT, "_build", "obj")
 LIB = os.path.join(HERE, "libns3d_b200.so")
 
-SOURCES = ["k_xy.cu", "k_z.cu", "k_fwdx.cu", "aux_kernels.cu", "solver.cu", "noalloc.cu",
-           "krylov.cu", "qr_shifts.cpp"]
+SOURCES = ["k_xy.cu", "k_z.cu", "k_fwdx.cu", "k_fft3d.cu", "aux_kernels.cu", "solver.cu",
+           "noalloc.cu", "krylov.cu", "qr_shifts.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",

@@ -22,6 +22,12 @@ cudaError_t run_z(const ZArgs<6>& a, const PassGeom& g, cudaStream_t st);
 // device; called when a handle is created (outside any stream capture).
 cudaError_t prepare_xy(const PassGeom& g);
 cudaError_t prepare_fwdx(const PassGeom& g);
+// Plain 3-D transforms (k_fft3d.cu): one complex line pass along x (axis 0)
+// or y (axis 1), dir +1 inverse / -1 forward; the paired z passes.
+cudaError_t run_line(int axis, int dir, const LineArgs& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_z_c2r(const ZPlainArgs& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_z_r2c(const ZPlainArgs& a, const PassGeom& g, cudaStream_t st);
+cudaError_t prepare_fft3d(const PassGeom& g);
 // mode: UpdateMode; combine: out = ca*un + cb*base
 cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs& a, const PassGeom& g,
                       cudaStream_t st);

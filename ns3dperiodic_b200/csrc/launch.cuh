@@ -186,4 +186,47 @@ inline cudaError_t launch_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream
   }
 }
 
+template <int AXIS, int DIR>
+cudaError_t launch_line(const LineArgs& a, const PassGeom& g, cudaStream_t st,
+                        bool prepare_only = false) {
+  const long long lines = AXIS == 0 ? (long long)g.Ny * g.Mz : (long long)g.Nx * g.Mz;
+  switch (AXIS == 0 ? g.Nx : g.Ny) {
+#define NS3D_CASE(N)                                                                    \
+  case N: {                                                                             \
+    constexpr int P = p_xy(N);                                                          \
+    using S = PassSmem<N, P>;                                                           \
+    const unsigned grid = persistent_grid<KTag<30 + 2 * AXIS + (DIR > 0 ? 1 : 0), N, P, 0>>( \
+        line_kernel<N, P, AXIS, DIR>, S::BYTES, (lines + S::LPC - 1) / S::LPC);         \
+    if (prepare_only) return cudaGetLastError();                                        \
+    line_kernel<N, P, AXIS, DIR><<<grid, kThreads, S::BYTES, st>>>(a, g);                \
+    return cudaGetLastError();                                                          \
+  }
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <bool C2R>
+cudaError_t launch_z_plain(const ZPlainArgs& a, const PassGeom& g, cudaStream_t st) {
+  const long long pairs = ((long long)g.Nx * g.Ny) / 2;
+  switch (g.Nz) {
+#define NS3D_CASE(N)                                                                  \
+  case N: {                                                                           \
+    constexpr int P = p_z(N);                                                         \
+    const unsigned grid = blocks_for(pairs, lines_per_cta_z<N, P>());                 \
+    if (C2R)                                                                          \
+      z_c2r_kernel<N, P><<<grid, kWarpsPerCta * 32, 0, st>>>(a, g);                   \
+    else                                                                              \
+      z_r2c_kernel<N, P><<<grid, kWarpsPerCta * 32, 0, st>>>(a, g);                   \
+    return cudaGetLastError();                                                        \
+  }
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
 }  // namespace ns3d

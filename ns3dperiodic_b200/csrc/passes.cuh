@@ -70,11 +70,12 @@ struct LaneMap {
 
 
 // ---------------------------------------------------------------------------
-// Persistent, software-pipelined x / y passes.  Each CTA walks groups of LPC
-// lines (grid = resident CTAs); every thread owns a private double buffer in
-// shared memory and, while the current line of field f is transformed,
-// prefetches with cp.async the P samples it will need for the next unit (the
-// next field of the same lines, or the first field of the next group).
+// Software-pipelined x / y passes.  A CTA handles groups of LPC lines (one
+// group per CTA by default, see NS3D_SCHED); every thread owns a private
+// double buffer in shared memory and, while the current line of field f is
+// transformed, prefetches with cp.async the P samples it will need for the
+// next unit (the next field of the same lines, or the first field of the
+// next group).
 // ---------------------------------------------------------------------------
 constexpr int kThreads = kWarpsPerCta * 32;
 
@@ -650,6 +651,160 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) fwd_y_kernel(FwdYArgs a,
     }
   }
   cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// Plain 3-D transforms of one field (FFTN_Device / iFFTN_Device,
+// Source/math_support.cu:301-334): no mask, no derivatives.
+//
+// line_kernel: one complex line pass, lines along x (AXIS 0: batch
+// L = y*Mz + z, stride Ny*Mz) or y (AXIS 1: batch b = x*Mz + z, base
+// x*Ny*Mz + z, stride Mz); `out` may alias `in` (every line is read before it
+// is written, and the prefetch only touches lines of later groups).
+// ---------------------------------------------------------------------------
+struct LineArgs {
+  const double2* in;
+  double2* out;
+  const double2* tw;
+};
+
+template <int N, int P, int AXIS, int DIR>
+__global__ void __launch_bounds__(kThreads, kMinCtasXY) line_kernel(LineArgs a, PassGeom g) {
+  using S = PassSmem<N, P>;
+  using F = typename S::F;
+  using LM = typename S::LM;
+  constexpr int T = F::T;
+  extern __shared__ double2 dsm[];
+  F::load_tw(dsm + S::TW, a.tw);
+  const double2* tw_s = dsm + S::TW;
+  int li, t;
+  LM::get(li, t);
+  double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
+  double2* pf = dsm + S::PF + threadIdx.x;
+  const int nb = AXIS == 0 ? g.Ny * g.Mz : g.Nx * g.Mz;
+  const size_t stride = AXIS == 0 ? (size_t)g.Ny * g.Mz : (size_t)g.Mz;
+  const int groups = (nb + LM::LPC - 1) / LM::LPC;
+  const GroupRange gr = group_range(groups);
+  int grp = gr.grp;
+  if (grp >= gr.end) return;
+  auto line_base = [&](int gidx) -> size_t {
+    const int b = gidx * LM::LPC + li;
+    const int bc = b < nb ? b : 0;
+    if (AXIS == 0) return (size_t)bc;
+    const int x = bc / g.Mz, z = bc - x * g.Mz;
+    return (size_t)x * g.Ny * g.Mz + z;
+  };
+  issue_line<P, T>(pf, a.in, line_base(grp), stride, t);
+  cp_async_commit();
+  int ub = 0;
+  for (; grp < gr.end; grp += gr.step) {
+    const bool valid = grp * LM::LPC + li < nb;
+    const size_t base = line_base(grp);
+    const int gn = grp + gr.step;
+    const double2* cur = pf + ub * (P * kThreads);
+    double2* nxt = pf + (ub ^ 1) * (P * kThreads);
+    if (gn < gr.end) issue_line<P, T>(nxt, a.in, line_base(gn), stride, t);
+    cp_async_commit();
+    cp_async_wait<1>();
+    double2 v[P];
+#pragma unroll
+    for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
+    F::template run<DIR>(v, t, sbuf, tw_s);
+    if (valid) {
+#pragma unroll
+      for (int s = 0; s < P; ++s) a.out[base + (size_t)(t + T * s) * stride] = v[s];
+    }
+    ub ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
+// z passes of the plain transforms: two z lines b and b + nb/2 of one field
+// share one complex FFT (nb = Nx*Ny, even for every compiled extent).
+struct ZPlainArgs {
+  const double2* cin;  // complex [nb][Mz] (C2R input)
+  const double* rin;   // real [nb][Nz]   (R2C input)
+  double2* cout;       // complex [nb][Mz] (R2C output)
+  double* rout;        // real [nb][Nz]   (C2R output)
+  const double2* tw;
+};
+
+// C2R along z with the 1/(Nx Ny Nz) scale: the Hermitian extension of each
+// half line keeps only the real part of its kz = 0 and kz = Nz/2 bins (what
+// cufftExecZ2D does with the non-Hermitian planes the reference produces).
+template <int NZ, int P>
+__global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_c2r_kernel(ZPlainArgs a,
+                                                                              PassGeom g) {
+  using F = LineFFT<NZ, P>;
+  constexpr int T = F::T;
+  using LM = ZLaneMap<T>;
+  __shared__ double2 tw_s[F::TWLEN];
+  __shared__ double2 sbuf_all[LM::LPC][F::BUF];
+  F::load_tw(tw_s, a.tw);
+  int li, t;
+  LM::get(li, t);
+  const int half = (g.Nx * g.Ny) >> 1;
+  const int p = blockIdx.x * LM::LPC + li;
+  const bool valid = p < half;
+  const int pc = valid ? p : 0;
+  double2* sbuf = sbuf_all[li];
+  double2 w[P];
+#pragma unroll
+  for (int s = 0; s < P; ++s) {
+    const int k = t + T * s;
+    const bool upper = k > NZ / 2;
+    const int q = upper ? NZ - k : k;
+    double2 c1 = __ldg(a.cin + (size_t)pc * g.Mz + q);
+    double2 c2 = __ldg(a.cin + (size_t)(pc + half) * g.Mz + q);
+    if (k == 0 || k == NZ / 2) {
+      c1.y = 0.0;
+      c2.y = 0.0;
+    }
+    if (upper) {
+      c1.y = -c1.y;
+      c2.y = -c2.y;
+    }
+    w[s] = make_double2(c1.x - c2.y, c1.y + c2.x);
+  }
+  F::template run<+1>(w, t, sbuf, tw_s);
+  if (valid) {
+    const double sc = g.inv_vol;
+#pragma unroll
+    for (int s = 0; s < P; ++s) {
+      const int k = t + T * s;
+      a.rout[(size_t)pc * NZ + k] = w[s].x * sc;
+      a.rout[(size_t)(pc + half) * NZ + k] = w[s].y * sc;
+    }
+  }
+}
+
+// R2C along z (unnormalised), the half spectra k = 0..Nz/2.
+template <int NZ, int P>
+__global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_r2c_kernel(ZPlainArgs a,
+                                                                              PassGeom g) {
+  using F = LineFFT<NZ, P>;
+  constexpr int T = F::T;
+  using LM = ZLaneMap<T>;
+  __shared__ double2 tw_s[F::TWLEN];
+  __shared__ double2 sbuf_all[LM::LPC][F::BUF];
+  F::load_tw(tw_s, a.tw);
+  int li, t;
+  LM::get(li, t);
+  const int half = (g.Nx * g.Ny) >> 1;
+  const int p = blockIdx.x * LM::LPC + li;
+  const bool valid = p < half;
+  const int pc = valid ? p : 0;
+  double2* sbuf = sbuf_all[li];
+  double2 w[P];
+#pragma unroll
+  for (int s = 0; s < P; ++s) {
+    const int k = t + T * s;
+    w[s] = make_double2(__ldg(a.rin + (size_t)pc * NZ + k),
+                        __ldg(a.rin + (size_t)(pc + half) * NZ + k));
+  }
+  F::template run<-1>(w, t, sbuf, tw_s);
+  store_pair_spectrum<NZ, P>(w, sbuf, t, a.cout + (size_t)pc * g.Mz,
+                             a.cout + (size_t)(pc + half) * g.Mz, 0, valid);
 }
 
 // ---------------------------------------------------------------------------

@@ -380,6 +380,7 @@ ns3d_status ns3d_create(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
     return bail(NS3D_ERR_OOM);
   if ((e = ns3d::prepare_xy(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   if ((e = ns3d::prepare_fwdx(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
+  if ((e = ns3d::prepare_fft3d(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   *out = h;
   return NS3D_OK;
@@ -531,6 +532,45 @@ ns3d_status ns3d_rhs(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex*
   double2* r[3] = {(double2*)rx, (double2*)ry, (double2*)rz};
   NS3D_TRY(conv_front(h, uc, nullptr));
   return finish(h, ns3d::kRhs, true, uc, r, nullptr, 0.0, 1.0, 0.0, Re);
+}
+
+ns3d_status ns3d_fft_r2c(ns3d_solver* h, const double* in, ns3d_complex* out) {
+  NS3D_TRY(check_handle(h));
+  if (!in || !out) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  const PassGeom& g = h->geom;
+  ns3d::ZPlainArgs z{};
+  z.rin = in;
+  z.cout = (double2*)out;
+  z.tw = h->tw[2];
+  NS3D_CHECK(h, ns3d::run_z_r2c(z, g, h->stream), "z_r2c");
+  ns3d::LineArgs l{};
+  l.in = (const double2*)out;
+  l.out = (double2*)out;
+  l.tw = h->tw[1];
+  NS3D_CHECK(h, ns3d::run_line(1, -1, l, g, h->stream), "line_y");
+  l.tw = h->tw[0];
+  NS3D_CHECK(h, ns3d::run_line(0, -1, l, g, h->stream), "line_x");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_fft_c2r(ns3d_solver* h, const ns3d_complex* in, double* out) {
+  NS3D_TRY(check_handle(h));
+  if (!in || !out) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  const PassGeom& g = h->geom;
+  ns3d::LineArgs l{};
+  l.in = (const double2*)in;
+  l.out = h->A[0];
+  l.tw = h->tw[0];
+  NS3D_CHECK(h, ns3d::run_line(0, +1, l, g, h->stream), "line_x");
+  l.in = h->A[0];
+  l.tw = h->tw[1];
+  NS3D_CHECK(h, ns3d::run_line(1, +1, l, g, h->stream), "line_y");
+  ns3d::ZPlainArgs z{};
+  z.cin = h->A[0];
+  z.rout = out;
+  z.tw = h->tw[2];
+  NS3D_CHECK(h, ns3d::run_z_c2r(z, g, h->stream), "z_c2r");
+  return NS3D_OK;
 }
 
 ns3d_status ns3d_convolution(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,

@@ -178,6 +178,35 @@ class Solver:
                     "ns3d_convolution_uv")
         return out
 
+    # -- Source/math_support.h: FFTN_Device / iFFTN_Device -----------------
+    @property
+    def real_shape(self):
+        return (self.Nx, self.Ny, self.Nz)
+
+    def fftn(self, x, out=None):
+        """FFTN_Device: unnormalised R2C of a real (Nx, Ny, Nz) float64 tensor."""
+        t = self._torch
+        if (x.dtype != t.float64 or x.device != self.device
+                or tuple(x.shape) != self.real_shape or not x.is_contiguous()):
+            raise ValueError(f"x: expected contiguous float64 {self.real_shape} on {self.device}")
+        out = out if out is not None else t.empty(self.shape, dtype=t.complex128,
+                                                  device=self.device)
+        self._check(self._L.ns3d_fft_r2c(self._h, _ptr(x), self._fields([out] * 3, "out")[0]),
+                    "ns3d_fft_r2c")
+        return out
+
+    def ifftn(self, X, out=None):
+        """iFFTN_Device: C2R of a complex (Nx, Ny, Nz//2+1) tensor, scaled by 1/(Nx Ny Nz)."""
+        t = self._torch
+        p = self._fields([X] * 3, "X")[0]
+        out = out if out is not None else t.empty(self.real_shape, dtype=t.float64,
+                                                  device=self.device)
+        if (out.dtype != t.float64 or tuple(out.shape) != self.real_shape
+                or not out.is_contiguous() or out.device != self.device):
+            raise ValueError("out: expected a contiguous float64 real-space tensor")
+        self._check(self._L.ns3d_fft_c2r(self._h, p, _ptr(out)), "ns3d_fft_c2r")
+        return out
+
     # -- Krylov adapters (Source/NS3D_periodic.cu:173-385) ------------------
     @property
     def krylov_length(self) -> int:
