@@ -119,7 +119,8 @@ ns3d_status ns3d_euler_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, 
                             double dt, double Re);
 
 /* rhs = -P.Q(u) - |k|^2/Re u + f: return_RHS (Source/RK_time_step.h:34,
- * Source/RK_time_step.cu:231-245).  rhs must not alias u. */
+ * Source/RK_time_step.cu:231-245).  rhs may be u itself (in place), as in
+ * NSCallRHS_reduced (Source/NS3D_periodic.cu:415-441). */
 ns3d_status ns3d_rhs(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
                      const ns3d_complex* uz, ns3d_complex* rx, ns3d_complex* ry, ns3d_complex* rz,
                      double Re);
@@ -146,6 +147,14 @@ ns3d_status ns3d_convolution_uv(ns3d_solver* h, const ns3d_complex* ux, const ns
 ns3d_status ns3d_jvp_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
                           ns3d_complex* vx, ns3d_complex* vy, ns3d_complex* vz, double dt,
                           double Re);
+
+/* v <- v + dt (-P.B(u,v) - |k|^2/Re v): single_time_step_UV
+ * (Source/RK_time_step.h:21, Source/RK_time_step.cu:265-278); u is not
+ * changed. */
+ns3d_status ns3d_tangent_euler_step(ns3d_solver* h, const ns3d_complex* ux,
+                                    const ns3d_complex* uy, const ns3d_complex* uz,
+                                    ns3d_complex* vx, ns3d_complex* vy, ns3d_complex* vz,
+                                    double dt, double Re);
 
 /* nsteps tangent steps (the Timesteps_period loop of
  * NSCallMatrixVector_exponential, Source/NS3D_periodic.cu:444-470). */
@@ -205,6 +214,10 @@ ns3d_status ns3d_fft_r2c(ns3d_solver* h, const double* in, ns3d_complex* out);
  * of the kz = 0 and kz = Nz/2 planes contributes.  `in` is not modified
  * (cuFFT's Z2D may overwrite its input); the handle's scratch is used. */
 ns3d_status ns3d_fft_c2r(ns3d_solver* h, const ns3d_complex* in, double* out);
+
+/* The same transform without the scale: iFFTN_Device(source, destination)
+ * (Source/math_support.cu:314-322), which runs cufftExecZ2D alone. */
+ns3d_status ns3d_fft_c2r_unscaled(ns3d_solver* h, const ns3d_complex* in, double* out);
 
 /* ----------------------------------------------------------------------- */
 /* diagnostics (Source/math_support.cu:720-806, Source/divergence.cu:8-31)    */

@@ -31,7 +31,8 @@ EXPORTS = (
     "ns3d_jvp_step", "ns3d_jvp_steps", "ns3d_linearised_rhs", "ns3d_implicit_tangent_step",
     "ns3d_krylov_length", "ns3d_pack_reduced", "ns3d_unpack_reduced", "ns3d_matvec_reduced",
     "ns3d_diagnostics", "ns3d_profile_passes", "ns3d_mask_cutoff", "ns3d_twiddles",
-    "ns3d_convolution_noalloc", "ns3d_fft_r2c", "ns3d_fft_c2r",
+    "ns3d_convolution_noalloc", "ns3d_fft_r2c", "ns3d_fft_c2r", "ns3d_fft_c2r_unscaled",
+    "ns3d_tangent_euler_step",
     "ns3d_krylov_create", "ns3d_krylov_destroy", "ns3d_krylov_set_stream",
     "ns3d_krylov_last_error", "ns3d_arnoldi", "ns3d_krylov_stats", "ns3d_qr_shifts",
     "ns3d_ira_restart", "ns3d_map_linearised", "ns3d_map_exponential", "ns3d_map_laplace1d",
@@ -110,6 +111,8 @@ def _sig(lib):
                                      + [_P] * 6 + [_P], c_int),
         "ns3d_fft_r2c": ([_P, _P, _P], c_int),
         "ns3d_fft_c2r": ([_P, _P, _P], c_int),
+        "ns3d_fft_c2r_unscaled": ([_P, _P, _P], c_int),
+        "ns3d_tangent_euler_step": ([_P] + [_P] * 6 + [c_double, c_double], c_int),
         "ns3d_krylov_create": ([c_int64, c_int, ctypes.POINTER(c_void_p)], c_int),
         "ns3d_krylov_destroy": ([_P], c_int),
         "ns3d_krylov_set_stream": ([_P, _P], c_int),

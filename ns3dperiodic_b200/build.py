@@ -1,8 +1,9 @@
-"""Builds the CUDA library in-tree: ns3dperiodic_b200/libns3d_b200.so.
+"""Builds the CUDA libraries in-tree: ns3dperiodic_b200/libns3d_b200.so (the
+C ABI of include/ns3d.h) and ns3dperiodic_b200/libns3d_compat.so (the
+reference-signature C++ layer of include/ns3d_compat.h over that ABI).
 
 nvcc for sm_100a only, one object per translation unit (compiled in
-parallel), linked into a shared library exporting the C ABI of
-include/ns3d.h.  Usage: ``python -m ns3dperiodic_b200.build [-j N]``.
+parallel).  Usage: ``python -m ns3dperiodic_b200.build [-j N]``.
 """
 from __future__ import annotations
 
@@ -18,6 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(ROOT, "_build", "obj")
 LIB = os.path.join(HERE, "libns3d_b200.so")
+COMPAT_LIB = os.path.join(HERE, "libns3d_compat.so")
+COMPAT_SOURCE = "compat.cu"
 
 SOURCES = ["k_xy.cu", "k_z.cu", "k_fwdx.cu", "k_fft3d.cu", "aux_kernels.cu", "solver.cu",
            "noalloc.cu", "krylov.cu", "qr_shifts.cpp"]
@@ -44,10 +47,11 @@ def _compile(src: str) -> tuple[str, str]:
 
 
 def _stale(objs) -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(COMPAT_LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "ns3d.h")]
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [
+        os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
@@ -67,6 +71,13 @@ def build(jobs: int = 0, force: bool = False, verbose: bool = False) -> str:
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")
+    # the reference-signature C++ layer over the C ABI, in its own library
+    cobj, _ = _compile(COMPAT_SOURCE)
+    cmd = [nvcc(), *ARCH, "-shared", "-o", COMPAT_LIB, cobj, "-L" + HERE, "-lns3d_b200",
+           "-Xlinker", "-rpath=$ORIGIN", "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"compat link failed:\n{r.stderr}")
     if verbose:
         print("built", LIB, file=sys.stderr)
     return LIB

@@ -726,10 +726,11 @@ struct ZPlainArgs {
   const double* rin;   // real [nb][Nz]   (R2C input)
   double2* cout;       // complex [nb][Mz] (R2C output)
   double* rout;        // real [nb][Nz]   (C2R output)
+  double scale;        // C2R output factor: 1/(Nx Ny Nz) or 1
   const double2* tw;
 };
 
-// C2R along z with the 1/(Nx Ny Nz) scale: the Hermitian extension of each
+// C2R along z times `scale`: the Hermitian extension of each
 // half line keeps only the real part of its kz = 0 and kz = Nz/2 bins (what
 // cufftExecZ2D does with the non-Hermitian planes the reference produces).
 template <int NZ, int P>
@@ -768,7 +769,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_c2r_kernel(ZPl
   }
   F::template run<+1>(w, t, sbuf, tw_s);
   if (valid) {
-    const double sc = g.inv_vol;
+    const double sc = a.scale;
 #pragma unroll
     for (int s = 0; s < P; ++s) {
       const int k = t + T * s;

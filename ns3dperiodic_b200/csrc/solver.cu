@@ -553,7 +553,8 @@ ns3d_status ns3d_fft_r2c(ns3d_solver* h, const double* in, ns3d_complex* out) {
   return NS3D_OK;
 }
 
-ns3d_status ns3d_fft_c2r(ns3d_solver* h, const ns3d_complex* in, double* out) {
+namespace {
+ns3d_status fft_c2r(ns3d_solver* h, const ns3d_complex* in, double* out, double scale) {
   NS3D_TRY(check_handle(h));
   if (!in || !out) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
   const PassGeom& g = h->geom;
@@ -568,9 +569,19 @@ ns3d_status ns3d_fft_c2r(ns3d_solver* h, const ns3d_complex* in, double* out) {
   ns3d::ZPlainArgs z{};
   z.cin = h->A[0];
   z.rout = out;
+  z.scale = scale;
   z.tw = h->tw[2];
   NS3D_CHECK(h, ns3d::run_z_c2r(z, g, h->stream), "z_c2r");
   return NS3D_OK;
+}
+}  // namespace
+
+ns3d_status ns3d_fft_c2r(ns3d_solver* h, const ns3d_complex* in, double* out) {
+  return h ? fft_c2r(h, in, out, h->geom.inv_vol) : NS3D_ERR_BAD_ARG;
+}
+
+ns3d_status ns3d_fft_c2r_unscaled(ns3d_solver* h, const ns3d_complex* in, double* out) {
+  return fft_c2r(h, in, out, 1.0);
 }
 
 ns3d_status ns3d_convolution(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
@@ -597,6 +608,22 @@ ns3d_status ns3d_convolution_uv(ns3d_solver* h, const ns3d_complex* ux, const ns
   double2* q[3] = {(double2*)Qx, (double2*)Qy, (double2*)Qz};
   NS3D_TRY(conv_front(h, uc, vc));
   return finish(h, ns3d::kConvOut, false, nullptr, q, nullptr, 0.0, 1.0, 0.0, 1.0);
+}
+
+// single_time_step_UV (Source/RK_time_step.cu:265-278): v <- v + dt J(u) v.
+ns3d_status ns3d_tangent_euler_step(ns3d_solver* h, const ns3d_complex* ux,
+                                    const ns3d_complex* uy, const ns3d_complex* uz,
+                                    ns3d_complex* vx, ns3d_complex* vy, ns3d_complex* vz,
+                                    double dt, double Re) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, dt, Re));
+  if (!args_ok3(ux, uy, uz) || !args_ok3(vx, vy, vz))
+    return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  const double2* uc[3] = {(const double2*)ux, (const double2*)uy, (const double2*)uz};
+  double2* v[3] = {(double2*)vx, (double2*)vy, (double2*)vz};
+  const double2* vc[3] = {v[0], v[1], v[2]};
+  NS3D_TRY(conv_front(h, uc, vc));
+  return finish(h, ns3d::kExplicit, false, vc, v, nullptr, 0.0, 1.0, dt, Re);
 }
 
 ns3d_status ns3d_jvp_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,

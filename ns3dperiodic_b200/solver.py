@@ -156,6 +156,14 @@ class Solver:
         self._check(self._L.ns3d_linearised_rhs(self._h, *p, *q, Re), "ns3d_linearised_rhs")
         return V
 
+    def single_time_step_uv(self, U, V, dt: float, Re: float):
+        """single_time_step_UV: V <- V + dt J(U) V in place (U unchanged)."""
+        p = self._fields(U, "U")
+        q = self._fields(V, "V")
+        self._check(self._L.ns3d_tangent_euler_step(self._h, *p, *q, dt, Re),
+                    "ns3d_tangent_euler_step")
+        return V
+
     def single_time_step_iuv_rhs(self, U, V, dt: float, Re: float):
         p = self._fields(U, "U")
         q = self._fields(V, "V")
@@ -195,8 +203,9 @@ class Solver:
                     "ns3d_fft_r2c")
         return out
 
-    def ifftn(self, X, out=None):
-        """iFFTN_Device: C2R of a complex (Nx, Ny, Nz//2+1) tensor, scaled by 1/(Nx Ny Nz)."""
+    def ifftn(self, X, out=None, scale: bool = True):
+        """iFFTN_Device: C2R of a complex (Nx, Ny, Nz//2+1) tensor, scaled by
+        1/(Nx Ny Nz) (scale=False: the two-argument iFFTN_Device, no scale)."""
         t = self._torch
         p = self._fields([X] * 3, "X")[0]
         out = out if out is not None else t.empty(self.real_shape, dtype=t.float64,
@@ -204,7 +213,8 @@ class Solver:
         if (out.dtype != t.float64 or tuple(out.shape) != self.real_shape
                 or not out.is_contiguous() or out.device != self.device):
             raise ValueError("out: expected a contiguous float64 real-space tensor")
-        self._check(self._L.ns3d_fft_c2r(self._h, p, _ptr(out)), "ns3d_fft_c2r")
+        fn = self._L.ns3d_fft_c2r if scale else self._L.ns3d_fft_c2r_unscaled
+        self._check(fn(self._h, p, _ptr(out)), "ns3d_fft_c2r")
         return out
 
     # -- Krylov adapters (Source/NS3D_periodic.cu:173-385) ------------------

@@ -1,4 +1,4 @@
-"""ctypes binding of oracle/_ref/libns3d_ref.so (TEST INFRASTRUCTURE).
+"""ctypes binding of oracle/_ref/libns3d_ref[_compat].so (TEST INFRASTRUCTURE).
 
 The library is the reference's own CUDA path (unmodified sources, built for
 sm_100a by oracle/Makefile) plus the project-written harness
@@ -26,14 +26,23 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_dp)
 
 
+COMPAT_LIB_PATH = os.path.join(_HERE, "_ref", "libns3d_ref_compat.so")
+
+
 class RefSolver:
-    """One instance of the reference's file-static state (it is not re-entrant)."""
+    """One instance of the reference's file-static state (it is not re-entrant).
 
-    _lib = None
+    ``lib_path`` selects the build of the harness: the default links the
+    reference's own objects; COMPAT_LIB_PATH links the same harness object
+    against this project's reference-signature layer (libns3d_compat.so).
+    """
 
-    def __init__(self, Nx, Ny, Nz, Lx=2 * np.pi, Ly=2 * np.pi, Lz=2 * np.pi):
-        if RefSolver._lib is None:
-            lib = ctypes.CDLL(LIB_PATH)
+    _libs = {}
+
+    def __init__(self, Nx, Ny, Nz, Lx=2 * np.pi, Ly=2 * np.pi, Lz=2 * np.pi, lib_path=None):
+        path = lib_path or LIB_PATH
+        if path not in RefSolver._libs:
+            lib = ctypes.CDLL(path)
             for name in ("ref_set_u", "ref_set_v", "ref_set_f", "ref_get_u", "ref_get_v",
                          "ref_conv", "ref_conv_uv"):
                 getattr(lib, name).argtypes = [_dp]
@@ -54,8 +63,8 @@ class RefSolver:
             lib.ref_time_rk3.restype = ctypes.c_double
             lib.ref_u_ptr.argtypes = [ctypes.c_int]
             lib.ref_u_ptr.restype = ctypes.c_void_p
-            RefSolver._lib = lib
-        self.lib = RefSolver._lib
+            RefSolver._libs[path] = lib
+        self.lib = RefSolver._libs[path]
         self.Nx, self.Ny, self.Nz = Nx, Ny, Nz
         self.Mz = Nz // 2 + 1
         rc = self.lib.ref_create(Nx, Ny, Nz, Lx, Ly, Lz)
