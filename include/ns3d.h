@@ -339,6 +339,15 @@ ns3d_status ns3d_qr_shifts(int k, int m, double* Q, double* H, const double* eig
 ns3d_status ns3d_ira_restart(ns3d_krylov* kr, double* V, double* f, double* Q, const double* H,
                              int k0, int m, double* f_norm);
 
+/* Device time per launch (CUDA events on the workspace stream, averaged over
+ * `reps` after one warm-up) of the three basis kernels on the first `ncols`
+ * columns of V (device, n x ncols, leading dimension n) and the vector x:
+ * ms[0] the dot products V^T x (with their fixed-order reduction), ms[1]
+ * y = x - V c, ms[2] the restart pass over V with identity coefficients (V
+ * and x are not changed).  For roofline reports. */
+ns3d_status ns3d_krylov_profile(ns3d_krylov* kr, const double* V, int ncols, const double* x,
+                                int reps, double* ms);
+
 /* Built-in maps for ns3d_arnoldi.  Each finishes its work before returning
  * and, on failure, records the first non-OK status in `status` and fills
  * `out` with NaN so the driver stops with NS3D_ERR_NONFINITE. */

@@ -28,6 +28,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "ns3d.h"
 
@@ -475,6 +476,49 @@ ns3d_status ns3d_ira_restart(ns3d_krylov* kr, double* V, double* f, double* Q, c
   for (int j = k0; j < m; ++j)
     for (int i = 0; i < m; ++i) Q[i + (int64_t)j * m] = (i == j) ? 1.0 : 0.0;
   if (!std::isfinite(kr->host[0])) return kfail(kr, NS3D_ERR_NONFINITE, "||f|| is not finite");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_krylov_profile(ns3d_krylov* kr, const double* V, int ncols, const double* x,
+                                int reps, double* ms) {
+  KR_TRY(enter(kr));
+  if (!V || !x || !ms || reps < 1 || ncols < 1 || ncols > kr->m_max)
+    return kfail(kr, NS3D_ERR_BAD_ARG, "need V, x, ms, reps >= 1, 1 <= ncols <= m_max");
+  cudaEvent_t e0, e1;
+  KR_CHECK(kr, cudaEventCreate(&e0), "event");
+  KR_CHECK(kr, cudaEventCreate(&e1), "event");
+  double* cd = kr->small + 2 + kr->m_max;
+  // identity coefficients for the restart: V Q = V, f = 0 * (V q) + 1 * f
+  std::vector<double> eye((size_t)ncols * ncols, 0.0);
+  for (int i = 0; i < ncols; ++i) eye[(size_t)i * ncols + i] = 1.0;
+  const int k0 = ncols - 1;
+  KR_CHECK(kr, cudaMemcpy(kr->qcoef, eye.data(), sizeof(double) * (size_t)ncols * (k0 + 1),
+                          cudaMemcpyHostToDevice), "Q upload");
+  KR_CHECK(kr, cudaMemcpyAsync(kr->w, x, sizeof(double) * kr->n, cudaMemcpyDeviceToDevice,
+                               kr->stream), "x copy");
+  for (int which = 0; which < 3; ++which) {
+    for (int r = -1; r < reps; ++r) {  // r = -1: warm-up
+      if (r == 0) cudaEventRecord(e0, kr->stream);
+      if (which == 0) {
+        KR_TRY(dots(kr, V, ncols, x, kStore, cd, nullptr, nullptr));
+      } else if (which == 1) {
+        KR_TRY(subtract(kr, V, ncols, cd, x, kr->w));
+      } else {
+        const size_t smem = sizeof(double) * (size_t)ncols * kRestartThreads;
+        restart_rows<<<blocks_for(kr->n, kRestartThreads, 148 * 8), kRestartThreads, smem,
+                       kr->stream>>>(const_cast<double*>(V), kr->n, ncols, k0, kr->qcoef, 0.0,
+                                     1.0, kr->w);
+        KR_CHECK(kr, cudaGetLastError(), "restart_rows");
+      }
+    }
+    cudaEventRecord(e1, kr->stream);
+    KR_CHECK(kr, cudaEventSynchronize(e1), "profile sync");
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    ms[which] = (double)t / reps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   return NS3D_OK;
 }
 

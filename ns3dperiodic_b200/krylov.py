@@ -227,6 +227,17 @@ class Krylov:
         self._check(rc, "ns3d_ira_restart")
         return fn.value
 
+    def profile(self, V, ncols: int, x, reps: int = 10):
+        """Per-launch device ms of the dot, update and restart kernels on
+        ncols columns (see ns3d_krylov_profile)."""
+        self._basis(V, ncols)
+        self._vector(x)
+        ms = (ctypes.c_double * 3)()
+        self._check(self._L.ns3d_krylov_profile(self._h, ctypes.c_void_p(V.data_ptr()), ncols,
+                                                ctypes.c_void_p(x.data_ptr()), reps, ms),
+                    "ns3d_krylov_profile")
+        return list(ms)
+
     def implicit_restart_arnoldi(self, A: Map, which: str = "LR", k: int = 6, m: int = 30,
                                  tol: float = 5.0e-8, max_iter: int = 3000, seed: int = 0,
                                  f0=None):

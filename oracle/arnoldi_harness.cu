@@ -146,6 +146,61 @@ int ref_arnoldi_dense(int n, int m, int k, const double* A, double* V, double* H
     return rc;
 }
 
+// Device-resident timing of `reps` factorisations (k = 0 to m) with the
+// reference's Laplacian, each restarted from the same f0 (a device copy
+// inside the timed region): CUDA events on the legacy stream, ms total.
+// *h00 receives H(0,0) of the last factorisation (a consistency check).
+double ref_time_arnoldi_laplace(int n, int m, int reps, const double* f0, double* h00)
+{
+    cublasHandle_t handle;
+    if (cublasCreate(&handle) != CUBLAS_STATUS_SUCCESS) return -1.0;
+    Ax_struct ctx;
+    ctx.N = n;
+    const size_t nb = sizeof(double) * static_cast<size_t>(n);
+    double *V_d = nullptr, *f_d = nullptr, *f0_d = nullptr, *v_d = nullptr, *w_d = nullptr,
+           *c_d = nullptr, *h_d = nullptr;
+    if (cudaMalloc(&V_d, nb * m) != cudaSuccess) return -1.0;
+    cudaMalloc(&f_d, nb);
+    cudaMalloc(&f0_d, nb);
+    cudaMalloc(&v_d, nb);
+    cudaMalloc(&w_d, nb);
+    cudaMalloc(&c_d, sizeof(double) * m);
+    cudaMalloc(&h_d, sizeof(double) * m);
+    cudaMemset(V_d, 0, nb * m);
+    cudaMemcpy(f0_d, f0, nb, cudaMemcpyHostToDevice);
+    std::vector<double> H(static_cast<size_t>(m) * m, 0.0), vec_h(m, 0.0);
+    // one untimed factorisation (cuBLAS initialisation, first touches)
+    cudaMemcpy(f_d, f0_d, nb, cudaMemcpyDeviceToDevice);
+    Arnoldi_driver(handle, n, laplace_map, &ctx, V_d, H.data(), f_d, 0, m, v_d, w_d, c_d, h_d,
+                   vec_h.data());
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaDeviceSynchronize();
+    cudaEventRecord(a, 0);
+    for (int r = 0; r < reps; ++r) {
+        cudaMemcpyAsync(f_d, f0_d, nb, cudaMemcpyDeviceToDevice, 0);
+        Arnoldi_driver(handle, n, laplace_map, &ctx, V_d, H.data(), f_d, 0, m, v_d, w_d, c_d,
+                       h_d, vec_h.data());
+    }
+    cudaEventRecord(b, 0);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (h00) *h00 = H[0];
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(V_d);
+    cudaFree(f_d);
+    cudaFree(f0_d);
+    cudaFree(v_d);
+    cudaFree(w_d);
+    cudaFree(c_d);
+    cudaFree(h_d);
+    cublasDestroy(handle);
+    return cudaDeviceSynchronize() == cudaSuccess ? static_cast<double>(ms) : -1.0;
+}
+
 // The reference's 1-D periodic Laplacian applied once (for checking the
 // project's copy of the test operator).
 int ref_laplace_apply(int n, const double* in, double* out)
