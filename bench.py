@@ -7,6 +7,7 @@ dt from CFL 0.3 on the laminar peak velocity, FP64 throughout.  A "step" is
 one RK3_SSP step (3 right-hand sides).  The metric is RK3 steps/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--N 128]
+  python bench.py --workload arnoldi [--n-arnoldi 2300000] [--m-arnoldi 30] [...]
 
 --impl ours       : the CUDA library (libns3d_b200.so) through its C ABI.
 --impl reference  : the reference's own CUDA path (unmodified sources built
@@ -14,6 +15,14 @@ one RK3_SSP step (3 right-hand sides).  The metric is RK3 steps/s.
                     workload.
 Multi-GPU runs (torchrun) are independent replicas, one per GPU (the path
 does not shard); value = steps of all ranks / max elapsed over ranks.
+
+--workload arnoldi: one "step" is one Arnoldi factorisation (k = 0 to m,
+classical Gram-Schmidt with reorthogonalisation) with the reference's
+Krylov self-test operator, the 1-D periodic Laplacian of
+Source/Arnoldi/Matrix_Vector_emulator.cu at its test size n = 2,300,000,
+m = 30 (Source/Arnoldi/cuda_test.cu:63-70); the reference arm runs the
+reference's own Arnoldi_driver (cuBLAS) on the same operator and start
+vector.
 """
 from __future__ import annotations
 
@@ -45,6 +54,10 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
+    ap.add_argument("--workload", choices=["rk3", "arnoldi"], default="rk3",
+                    help="rk3: the RK3 step (default); arnoldi: the Krylov factorisation")
+    ap.add_argument("--n-arnoldi", type=int, default=2300000)
+    ap.add_argument("--m-arnoldi", type=int, default=30)
     return ap.parse_args()
 
 
@@ -187,6 +200,32 @@ def sizes(N):
 # CPU baseline: the oracle (numpy/scipy pocketfft) on the host cores
 # ---------------------------------------------------------------------------
 def cpu_baseline(N, Re, seed):
+    """The C++ / OpenMP restatement (oracle/cpu_rk3.cpp, all host threads) on
+    a bounded sample; the numpy/scipy oracle as a secondary figure."""
+    from oracle import cpu_lib
+
+    secondary = cpu_baseline_scipy(N, Re, seed)
+    if not cpu_lib.available():
+        return secondary
+    U, F, dt = workload(N, Re, seed)
+    with cpu_lib.CpuRK3(N, N, N) as C:
+        C.set_forcing(F)
+        t0 = time.perf_counter()
+        U = C.rk3_ssp(U, dt, Re, 1)  # warm-up (page faults, thread pool)
+        t1 = time.perf_counter()
+        k = max(5, min(200, int(15.0 / max(t1 - t0, 1e-3))))
+        t0 = time.perf_counter()
+        U = C.rk3_ssp(U, dt, Re, k)
+        el = time.perf_counter() - t0
+        threads = C.threads
+    return {"value": k / el, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"{k} RK3 steps of the {N}^3 Kolmogorov workload after 1 warm-up step, "
+                      f"{el:.1f} s (oracle/cpu_rk3.cpp: C++17 + OpenMP, project-written "
+                      f"mixed-radix FFT; FFTW is not installed)",
+            "secondary": secondary}
+
+
+def cpu_baseline_scipy(N, Re, seed):
     from oracle import ns3d_oracle as O
 
     cores = os.cpu_count() or 1
@@ -387,11 +426,199 @@ def run_reference(args, world, rank, local, pg):
     }
 
 
+# ---------------------------------------------------------------------------
+# Krylov workload: Arnoldi factorisations with the reference's self-test
+# operator (Source/Arnoldi/cuda_test.cu:63-70: N = 2,300,000, m = k*5 = 30)
+# ---------------------------------------------------------------------------
+def arnoldi_bytes(n, m):
+    """Gram-Schmidt bytes of one factorisation: the sum over columns of
+    4 (j+1) n 8 B (one classical pass plus one reorthogonalisation pass,
+    each reading V(:, 0..j) twice)."""
+    return sum(4 * (j + 1) * n * 8 for j in range(1, m))
+
+
+def arnoldi_start(n, seed):
+    import numpy as np
+
+    return np.random.default_rng(seed).standard_normal(n)
+
+
+def run_ours_arnoldi(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+
+    from ns3dperiodic_b200 import Krylov
+
+    n, m = args.n_arnoldi, args.m_arnoldi
+    f0 = arnoldi_start(n, args.seed + rank)
+    kr = Krylov(n, m)
+    A = kr.laplace_map()
+    V = torch.zeros((m, n), dtype=torch.float64, device="cuda")
+    H = np.zeros((m, m))
+    f0d = torch.as_tensor(f0, device="cuda")
+    f = f0d.clone()
+    for _ in range(args.warmup):
+        f.copy_(f0d)
+        kr.arnoldi(A, V, H, f, 0, m)
+    barrier(pg)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    s0 = torch.cuda.default_stream()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(s0)
+    st = None
+    for _ in range(args.steps):
+        f.copy_(f0d)
+        st = kr.arnoldi(A, V, H, f, 0, m)
+    ev1.record(s0)
+    ev1.synchronize()
+    ms_local = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    barrier(pg)
+    ms = max_over_ranks(ms_local, pg)
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+    peak, peak_src = peaks()
+    # dominant kernel: the dot products over all m columns (the widest launch)
+    pm = kr.profile(V, m, f0d, reps=20)
+    alg_t = (m + 1) * n * 8
+    achieved = alg_t / (pm[0] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "gemv_t_partial+reduce_cols",
+                "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_src,
+                "alg_bytes_per_launch": alg_t, "ms_per_launch": round(pm[0], 5),
+                "kernel_ms": {"dots": round(pm[0], 5), "update": round(pm[1], 5),
+                              "restart": round(pm[2], 5)},
+                "kernel_frac": {"dots": round(alg_t / (pm[0] * 1e-3) / 1e9 / peak, 4),
+                                "update": round((m + 2) * n * 8 / (pm[1] * 1e-3) / 1e9 / peak, 4),
+                                "restart": round((2 * m + 1) * n * 8 / (pm[2] * 1e-3) / 1e9
+                                                 / peak, 4)}}
+    # e2e: the start vector from pinned host memory each factorisation; H is
+    # assembled on the host column by column, as in the reference
+    K = args.e2e_steps or args.steps
+    hf = torch.from_numpy(f0).pin_memory()
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(K):
+        f.copy_(hf, non_blocking=True)
+        kr.arnoldi(A, V, H, f, 0, m)
+    torch.cuda.synchronize()
+    el = max_over_ranks(time.perf_counter() - t0, pg)
+    kr.close()
+    B = arnoldi_bytes(n, m)
+    return {
+        "metric": f"Arnoldi factorisations/s (1-D periodic Laplacian, n={n}, m={m}, FP64)",
+        "value": round(value, 3),
+        "unit": "factorisations/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"arnoldi_laplace1d_n{n}_m{m}", "n": n, "m": m,
+                   "operator": "Source/Arnoldi/Matrix_Vector_emulator.cu:10-36",
+                   "parallelism": f"replicas x{world}",
+                   "l2": f"basis {m * n * 8 / 1e6:.0f} MB > 126 MB L2",
+                   "gs_bytes_per_factorisation": B,
+                   "gs_gbs": round(B / (ms_step * 1e-3) / 1e9, 1),
+                   "gs_frac": round(B / (ms_step * 1e-3) / 1e9 / peak, 4),
+                   "max_reorth_passes": st["max_passes"], "H00": float(H[0, 0])},
+        "roofline": roofline,
+        "e2e": {"value": round(world * K / el, 3), "unit": "factorisations/s",
+                "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * m * (m + 2), "steps": K,
+                "protocol": "pinned host start vector -> device, ns3d_arnoldi (H to the host "
+                            "per column, as the reference); wall clock"},
+        # the driver's own launches plus one Laplacian launch per column
+        "gpu_launches": args.steps * (st["launches"] + m),
+        "clocks": clocks,
+    }
+
+
+def cpu_baseline_arnoldi(n, m, seed):
+    import numpy as np
+
+    from oracle import krylov_oracle as K
+
+    f = arnoldi_start(n, seed)
+    V, H = np.zeros((m, n)), np.zeros((m, m))
+    t0 = time.perf_counter()
+    K.arnoldi_driver(K.laplace1d, V, H, f.copy(), 0, m)
+    el = time.perf_counter() - t0
+    k = max(1, min(10, int(15.0 / max(el, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        K.arnoldi_driver(K.laplace1d, V, H, f.copy(), 0, m)
+    el = time.perf_counter() - t0
+    return {"value": k / el, "unit": "factorisations/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": f"{k} factorisations (oracle: numpy, BLAS threads as numpy configures "
+                      f"them) after 1 warm-up, {el:.1f} s"}
+
+
+def run_reference_arnoldi(args, world, rank, local, pg):
+    import ctypes
+
+    import numpy as np
+
+    if rank != 0:
+        return None
+    path = os.path.join(ROOT, "oracle", "_ref", "libarnoldi_ref.so")
+    if not os.path.exists(path):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libarnoldi_ref.so not built "
+                                                    "(needs the reference tree to compile)"}
+    lib = ctypes.CDLL(path)
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.ref_time_arnoldi_laplace.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
+    lib.ref_time_arnoldi_laplace.restype = ctypes.c_double
+    n, m = args.n_arnoldi, args.m_arnoldi
+    f0 = np.ascontiguousarray(arnoldi_start(n, args.seed))
+    h00 = np.zeros(1)
+    sampler = ClockSampler(local)
+    lib.ref_time_arnoldi_laplace(n, m, args.warmup, f0.ctypes.data_as(dp), h00.ctypes.data_as(dp))
+    sampler.start()
+    time.sleep(0.3)
+    ms = lib.ref_time_arnoldi_laplace(n, m, args.steps, f0.ctypes.data_as(dp),
+                                      h00.ctypes.data_as(dp))
+    clocks = sampler.stop()
+    if ms < 0:
+        return {"impl": "reference", "unavailable": "reference Arnoldi_driver run failed"}
+    value = args.steps / (ms / 1e3)
+    B = arnoldi_bytes(n, m)
+    return {"impl": "reference",
+            "metric": f"Arnoldi factorisations/s (1-D periodic Laplacian, n={n}, m={m}, FP64)",
+            "value": round(value, 3), "unit": "factorisations/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"arnoldi_laplace1d_n{n}_m{m}", "n": n, "m": m,
+                       "reference": "unmodified Source/Arnoldi/Arnoldi_Driver.cu with cuBLAS and "
+                                    "its user_Ax_function, sm_100a",
+                       "gs_gbs": round(B / (ms / args.steps * 1e-3) / 1e9, 1),
+                       "H00": float(h00[0])},
+            "e2e": {"value": round(value, 3), "unit": "factorisations/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": clocks}
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
     try:
-        if args.impl == "reference":
+        if args.workload == "arnoldi":
+            if args.impl == "reference":
+                line = run_reference_arnoldi(args, world, rank, local, pg)
+            else:
+                line = run_ours_arnoldi(args, world, rank, local, pg)
+                if rank == 0 and world == 1 and not args.no_cpu_baseline:
+                    line["cpu_baseline"] = cpu_baseline_arnoldi(args.n_arnoldi, args.m_arnoldi,
+                                                                args.seed)
+        elif args.impl == "reference":
             line = run_reference(args, world, rank, local, pg)
         else:
             line = run_ours(args, world, rank, local, pg)

@@ -314,8 +314,11 @@ ns3d_status ns3d_arnoldi(ns3d_krylov* kr, ns3d_user_map_vector Axb, void* user, 
                          double* H, double* f, int k, int m);
 
 /* Largest number of reorthogonalisation passes a column of the last
- * ns3d_arnoldi call took, and how many columns reached the pass limit. */
-ns3d_status ns3d_krylov_stats(const ns3d_krylov* kr, int* max_passes, int* limit_hits);
+ * ns3d_arnoldi call took, how many columns reached the pass limit, and how
+ * many kernels the driver itself launched (the map's launches not
+ * included).  Any output pointer may be null. */
+ns3d_status ns3d_krylov_stats(const ns3d_krylov* kr, int* max_passes, int* limit_hits,
+                              int64_t* launches);
 
 /* HOST ONLY (no GPU needed).  QR_shifts (Source/Arnoldi/QR_Shifts.cpp:46-72):
  * for j = m, m-1, ... while j > k, one shifted QR step of H with the shift
@@ -348,6 +351,31 @@ ns3d_status ns3d_ira_restart(ns3d_krylov* kr, double* V, double* f, double* Q, c
 ns3d_status ns3d_krylov_profile(ns3d_krylov* kr, const double* V, int ncols, const double* x,
                                 int reps, double* ms);
 
+/* BiCGStabL (Source/Arnoldi/BiCGStabL.cu:18-185): solves A x = rhs with
+ * BiCGStab(L), 1 <= L <= 16, x (device, length n) the initial guess on entry
+ * and the solution on exit, rhs (device) unchanged.  *tol and *iter are the
+ * reference's in/out arguments: the relative residual ||b - A x|| / ||b||
+ * to reach and the iteration cap on entry; the residual reached and the
+ * index of the last iteration on exit.  *flag receives the reference's
+ * outcome: 0 converged, 1 not converged, -1 rho = 0, -3 NaN.  Synchronous
+ * (one host read per inner product, as the reference). */
+ns3d_status ns3d_bicgstabl(ns3d_krylov* kr, int L, ns3d_user_map_vector Axb, void* user,
+                           double* x, const double* rhs, double* tol, int* iter, int* flag);
+
+/* Newton (Source/Arnoldi/Newton.cu:9-98): damped (0.8) Newton iteration for
+ * F(x) = 0 with BiCGStab(6) linear solves J delta = -F(x), delta starting
+ * from the reference's initial vector and carried between iterations.
+ * `residual` maps x to F(x) and, as the reference's NSCallRHS_reduced does,
+ * may record x as the point `jacobian` linearises about.  *tol: the residual
+ * norm to reach (on success it receives ||delta|| of the last step); *iter:
+ * the iteration cap on entry, the iterations run on exit.  *flag: 0
+ * converged, 1 not converged, 2 a linear solve failed with
+ * *linsolve_flag (the reference prints and exits there).  n >= 5. */
+ns3d_status ns3d_newton(ns3d_krylov* kr, ns3d_user_map_vector jacobian, void* jacobian_user,
+                        ns3d_user_map_vector residual, void* residual_user, double* x,
+                        double* tol, int* iter, double tol_linsolve, int iter_linsolve,
+                        int* flag, int* linsolve_flag);
+
 /* Built-in maps for ns3d_arnoldi.  Each finishes its work before returning
  * and, on failure, records the first non-OK status in `status` and fills
  * `out` with NaN so the driver stops with NS3D_ERR_NONFINITE. */
@@ -368,6 +396,13 @@ typedef struct ns3d_map_context {
  * reduced vectors: NSCallMatrixVector_reduced[_Newton_Globalization]
  * (Source/NS3D_periodic.cu:340-385) through ns3d_matvec_reduced. */
 void ns3d_map_linearised(void* user, void* in, void* out);
+
+/* user = ns3d_map_context*: NSCallRHS_reduced (Source/NS3D_periodic.cu:
+ * 415-441): in -> u (the context's base flow, reduced unpacking), out =
+ * RHS(u) = -P.Q(u) - |k|^2/Re u + f packed, with the context's v fields as
+ * scratch.  Setting u is what lets a linearised map sharing the same u
+ * serve as the Newton Jacobian. */
+void ns3d_map_rhs(void* user, void* in, void* out);
 
 /* user = ns3d_map_context*: in -> v (reduced unpacking), `steps` Heun tangent
  * steps of (u, v) with ns3d_jvp_steps, v -> out: NSCallMatrixVector_exponential

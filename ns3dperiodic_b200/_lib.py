@@ -35,7 +35,8 @@ EXPORTS = (
     "ns3d_tangent_euler_step",
     "ns3d_krylov_create", "ns3d_krylov_destroy", "ns3d_krylov_set_stream",
     "ns3d_krylov_last_error", "ns3d_arnoldi", "ns3d_krylov_stats", "ns3d_qr_shifts",
-    "ns3d_ira_restart", "ns3d_krylov_profile", "ns3d_map_linearised", "ns3d_map_exponential", "ns3d_map_laplace1d",
+    "ns3d_ira_restart", "ns3d_krylov_profile", "ns3d_bicgstabl", "ns3d_newton",
+    "ns3d_map_rhs", "ns3d_map_linearised", "ns3d_map_exponential", "ns3d_map_laplace1d",
 )
 
 # the matrix-vector callback type of ns3d_arnoldi: void (*)(void*, void*, void*)
@@ -118,10 +119,13 @@ def _sig(lib):
         "ns3d_krylov_set_stream": ([_P, _P], c_int),
         "ns3d_krylov_last_error": ([_P], ctypes.c_char_p),
         "ns3d_arnoldi": ([_P, _P, _P, _P, _P, _P, c_int, c_int], c_int),
-        "ns3d_krylov_stats": ([_P, _P, _P], c_int),
+        "ns3d_krylov_stats": ([_P, _P, _P, _P], c_int),
         "ns3d_qr_shifts": ([c_int, c_int, _P, _P, _P, _P, _P], c_int),
         "ns3d_ira_restart": ([_P, _P, _P, _P, _P, c_int, c_int, _P], c_int),
         "ns3d_krylov_profile": ([_P, _P, c_int, _P, c_int, _P], c_int),
+        "ns3d_bicgstabl": ([_P, c_int, _P, _P, _P, _P, _P, _P, _P], c_int),
+        "ns3d_newton": ([_P, _P, _P, _P, _P, _P, _P, _P, c_double, c_int, _P, _P], c_int),
+        "ns3d_map_rhs": ([_P, _P, _P], None),
         "ns3d_map_linearised": ([_P, _P, _P], None),
         "ns3d_map_exponential": ([_P, _P, _P], None),
         "ns3d_map_laplace1d": ([_P, _P, _P], None),

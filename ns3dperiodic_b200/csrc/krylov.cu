@@ -43,8 +43,12 @@ struct ns3d_krylov {
   double* small = nullptr;        // [0] norm, [1] ||c||, [2..2+m) h, [2+m..2+2m) c
   double* qcoef = nullptr;        // m_max * (m_max + 1): the Q columns used by a restart
   double* host = nullptr;         // pinned: mirror of `small` + staging of qcoef
+  double* lin = nullptr;          // BiCGStab(L) vectors: r[0..L], u[0..L], r~
+  int lin_L = 0;
+  double* newton = nullptr;       // Newton vectors: delta, -F(x)
   int max_passes = 0;
   int limit_hits = 0;
+  long long launches = 0;  // kernels the driver launched in its last call
   std::string err;
 };
 
@@ -57,6 +61,11 @@ constexpr int kRestartThreads = 128;
 constexpr int kMaxColumns = 200;        // restart row staging: m * 1 KB of shared memory
 constexpr double kReorthTol = 5.0e-12;  // Arnoldi_Driver.cu:31
 constexpr int kPassLimitIndex = 12;     // "if(it>12) break" after the pass
+
+int blocks_for(int64_t n, int threads, int cap) {
+  const int64_t b = (n + threads - 1) / threads;
+  return (int)(b < cap ? (b > 0 ? b : 1) : cap);
+}
 
 // ---------------------------------------------------------------------------
 // kernels
@@ -205,6 +214,125 @@ __global__ void __launch_bounds__(kRestartThreads) restart_rows(double* V, int64
   }
 }
 
+// Register-tiled form of restart_rows for k0 <= KMAX basis outputs: each
+// thread keeps the outputs of RR rows (2, or 1 for KMAX = 64) in registers,
+// streams its rows of V in chunks of 8 columns (coalesced across the warp)
+// and reads each coefficient, staged in shared memory, once per RR rows (a
+// broadcast).  The residual column Q(:, k0) has its own accumulator, so no
+// output is selected by a runtime index.
+template <int KMAX, int RR>
+__global__ void __launch_bounds__(kRestartThreads) restart_rows_reg(double* V, int64_t n, int m,
+                                                                    int k0,
+                                                                    const double* __restrict__ qc,
+                                                                    double hl, double ql,
+                                                                    double* f) {
+  // sq: Q(:, 0..k0-1) column-major, zero-padded to KMAX columns, then
+  // Q(:, k0); 8 words of zero padding after each part
+  extern __shared__ double sq[];
+  const int nb = m * KMAX + 8;
+  for (int i = threadIdx.x; i < nb + m + 8; i += kRestartThreads) {
+    double x = 0.0;
+    if (i < m * k0)
+      x = qc[i];
+    else if (i >= nb && i < nb + m)
+      x = qc[(size_t)k0 * m + (i - nb)];
+    sq[i] = x;
+  }
+  __syncthreads();
+  const double* sqf = sq + nb;
+  const int64_t stride = (int64_t)gridDim.x * kRestartThreads * RR;
+  for (int64_t r0 = (int64_t)blockIdx.x * kRestartThreads * RR + threadIdx.x; r0 < n;
+       r0 += stride) {
+    double acc[RR][KMAX];
+    double accf[RR];
+#pragma unroll
+    for (int rr = 0; rr < RR; ++rr) {
+      accf[rr] = 0.0;
+#pragma unroll
+      for (int j = 0; j < KMAX; ++j) acc[rr][j] = 0.0;
+    }
+#pragma unroll 1
+    for (int c0 = 0; c0 < m; c0 += 8) {
+      double v[RR][8];
+#pragma unroll
+      for (int rr = 0; rr < RR; ++rr) {
+        const int64_t r = r0 + (int64_t)rr * kRestartThreads;
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+          v[rr][t] = (r < n && c0 + t < m) ? V[(int64_t)(c0 + t) * n + r] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < KMAX; ++j) {
+        const double* q = sq + j * m + c0;  // entries past column j meet v = 0
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          const double qv = q[t];
+#pragma unroll
+          for (int rr = 0; rr < RR; ++rr) acc[rr][j] = fma(v[rr][t], qv, acc[rr][j]);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const double qv = sqf[c0 + t];
+#pragma unroll
+        for (int rr = 0; rr < RR; ++rr) accf[rr] = fma(v[rr][t], qv, accf[rr]);
+      }
+    }
+#pragma unroll
+    for (int rr = 0; rr < RR; ++rr) {
+      const int64_t r = r0 + (int64_t)rr * kRestartThreads;
+      if (r < n) {
+#pragma unroll
+        for (int j = 0; j < KMAX; ++j)
+          if (j < k0) V[(int64_t)j * n + r] = acc[rr][j];
+        f[r] = hl * accf[rr] + ql * f[r];
+      }
+    }
+  }
+}
+
+// Launches the restart pass for the basis columns 0..k0-1 and the residual.
+cudaError_t launch_restart(double* V, int64_t n, int m, int k0, const double* qc, double hl,
+                           double ql, double* f, cudaStream_t st) {
+  const int kmax = k0 <= 8 ? 8 : k0 <= 16 ? 16 : k0 <= 32 ? 32 : 64;
+  const size_t sq = sizeof(double) * ((size_t)m * kmax + 8 + m + 8);
+  const int b2 = blocks_for(n, kRestartThreads * 2, 148 * 8);
+  const int b1 = blocks_for(n, kRestartThreads, 148 * 8);
+  if (k0 <= 8)
+    restart_rows_reg<8, 2><<<b2, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f);
+  else if (k0 <= 16)
+    restart_rows_reg<16, 2><<<b2, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f);
+  else if (k0 <= 32)
+    restart_rows_reg<32, 2><<<b2, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f);
+  else if (k0 <= 64)
+    restart_rows_reg<64, 1><<<b1, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f);
+  else
+    restart_rows<<<b1, kRestartThreads, sizeof(double) * (size_t)m * kRestartThreads, st>>>(
+        V, n, m, k0, qc, hl, ql, f);
+  return cudaGetLastError();
+}
+
+// out = a x + b y (out may be y); b = 0 ignores y
+__global__ void __launch_bounds__(kThreads) axpby(int64_t n, double a, const double* x, double b,
+                                                  const double* y, double* out) {
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride)
+    out[i] = b == 0.0 ? a * x[i] : a * x[i] + b * y[i];
+}
+
+// zeros with 1.0, 1.5, 0.5, 1.0, 1.0 at 1, n/4, n/2, n-1, n-4
+// (set_initial_Krylov_vector_value_kernel, Source/Arnoldi/cuda_supp.cu:451-465)
+__global__ void __launch_bounds__(kThreads) newton_start(int64_t n, double* d) {
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+    double v = 0.0;
+    if (i == 1 || i == n - 1 || i == n - 4) v = 1.0;
+    if (i == n / 4) v = 1.5;
+    if (i == n / 2) v = 0.5;
+    d[i] = v;
+  }
+}
+
 // out_i = in_{i+1} - 2 in_i + in_{i-1} (periodic), out_0 = 0
 __global__ void __launch_bounds__(kThreads) laplace1d_kernel(const double* __restrict__ in,
                                                              double* __restrict__ out, int64_t n) {
@@ -241,10 +369,6 @@ ns3d_status kcuda(ns3d_krylov* kr, cudaError_t e, const char* where) {
   } while (0)
 #define KR_CHECK(kr, expr, where) KR_TRY(kcuda(kr, (expr), where))
 
-int blocks_for(int64_t n, int threads, int cap) {
-  const int64_t b = (n + threads - 1) / threads;
-  return (int)(b < cap ? (b > 0 ? b : 1) : cap);
-}
 
 ns3d_status enter(ns3d_krylov* kr) {
   if (!kr) return NS3D_ERR_BAD_ARG;
@@ -261,6 +385,7 @@ ns3d_status dots(ns3d_krylov* kr, const double* V, int ncols, const double* x, i
   KR_CHECK(kr, cudaGetLastError(), "gemv_t_partial");
   reduce_cols<<<1, kThreads, 0, kr->stream>>>(kr->part, nb, ncols, mode, out, acc, nrm);
   KR_CHECK(kr, cudaGetLastError(), "reduce_cols");
+  kr->launches += 2;
   return NS3D_OK;
 }
 
@@ -270,6 +395,7 @@ ns3d_status subtract(ns3d_krylov* kr, const double* V, int ncols, const double* 
   gemv_n_sub<<<nb, kThreads, sizeof(double) * ncols, kr->stream>>>(V, kr->n, ncols, c, y_in,
                                                                    y_out, kr->n);
   KR_CHECK(kr, cudaGetLastError(), "gemv_n_sub");
+  kr->launches += 1;
   return NS3D_OK;
 }
 
@@ -279,6 +405,7 @@ ns3d_status normalise_into(ns3d_krylov* kr, double* f, double* vcol) {
   scale_copy<<<blocks_for(kr->n, kThreads, kMaxBlocks * 2), kThreads, 0, kr->stream>>>(
       f, kr->small, kr->v, vcol, kr->n);
   KR_CHECK(kr, cudaGetLastError(), "scale_copy");
+  kr->launches += 1;
   return NS3D_OK;
 }
 
@@ -295,6 +422,150 @@ ns3d_status call_map(ns3d_krylov* kr, ns3d_user_map_vector Axb, void* user) {
   KR_CHECK(kr, cudaStreamSynchronize(kr->stream), "sync before map");
   Axb(user, kr->v, kr->w);
   KR_CHECK(kr, cudaGetLastError(), "matrix-vector map");
+  return NS3D_OK;
+}
+
+ns3d_status apply_map(ns3d_krylov* kr, ns3d_user_map_vector Axb, void* user, const double* in,
+                      double* out) {
+  KR_CHECK(kr, cudaStreamSynchronize(kr->stream), "sync before map");
+  Axb(user, const_cast<double*>(in), out);
+  KR_CHECK(kr, cudaGetLastError(), "matrix-vector map");
+  return NS3D_OK;
+}
+
+// out = a x + b y
+ns3d_status combine(ns3d_krylov* kr, double a, const double* x, double b, const double* y,
+                double* out) {
+  axpby<<<blocks_for(kr->n, kThreads, kMaxBlocks * 2), kThreads, 0, kr->stream>>>(kr->n, a, x, b,
+                                                                                y, out);
+  KR_CHECK(kr, cudaGetLastError(), "axpby");
+  kr->launches += 1;
+  return NS3D_OK;
+}
+
+// x . y, returned to the host (synchronous, like cublasDdot)
+ns3d_status dot(ns3d_krylov* kr, const double* x, const double* y, double* out) {
+  double* cd = kr->small + 2 + kr->m_max;
+  KR_TRY(dots(kr, x, 1, y, kStore, cd, nullptr, nullptr));
+  KR_CHECK(kr, cudaMemcpyAsync(kr->host, cd, sizeof(double), cudaMemcpyDeviceToHost, kr->stream),
+           "dot copy");
+  KR_CHECK(kr, cudaStreamSynchronize(kr->stream), "dot sync");
+  *out = kr->host[0];
+  return NS3D_OK;
+}
+
+ns3d_status norm2(ns3d_krylov* kr, const double* x, double* out) {
+  KR_TRY(dots(kr, x, 1, x, kNorm, kr->small, nullptr, nullptr));
+  KR_TRY(fetch(kr, 1));
+  *out = kr->host[0];
+  return NS3D_OK;
+}
+
+// BiCGStabL (Source/Arnoldi/BiCGStabL.cu:18-185) on the workspace's vectors.
+ns3d_status bicgstabl(ns3d_krylov* kr, int L, ns3d_user_map_vector Axb, void* user, double* x,
+                      const double* rhs, double* tol, int* iter, int* flag_out) {
+  const int64_t n = kr->n;
+  if (!kr->lin || kr->lin_L < L) {
+    cudaFree(kr->lin);
+    kr->lin = nullptr;
+    kr->lin_L = 0;
+    KR_CHECK(kr, cudaMalloc(&kr->lin, sizeof(double) * (size_t)(2 * L + 3) * n),
+             "BiCGStab(L) vectors");
+    kr->lin_L = L;
+  }
+  double* r0 = kr->lin;
+  double* u0 = kr->lin + (size_t)(L + 1) * n;
+  double* rt = kr->lin + (size_t)(2 * L + 2) * n;
+  auto r = [&](int i) { return r0 + (size_t)i * n; };
+  auto u = [&](int i) { return u0 + (size_t)i * n; };
+  KR_CHECK(kr, cudaMemsetAsync(kr->lin, 0, sizeof(double) * (size_t)(2 * L + 2) * n, kr->stream),
+           "BiCGStab(L) clear");
+  std::vector<double> tau((size_t)L * L, 0.0), sigma(L + 1, 0.0), gamma(L + 1, 0.0),
+      gamma_p(L + 1, 0.0), gamma_pp(L + 1, 0.0);
+  const double tl = *tol;
+  const int maxit = *iter;
+  int flag = 1, it = 0;
+  double error = 1.0, bnrm = 0.0, t = 0.0;
+  KR_TRY(norm2(kr, rhs, &bnrm));
+  if (bnrm < 1.0e-15) bnrm = 1.0;
+  // r0 = -(A x - b)
+  KR_TRY(apply_map(kr, Axb, user, x, r(0)));
+  KR_TRY(combine(kr, 1.0, r(0), -1.0, rhs, r(0)));
+  KR_TRY(combine(kr, -1.0, r(0), 0.0, nullptr, r(0)));
+  KR_TRY(norm2(kr, r(0), &t));
+  error = t / bnrm;
+  if (error < tl) flag = 0;
+  if (std::isnan(error)) flag = -3;
+  if (flag == 1) KR_TRY(combine(kr, 1.0 / t, r(0), 0.0, nullptr, rt));
+  double rho = 1.0, alpha = 0.0, omega = 1.0;
+  if (flag == 1) {
+    for (it = 0; it < maxit; ++it) {
+      rho = -omega * rho;
+      for (int j = 0; j < L; ++j) {
+        if (rho == 0.0) {
+          flag = -1;
+          rho = 1.0;
+        }
+        double rho1 = 0.0;
+        KR_TRY(dot(kr, r(j), rt, &rho1));
+        const double beta = alpha * rho1 / rho;
+        rho = rho1;
+        for (int i = 0; i <= j; ++i) KR_TRY(combine(kr, 1.0, r(i), -beta, u(i), u(i)));
+        KR_TRY(apply_map(kr, Axb, user, u(j), u(j + 1)));
+        double d = 0.0;
+        KR_TRY(dot(kr, u(j + 1), rt, &d));
+        alpha = rho / d;
+        for (int i = 0; i <= j; ++i) KR_TRY(combine(kr, -alpha, u(i + 1), 1.0, r(i), r(i)));
+        KR_TRY(apply_map(kr, Axb, user, r(j), r(j + 1)));
+        KR_TRY(combine(kr, alpha, u(0), 1.0, x, x));
+      }
+      for (int j = 1; j <= L; ++j) {
+        for (int i = 1; i < j; ++i) {
+          const int ij = (j - 1) * L + (i - 1);
+          double d = 0.0;
+          KR_TRY(dot(kr, r(j), r(i), &d));
+          tau[ij] = d / sigma[i];
+          KR_TRY(combine(kr, -tau[ij], r(i), 1.0, r(j), r(j)));
+        }
+        KR_TRY(dot(kr, r(j), r(j), &sigma[j]));
+        double d = 0.0;
+        KR_TRY(dot(kr, r(0), r(j), &d));
+        gamma_p[j] = d / sigma[j];
+      }
+      gamma[L] = gamma_p[L];
+      omega = gamma[L];
+      for (int j = L - 1; j >= 1; --j) {
+        gamma[j] = gamma_p[j];
+        for (int i = j + 1; i <= L; ++i) gamma[j] -= tau[(i - 1) * L + (j - 1)] * gamma[i];
+      }
+      for (int j = 1; j < L; ++j) {
+        gamma_pp[j] = gamma[j + 1];
+        for (int i = j + 1; i < L; ++i) gamma_pp[j] += tau[(i - 1) * L + (j - 1)] * gamma[i + 1];
+      }
+      KR_TRY(combine(kr, gamma[1], r(0), 1.0, x, x));
+      KR_TRY(combine(kr, -gamma_p[L], r(L), 1.0, r(0), r(0)));
+      KR_TRY(combine(kr, -gamma[L], u(L), 1.0, u(0), u(0)));
+      for (int j = 1; j < L; ++j) {
+        KR_TRY(combine(kr, gamma_pp[j], r(j), 1.0, x, x));
+        KR_TRY(combine(kr, -gamma_p[j], r(j), 1.0, r(0), r(0)));
+        KR_TRY(combine(kr, -gamma[j], u(j), 1.0, u(0), u(0)));
+      }
+      KR_TRY(norm2(kr, r(0), &t));
+      error = t / bnrm;
+      if (error < tl) {
+        flag = 0;
+        break;
+      }
+      if (error != error) {
+        flag = -3;
+        break;
+      }
+      if (flag < 0) break;
+    }
+  }
+  *iter = it;
+  *tol = error;
+  *flag_out = flag;
   return NS3D_OK;
 }
 
@@ -329,6 +600,20 @@ ns3d_status ns3d_krylov_create(int64_t n, int m_max, ns3d_krylov** out) {
     e = cudaFuncSetAttribute(restart_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
   }
+  if (e == cudaSuccess) {
+    const int sq = (int)(sizeof(double) * ((size_t)m_max * 64 + 8 + m_max + 8));
+    e = cudaFuncSetAttribute(restart_rows_reg<8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             sq);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(restart_rows_reg<16, 2>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, sq);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(restart_rows_reg<32, 2>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, sq);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(restart_rows_reg<64, 1>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, sq);
+  }
   if (e != cudaSuccess) {
     ns3d_krylov_destroy(kr);
     cudaGetLastError();
@@ -347,6 +632,8 @@ ns3d_status ns3d_krylov_destroy(ns3d_krylov* kr) {
   cudaFree(kr->part);
   cudaFree(kr->small);
   cudaFree(kr->qcoef);
+  cudaFree(kr->lin);
+  cudaFree(kr->newton);
   cudaFreeHost(kr->host);
   delete kr;
   return NS3D_OK;
@@ -362,10 +649,12 @@ const char* ns3d_krylov_last_error(const ns3d_krylov* kr) {
   return kr ? kr->err.c_str() : "null workspace";
 }
 
-ns3d_status ns3d_krylov_stats(const ns3d_krylov* kr, int* max_passes, int* limit_hits) {
+ns3d_status ns3d_krylov_stats(const ns3d_krylov* kr, int* max_passes, int* limit_hits,
+                              int64_t* launches) {
   if (!kr) return NS3D_ERR_BAD_ARG;
   if (max_passes) *max_passes = kr->max_passes;
   if (limit_hits) *limit_hits = kr->limit_hits;
+  if (launches) *launches = kr->launches;
   return NS3D_OK;
 }
 
@@ -377,6 +666,7 @@ ns3d_status ns3d_arnoldi(ns3d_krylov* kr, ns3d_user_map_vector Axb, void* user, 
     return kfail(kr, NS3D_ERR_BAD_ARG, "need 0 <= k < m <= m_max and m >= 2");
   kr->max_passes = 0;
   kr->limit_hits = 0;
+  kr->launches = 0;
   const int64_t n = kr->n;
   double* hd = kr->small + 2;      // h on the device
   double* cd = kr->small + 2 + m;  // c on the device (k == 0 uses cd[0] as the scalar)
@@ -467,10 +757,8 @@ ns3d_status ns3d_ira_restart(ns3d_krylov* kr, double* V, double* f, double* Q, c
   KR_CHECK(kr, cudaMemcpyAsync(kr->qcoef, staged, sizeof(double) * nq, cudaMemcpyHostToDevice,
                                kr->stream), "Q upload");
   KR_TRY(dots(kr, f, 1, f, kNorm, kr->small, nullptr, nullptr));
-  const size_t smem = sizeof(double) * (size_t)m * kRestartThreads;
-  restart_rows<<<blocks_for(kr->n, kRestartThreads, 148 * 8), kRestartThreads, smem,
-                 kr->stream>>>(V, kr->n, m, k0, kr->qcoef, hl, ql, f);
-  KR_CHECK(kr, cudaGetLastError(), "restart_rows");
+  KR_CHECK(kr, launch_restart(V, kr->n, m, k0, kr->qcoef, hl, ql, f, kr->stream),
+           "restart_rows");
   KR_TRY(fetch(kr, 1));
   if (f_norm) *f_norm = kr->host[0];
   for (int j = k0; j < m; ++j)
@@ -504,11 +792,9 @@ ns3d_status ns3d_krylov_profile(ns3d_krylov* kr, const double* V, int ncols, con
       } else if (which == 1) {
         KR_TRY(subtract(kr, V, ncols, cd, x, kr->w));
       } else {
-        const size_t smem = sizeof(double) * (size_t)ncols * kRestartThreads;
-        restart_rows<<<blocks_for(kr->n, kRestartThreads, 148 * 8), kRestartThreads, smem,
-                       kr->stream>>>(const_cast<double*>(V), kr->n, ncols, k0, kr->qcoef, 0.0,
-                                     1.0, kr->w);
-        KR_CHECK(kr, cudaGetLastError(), "restart_rows");
+        KR_CHECK(kr, launch_restart(const_cast<double*>(V), kr->n, ncols, k0, kr->qcoef, 0.0,
+                                    1.0, kr->w, kr->stream),
+                 "restart_rows");
       }
     }
     cudaEventRecord(e1, kr->stream);
@@ -519,6 +805,71 @@ ns3d_status ns3d_krylov_profile(ns3d_krylov* kr, const double* V, int ncols, con
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_bicgstabl(ns3d_krylov* kr, int L, ns3d_user_map_vector Axb, void* user,
+                           double* x, const double* rhs, double* tol, int* iter, int* flag) {
+  KR_TRY(enter(kr));
+  if (!Axb || !x || !rhs || !tol || !iter || !flag || L < 1 || L > 16 || *iter < 0)
+    return kfail(kr, NS3D_ERR_BAD_ARG, "need 1 <= L <= 16, non-null pointers, *iter >= 0");
+  kr->launches = 0;
+  return bicgstabl(kr, L, Axb, user, x, rhs, tol, iter, flag);
+}
+
+ns3d_status ns3d_newton(ns3d_krylov* kr, ns3d_user_map_vector jacobian, void* jacobian_user,
+                        ns3d_user_map_vector residual, void* residual_user, double* x,
+                        double* tol, int* iter, double tol_linsolve, int iter_linsolve,
+                        int* flag, int* linsolve_flag) {
+  KR_TRY(enter(kr));
+  if (!jacobian || !residual || !x || !tol || !iter || !flag || !linsolve_flag || *iter < 0 ||
+      kr->n < 5)
+    return kfail(kr, NS3D_ERR_BAD_ARG, "need non-null maps and pointers, *iter >= 0, n >= 5");
+  const int64_t n = kr->n;
+  kr->launches = 0;
+  if (!kr->newton)
+    KR_CHECK(kr, cudaMalloc(&kr->newton, sizeof(double) * 2 * (size_t)n), "Newton vectors");
+  double* delta = kr->newton;
+  double* bn = kr->newton + n;
+  newton_start<<<blocks_for(n, kThreads, kMaxBlocks * 2), kThreads, 0, kr->stream>>>(n, delta);
+  KR_CHECK(kr, cudaGetLastError(), "newton_start");
+  constexpr double kDamping = 0.8;  // Newton.cu:66
+  constexpr int kL = 6;             // Newton.cu:21
+  *linsolve_flag = 0;
+  int fl = 1, ll = 0;
+  double norm_rhs = 0.0;
+  KR_TRY(apply_map(kr, residual, residual_user, x, bn));
+  KR_TRY(norm2(kr, bn, &norm_rhs));
+  if (norm_rhs < *tol) {
+    fl = 0;
+  } else {
+    for (ll = 0; ll < *iter; ++ll) {
+      double tol_b = tol_linsolve;
+      int it_b = iter_linsolve, lf = 0;
+      KR_TRY(apply_map(kr, residual, residual_user, x, bn));
+      KR_TRY(combine(kr, -1.0, bn, 0.0, nullptr, bn));
+      KR_TRY(bicgstabl(kr, kL, jacobian, jacobian_user, delta, bn, &tol_b, &it_b, &lf));
+      if (lf != 0) {  // the reference prints and exits here
+        *linsolve_flag = lf;
+        *iter = ll;
+        *flag = 2;
+        return NS3D_OK;
+      }
+      KR_TRY(combine(kr, kDamping, delta, 1.0, x, x));
+      double tol_newton = 0.0;
+      KR_TRY(norm2(kr, delta, &tol_newton));
+      KR_TRY(norm2(kr, bn, &norm_rhs));
+      if (!std::isfinite(tol_newton) || !std::isfinite(norm_rhs))
+        return kfail(kr, NS3D_ERR_NONFINITE, "Newton update is not finite");
+      if (norm_rhs < *tol && ll > 2) {
+        *tol = tol_newton;
+        fl = 0;
+        break;
+      }
+    }
+  }
+  *iter = ll;
+  *flag = fl;
   return NS3D_OK;
 }
 
@@ -537,6 +888,21 @@ void ns3d_map_linearised(void* user, void* in, void* out) {
   ns3d_status s = ns3d_matvec_reduced(c->solver, c->ux, c->uy, c->uz,
                                       static_cast<const double*>(in), static_cast<double*>(out),
                                       c->Re, c->tau);
+  if (s == NS3D_OK) s = ns3d_synchronize(c->solver);
+  if (s != NS3D_OK) {
+    if (c->status == NS3D_OK) c->status = s;
+    map_poison(c, static_cast<double*>(out));
+  }
+}
+
+void ns3d_map_rhs(void* user, void* in, void* out) {
+  ns3d_map_context* c = static_cast<ns3d_map_context*>(user);
+  if (!c) return;
+  ns3d_status s = ns3d_unpack_reduced(c->solver, static_cast<const double*>(in), c->ux, c->uy,
+                                      c->uz);
+  if (s == NS3D_OK) s = ns3d_rhs(c->solver, c->ux, c->uy, c->uz, c->vx, c->vy, c->vz, c->Re);
+  if (s == NS3D_OK)
+    s = ns3d_pack_reduced(c->solver, c->vx, c->vy, c->vz, static_cast<double*>(out));
   if (s == NS3D_OK) s = ns3d_synchronize(c->solver);
   if (s != NS3D_OK) {
     if (c->status == NS3D_OK) c->status = s;

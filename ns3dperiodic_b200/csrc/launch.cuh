@@ -32,6 +32,11 @@ constexpr int p_z(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PZ); }
 constexpr int p_fx(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PFX); }
 // the tangent z pass keeps u, v and the three products live: fewer points
 constexpr int p_zuv(int n) { return n % 3 == 0 ? 6 : 4; }
+// points per thread of the plain line passes (8 measured slower than 16 at 256^3 and 512^3)
+#ifndef NS3D_PLINE
+#define NS3D_PLINE 16
+#endif
+constexpr int p_line(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PLINE); }
 
 inline bool extent_supported_inline(int n) {
   switch (n) {
@@ -193,7 +198,7 @@ cudaError_t launch_line(const LineArgs& a, const PassGeom& g, cudaStream_t st,
   switch (AXIS == 0 ? g.Nx : g.Ny) {
 #define NS3D_CASE(N)                                                                    \
   case N: {                                                                             \
-    constexpr int P = p_xy(N);                                                          \
+    constexpr int P = p_line(N);                                                           \
     using S = PassSmem<N, P>;                                                           \
     const unsigned grid = persistent_grid<KTag<30 + 2 * AXIS + (DIR > 0 ? 1 : 0), N, P, 0>>( \
         line_kernel<N, P, AXIS, DIR>, S::BYTES, (lines + S::LPC - 1) / S::LPC);         \

@@ -180,6 +180,50 @@ class Krylov:
         return Map(ctypes.cast(self._L.ns3d_map_exponential, ctypes.c_void_p).value, ctx,
                    keep=(U, Vscratch))
 
+    def rhs_map(self, solver, U, Vscratch, Re: float) -> Map:
+        """F(x) = RHS(unpack(x)) packed, writing unpack(x) into U first
+        (ns3d_map_rhs, as NSCallRHS_reduced): a linearised_map on the same U
+        is then the Jacobian at x."""
+        p = solver._fields(U, "U")
+        q = solver._fields(Vscratch, "V")
+        ctx = MapContext(solver._h.value, p[0], p[1], p[2], q[0], q[1], q[2], 0.0, float(Re),
+                         0.0, 0, 0)
+        return Map(ctypes.cast(self._L.ns3d_map_rhs, ctypes.c_void_p).value, ctx,
+                   keep=(U, Vscratch))
+
+    @staticmethod
+    def _fnptr(A: Map) -> int:
+        return A.fn if isinstance(A.fn, int) else ctypes.cast(A.fn, ctypes.c_void_p).value
+
+    def bicgstabl(self, A: Map, x, rhs, L: int = 6, tol: float = 1e-9, maxiter: int = 1000):
+        """BiCGStabL: solves A x = rhs in place (x: initial guess).  Returns
+        (flag, iterations, relative residual) as the reference reports them."""
+        self._vector(x)
+        self._vector(rhs)
+        t, it, fl = ctypes.c_double(tol), ctypes.c_int(maxiter), ctypes.c_int(0)
+        self._check(self._L.ns3d_bicgstabl(self._h, int(L), ctypes.c_void_p(self._fnptr(A)),
+                                           ctypes.c_void_p(A.ctx_ptr()),
+                                           ctypes.c_void_p(x.data_ptr()),
+                                           ctypes.c_void_p(rhs.data_ptr()), ctypes.byref(t),
+                                           ctypes.byref(it), ctypes.byref(fl)), "ns3d_bicgstabl")
+        return fl.value, it.value, t.value
+
+    def newton(self, jacobian: Map, residual: Map, x, tol: float = 5e-7, maxiter: int = 1000,
+               tol_linsolve: float = 1e-9, iter_linsolve: int = 1000) -> dict:
+        """Newton: damped Newton iteration for residual(x) = 0, x in place."""
+        self._vector(x)
+        t, it = ctypes.c_double(tol), ctypes.c_int(maxiter)
+        fl, lf = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(self._L.ns3d_newton(self._h, ctypes.c_void_p(self._fnptr(jacobian)),
+                                        ctypes.c_void_p(jacobian.ctx_ptr()),
+                                        ctypes.c_void_p(self._fnptr(residual)),
+                                        ctypes.c_void_p(residual.ctx_ptr()),
+                                        ctypes.c_void_p(x.data_ptr()), ctypes.byref(t),
+                                        ctypes.byref(it), float(tol_linsolve), int(iter_linsolve),
+                                        ctypes.byref(fl), ctypes.byref(lf)), "ns3d_newton")
+        return {"flag": fl.value, "iterations": it.value, "tol": t.value,
+                "linsolve_flag": lf.value}
+
     def _basis(self, V, m: int):
         torch = self._torch
         if (not isinstance(V, torch.Tensor) or V.dtype != torch.float64
@@ -201,15 +245,15 @@ class Krylov:
         self._basis(V, m)
         self._vector(f)
         Hf = np.asfortranarray(H[:m, :m], dtype=np.float64)
-        fn = A.fn if isinstance(A.fn, int) else ctypes.cast(A.fn, ctypes.c_void_p).value
+        fn = self._fnptr(A)
         rc = self._L.ns3d_arnoldi(self._h, ctypes.c_void_p(fn), ctypes.c_void_p(A.ctx_ptr()),
                                   ctypes.c_void_p(V.data_ptr()), Hf.ctypes.data,
                                   ctypes.c_void_p(f.data_ptr()), int(k), int(m))
         H[:m, :m] = Hf
         self._check(rc, "ns3d_arnoldi")
-        mp, lh = ctypes.c_int(0), ctypes.c_int(0)
-        self._L.ns3d_krylov_stats(self._h, ctypes.byref(mp), ctypes.byref(lh))
-        return {"max_passes": mp.value, "limit_hits": lh.value}
+        mp, lh, nl = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int64(0)
+        self._L.ns3d_krylov_stats(self._h, ctypes.byref(mp), ctypes.byref(lh), ctypes.byref(nl))
+        return {"max_passes": mp.value, "limit_hits": lh.value, "launches": nl.value}
 
     def ira_restart(self, V, f, Q: np.ndarray, H: np.ndarray, k0: int) -> float:
         """Restart update f = hl V q + ql f, V = V Q; Q's columns k0.. are

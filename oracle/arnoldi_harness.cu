@@ -1,7 +1,7 @@
 // Harness around the reference's own Krylov code (TEST INFRASTRUCTURE).
 //
 // oracle/Makefile compiles the reference's Source/Arnoldi/{Arnoldi_Driver.cu,
-// cuda_supp.cu, memory_operations.cu, Matrix_Vector_emulator.cu,
+// BiCGStabL.cu, Newton.cu, cuda_supp.cu, memory_operations.cu, Matrix_Vector_emulator.cu,
 // Products.cpp, QR_Shifts.cpp, Select_Shifts.cpp, LAPACK_routines.cpp}
 // unmodified (with oracle/c99_complex_prelude.h force-included) together with
 // this file into oracle/_ref/libarnoldi_ref.so.  This file adds only:
@@ -16,6 +16,8 @@
 // Arnoldi_driver needs a GPU; the QR-shift and shift-selection entry points
 // are host code and run anywhere the library loads.
 #include "Arnoldi_Driver.h"
+#include "BiCGStabL.h"
+#include "Newton.h"
 #include "QR_Shifts.h"
 #include "Select_Shifts.h"
 #include "Matrix_Vector_emulator.h"
@@ -199,6 +201,117 @@ double ref_time_arnoldi_laplace(int n, int m, int reps, const double* f0, double
     cudaFree(h_d);
     cublasDestroy(handle);
     return cudaDeviceSynchronize() == cudaSuccess ? static_cast<double>(ms) : -1.0;
+}
+
+// BiCGStabL (Source/Arnoldi/BiCGStabL.cu:18-185) on A x = rhs with a dense
+// column-major A; x is the initial guess on entry and the result on exit,
+// *tol / *iter are the reference's in/out arguments.  Returns its flag.
+int ref_bicgstabl_dense(int n, int L, const double* A, double* x, const double* rhs,
+                        double* tol, int* iter)
+{
+    cublasHandle_t handle;
+    if (cublasCreate(&handle) != CUBLAS_STATUS_SUCCESS) return 99;
+    DenseMap ctx;
+    ctx.handle = handle;
+    ctx.n = n;
+    const size_t nb = sizeof(double) * static_cast<size_t>(n);
+    double *x_d = nullptr, *b_d = nullptr;
+    cudaMalloc(&ctx.A, nb * n);
+    cudaMalloc(&x_d, nb);
+    cudaMalloc(&b_d, nb);
+    cudaMemcpy(ctx.A, A, nb * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(x_d, x, nb, cudaMemcpyHostToDevice);
+    cudaMemcpy(b_d, rhs, nb, cudaMemcpyHostToDevice);
+    const int flag = BiCGStabL(handle, L, n, dense_map, &ctx, x_d, b_d, tol, iter, false, 1000);
+    cudaMemcpy(x, x_d, nb, cudaMemcpyDeviceToHost);
+    cudaFree(ctx.A);
+    cudaFree(x_d);
+    cudaFree(b_d);
+    cublasDestroy(handle);
+    return cudaDeviceSynchronize() == cudaSuccess ? flag : 98;
+}
+
+// The nonlinear test problem of the Newton golden vectors:
+//   F(x) = A x + c x^3 - b (elementwise cube),  J(x) v = A v + 3 c x^2 v.
+// As with the reference's own NSCallRHS_reduced / Jacobian pair, the
+// residual map stores its argument as the point the Jacobian map linearises
+// about.
+struct CubicMap {
+    cublasHandle_t handle;
+    int n;
+    double* A;     // column-major n x n
+    double* b;
+    double* base;  // the point of the last residual evaluation
+    double c;
+};
+
+__global__ void cubic_rhs_tail(int n, double c, const double* x, const double* b, double* out,
+                               double* base)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const double xi = x[i];
+        base[i] = xi;
+        out[i] = out[i] + c * xi * xi * xi - b[i];
+    }
+}
+
+__global__ void cubic_jac_tail(int n, double c, const double* v, const double* base, double* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = out[i] + 3.0 * c * base[i] * base[i] * v[i];
+}
+
+void cubic_rhs(void* ctx, void* in, void* out)
+{
+    CubicMap* m = static_cast<CubicMap*>(ctx);
+    const double one = 1.0, zero = 0.0;
+    cublasDgemv(m->handle, CUBLAS_OP_N, m->n, m->n, &one, m->A, m->n,
+                static_cast<double*>(in), 1, &zero, static_cast<double*>(out), 1);
+    cubic_rhs_tail<<<(m->n + 255) / 256, 256>>>(m->n, m->c, static_cast<double*>(in), m->b,
+                                                static_cast<double*>(out), m->base);
+}
+
+void cubic_jac(void* ctx, void* in, void* out)
+{
+    CubicMap* m = static_cast<CubicMap*>(ctx);
+    const double one = 1.0, zero = 0.0;
+    cublasDgemv(m->handle, CUBLAS_OP_N, m->n, m->n, &one, m->A, m->n,
+                static_cast<double*>(in), 1, &zero, static_cast<double*>(out), 1);
+    cubic_jac_tail<<<(m->n + 255) / 256, 256>>>(m->n, m->c, static_cast<double*>(in), m->base,
+                                                static_cast<double*>(out));
+}
+
+// Newton (Source/Arnoldi/Newton.cu:9-98) on the cubic problem above; x is
+// the initial guess on entry, the result on exit.  Returns its flag.
+int ref_newton_cubic(int n, const double* A, const double* b, double c, double* x, double* tol,
+                     int* iter, double tol_lin, int iter_lin)
+{
+    cublasHandle_t handle;
+    if (cublasCreate(&handle) != CUBLAS_STATUS_SUCCESS) return 99;
+    CubicMap m;
+    m.handle = handle;
+    m.n = n;
+    m.c = c;
+    const size_t nb = sizeof(double) * static_cast<size_t>(n);
+    double* x_d = nullptr;
+    cudaMalloc(&m.A, nb * n);
+    cudaMalloc(&m.b, nb);
+    cudaMalloc(&m.base, nb);
+    cudaMalloc(&x_d, nb);
+    cudaMemcpy(m.A, A, nb * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(m.b, b, nb, cudaMemcpyHostToDevice);
+    cudaMemcpy(x_d, x, nb, cudaMemcpyHostToDevice);
+    cudaMemset(m.base, 0, nb);
+    const int flag = Newton(handle, cubic_jac, &m, cubic_rhs, &m, n, x_d, tol, iter, tol_lin,
+                            iter_lin, false, 100);
+    cudaMemcpy(x, x_d, nb, cudaMemcpyDeviceToHost);
+    cudaFree(m.A);
+    cudaFree(m.b);
+    cudaFree(m.base);
+    cudaFree(x_d);
+    cublasDestroy(handle);
+    return cudaDeviceSynchronize() == cudaSuccess ? flag : 98;
 }
 
 // The reference's 1-D periodic Laplacian applied once (for checking the

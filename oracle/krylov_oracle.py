@@ -194,3 +194,132 @@ def arnoldi_residual(Axb, V: np.ndarray, H: np.ndarray, f: np.ndarray, m: int) -
     R = AV - VH
     R[m - 1] -= f
     return float(np.abs(R).max() / max(np.abs(H).max(), 1.0))
+
+
+# ---------------------------------------------------------------------------
+# BiCGStab(L) and damped Newton (Source/Arnoldi/BiCGStabL.cu, Newton.cu)
+# ---------------------------------------------------------------------------
+
+def bicgstabl(Axb, x: np.ndarray, rhs: np.ndarray, L: int, tol: float, maxiter: int):
+    """BiCGStabL (BiCGStabL.cu:18-185), x updated in place.
+
+    Returns (flag, iterations, error) with the reference's flags: 0
+    converged, 1 not converged, -1 rho = 0, -3 NaN; ``error`` is
+    ||r||/||b|| and ``iterations`` the index of the last iteration run."""
+    n = x.size
+    r = [np.zeros(n) for _ in range(L + 1)]
+    u = [np.zeros(n) for _ in range(L + 1)]
+    tau = np.zeros(L * L)
+    sigma = np.zeros(L + 1)
+    gamma = np.zeros(L + 1)
+    gamma_p = np.zeros(L + 1)
+    gamma_pp = np.zeros(L + 1)
+    flag = 1
+    bnrm = float(np.sqrt(np.dot(rhs, rhs)))
+    if bnrm < 1.0e-15:
+        bnrm = 1.0
+    r[0] = -(Axb(x) - rhs)                        # get_residualL: A x - b, then negated
+    error = float(np.sqrt(np.dot(r[0], r[0]))) / bnrm
+    if error < tol:
+        flag = 0
+    if np.isnan(error):
+        flag = -3
+    rt = r[0] * (1.0 / float(np.sqrt(np.dot(r[0], r[0])))) if flag == 1 else r[0].copy()
+    rho, alpha, omega = 1.0, 0.0, 1.0
+    it = 0
+    if flag == 1:
+        for it in range(maxiter):
+            rho = -omega * rho
+            for j in range(L):
+                if rho == 0.0:
+                    flag = -1
+                    rho = 1.0
+                rho1 = float(np.dot(r[j], rt))
+                beta = alpha * rho1 / rho
+                rho = rho1
+                for i in range(j + 1):
+                    u[i] = r[i] - beta * u[i]
+                u[j + 1] = Axb(u[j])
+                alpha = rho / float(np.dot(u[j + 1], rt))
+                for i in range(j + 1):
+                    r[i] = r[i] - alpha * u[i + 1]
+                r[j + 1] = Axb(r[j])
+                x += alpha * u[0]
+            for j in range(1, L + 1):
+                for i in range(1, j):
+                    ij = (j - 1) * L + (i - 1)
+                    tau[ij] = float(np.dot(r[j], r[i])) / sigma[i]
+                    r[j] = r[j] - tau[ij] * r[i]
+                sigma[j] = float(np.dot(r[j], r[j]))
+                gamma_p[j] = float(np.dot(r[0], r[j])) / sigma[j]
+            gamma[L] = gamma_p[L]
+            omega = gamma[L]
+            for j in range(L - 1, 0, -1):
+                gamma[j] = gamma_p[j]
+                for i in range(j + 1, L + 1):
+                    gamma[j] -= tau[(i - 1) * L + (j - 1)] * gamma[i]
+            for j in range(1, L):
+                gamma_pp[j] = gamma[j + 1]
+                for i in range(j + 1, L):
+                    gamma_pp[j] += tau[(i - 1) * L + (j - 1)] * gamma[i + 1]
+            x += gamma[1] * r[0]
+            r[0] = r[0] - gamma_p[L] * r[L]
+            u[0] = u[0] - gamma[L] * u[L]
+            for j in range(1, L):
+                x += gamma_pp[j] * r[j]
+                r[0] = r[0] - gamma_p[j] * r[j]
+                u[0] = u[0] - gamma[j] * u[j]
+            error = float(np.sqrt(np.dot(r[0], r[0]))) / bnrm
+            if error < tol:
+                flag = 0
+                break
+            if error != error:
+                flag = -3
+                break
+            if flag < 0:
+                break
+        else:
+            it = maxiter
+    return flag, it, error
+
+
+def newton_initial_vector(n: int) -> np.ndarray:
+    """set_initial_Krylov_vector_value_kernel (Arnoldi/cuda_supp.cu:451-465):
+    zeros with 1.0, 1.5, 0.5, 1.0, 1.0 at indices 1, n/4, n/2, n-1, n-4 (every
+    thread stores the fixed entries after its own zero, so the result is
+    deterministic)."""
+    d = np.zeros(n)
+    d[1] = 1.0
+    d[n // 4] = 1.5
+    d[n // 2] = 0.5
+    d[n - 1] = 1.0
+    d[n - 4] = 1.0
+    return d
+
+
+def newton(jacobian, rhs_map, x: np.ndarray, tol: float, maxiter: int, tol_lin: float,
+           iter_lin: int, L: int = 6, damping: float = 0.8):
+    """Newton (Newton.cu:9-98), x updated in place.  ``rhs_map(x)`` returns
+    F(x) and may record x as the point ``jacobian`` linearises about, as the
+    reference's NSCallRHS_reduced does.  Returns (flag, iterations, tol_out,
+    linsolve_flag): flag 0 converged, 1 not converged, 2 the linear solve
+    failed (the reference exits there)."""
+    n = x.size
+    delta = newton_initial_vector(n)
+    flag, ll, tol_out, lflag = 1, 0, tol, 0
+    bn = rhs_map(x)
+    if float(np.sqrt(np.dot(bn, bn))) < tol:
+        return 0, 0, tol, 0
+    for ll in range(maxiter):
+        bn = -rhs_map(x)
+        lflag, _, _ = bicgstabl(jacobian, delta, bn, L, tol_lin, iter_lin)
+        if lflag != 0:
+            return 2, ll, tol_out, lflag
+        x += damping * delta
+        tol_newton = float(np.sqrt(np.dot(delta, delta)))
+        norm_rhs = float(np.sqrt(np.dot(bn, bn)))
+        if norm_rhs < tol and ll > 2:
+            return 0, ll, tol_newton, 0
+    else:
+        ll = maxiter
+    return flag, ll, tol_out, lflag

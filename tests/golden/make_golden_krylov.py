@@ -16,8 +16,12 @@ Made with:
 
     make -C oracle && python tests/golden/make_golden_krylov.py --out tests/golden
 
+* ``krylov_linsolve.npz`` BiCGStabL (L = 1, 2, 6) on a seeded dense system and
+                        Newton on a seeded cubic problem F(x) = A x + c x^3 - b
+                        (cuBLAS, needs a GPU).
+
 (``--host-only`` writes only krylov_qr.npz, without a GPU; ``--arnoldi-only``
-writes only krylov_arnoldi.npz.)
+writes only krylov_arnoldi.npz; ``--linsolve-only`` only krylov_linsolve.npz.)
 """
 from __future__ import annotations
 
@@ -153,11 +157,52 @@ def make_arnoldi(lib) -> dict:
     return out
 
 
+def linsolve_matrix(n: int, seed: int, diag: float, scale: float) -> np.ndarray:
+    """Seeded non-symmetric matrix diag*I + scale*N(0,1)/sqrt(n)."""
+    rng = np.random.default_rng(seed)
+    return diag * np.eye(n) + scale * rng.standard_normal((n, n)) / np.sqrt(n)
+
+
+BICG_CASES = [(300, L, 41) for L in (1, 2, 6)]  # (n, L, seed): tol 1e-10, 200 iterations
+NEWTON_CASE = (200, 42, 0.1)                     # (n, seed, c): tol 1e-9, 60 iterations
+
+
+def make_linsolve(lib) -> dict:
+    out = {}
+    for idx, (n, L, seed) in enumerate(BICG_CASES):
+        A = np.asfortranarray(linsolve_matrix(n, seed, 2.0, 0.5))
+        b = np.random.default_rng(seed + 1).standard_normal(n)
+        x = np.zeros(n)
+        tol = np.array([1e-10])
+        it = ctypes.c_int(200)
+        flag = lib.ref_bicgstabl_dense(n, L, _p(A), _p(x), _p(b), _p(tol), ctypes.byref(it))
+        assert flag == 0, flag
+        pre = f"bicg{idx}_"
+        out[pre + "b"] = b
+        out[pre + "x"] = x
+        out[pre + "meta"] = np.array([n, L, seed, flag, it.value])
+        out[pre + "err"] = tol
+    n, seed, c = NEWTON_CASE
+    A = np.asfortranarray(linsolve_matrix(n, seed, 3.0, 0.3))
+    b = np.random.default_rng(seed + 1).standard_normal(n)
+    x = np.zeros(n)
+    tol = np.array([1e-9])
+    it = ctypes.c_int(60)
+    flag = lib.ref_newton_cubic(n, _p(A), _p(b), c, _p(x), _p(tol), ctypes.byref(it), 1e-11, 200)
+    assert flag == 0, flag
+    out["newton_b"] = b
+    out["newton_x"] = x
+    out["newton_meta"] = np.array([n, seed, flag, it.value])
+    out["newton_c_tol"] = np.array([c, tol[0]])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
     ap.add_argument("--host-only", action="store_true")
     ap.add_argument("--arnoldi-only", action="store_true")
+    ap.add_argument("--linsolve-only", action="store_true")
     a = ap.parse_args()
     lib = ctypes.CDLL(LIB)
     lib.ref_select_shifts.argtypes = [ctypes.c_int, _dp, ctypes.c_char_p, _dp, _dp, _dp]
@@ -167,6 +212,14 @@ def main():
         getattr(lib, f).argtypes = [ctypes.c_int] * 3 + [_dp] * 3
     lib.ref_arnoldi_dense.argtypes = [ctypes.c_int] * 3 + [_dp] * 4
     lib.ref_laplace_apply.argtypes = [ctypes.c_int, _dp, _dp]
+    lib.ref_bicgstabl_dense.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp,
+                                        ctypes.POINTER(ctypes.c_int)]
+    lib.ref_newton_cubic.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double, _dp, _dp,
+                                     ctypes.POINTER(ctypes.c_int), ctypes.c_double, ctypes.c_int]
+    if a.linsolve_only:
+        np.savez_compressed(os.path.join(a.out, "krylov_linsolve.npz"), **make_linsolve(lib))
+        print("wrote krylov_linsolve.npz")
+        return
     if not a.arnoldi_only:
         np.savez_compressed(os.path.join(a.out, "krylov_qr.npz"), **make_qr(lib))
         print("wrote krylov_qr.npz")

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-13
 
 GRIDS = [(16, 16, 16), (32, 48, 24), (64, 64, 64), (8, 96, 16), (128, 128, 128),
-         (24, 16, 384), (256, 8, 8), (48, 512, 8)]
+         (24, 16, 384), (256, 8, 8), (48, 512, 8), (256, 256, 256)]
 
 
 @pytest.fixture(scope="module")

@@ -253,3 +253,117 @@ def test_krylov_errors_are_status_codes(torch):
     with pytest.raises(ValueError):
         kr.arnoldi(kr.laplace_map(), V.cpu(), H, f, 0, m)
     kr.close()
+
+
+@pytest.mark.parametrize("k0", [1, 7, 8, 9, 16, 17, 33, 64, 70])
+def test_restart_all_kernel_widths(torch, k0):
+    """Every width of the register-tiled restart (k0 <= 8, 16, 32, 64) and the
+    shared-memory form beyond, against the oracle's V Q and f update."""
+    n, m = 3001, 80
+    rng = np.random.default_rng(100 + k0)
+    Vo = rng.standard_normal((m, n))
+    fo = rng.standard_normal(n)
+    Q = np.linalg.qr(rng.standard_normal((m, m)))[0]
+    H = np.triu(rng.standard_normal((m, m)), -1)
+    kr = _kr(n, m)
+    V = torch.as_tensor(Vo, device="cuda").clone()
+    f = torch.as_tensor(fo, device="cuda").clone()
+    Qg = Q.copy()
+    fn = kr.ira_restart(V, f, Qg, H, k0)
+    Qo = Q.copy()
+    fno = K.ira_restart(Vo, fo, Qo, H, k0)
+    assert abs(fn / fno - 1.0) < 1e-13
+    assert np.abs(V.cpu().numpy() - Vo).max() < 1e-12
+    assert np.abs(f.cpu().numpy() - fo).max() < 1e-12
+    kr.close()
+
+
+def _lin_matrix(n, seed, diag, scale):
+    rng = np.random.default_rng(seed)
+    return diag * np.eye(n) + scale * rng.standard_normal((n, n)) / np.sqrt(n)
+
+
+@pytest.mark.parametrize("idx", range(3))
+def test_bicgstabl_matches_reference_golden(torch, idx):
+    d = np.load(os.path.join(GOLDEN, "krylov_linsolve.npz"))
+    n, L, seed, flag, it = (int(v) for v in d[f"bicg{idx}_meta"])
+    kr = _kr(n, 4)
+    A = _torch_dense_map(torch, kr, _lin_matrix(n, seed, 2.0, 0.5))
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    b = torch.as_tensor(d[f"bicg{idx}_b"], device="cuda")
+    fl, its, err = kr.bicgstabl(A, x, b, L, 1e-10, 200)
+    assert (fl, its) == (flag, it)
+    ref = d[f"bicg{idx}_x"]
+    assert np.abs(x.cpu().numpy() - ref).max() < 1e-10 * np.abs(ref).max()
+    kr.close()
+
+
+def test_newton_matches_reference_golden(torch):
+    d = np.load(os.path.join(GOLDEN, "krylov_linsolve.npz"))
+    n, seed, flag, it = (int(v) for v in d["newton_meta"])
+    c, tol_out = (float(v) for v in d["newton_c_tol"])
+    Ad = torch.as_tensor(_lin_matrix(n, seed, 3.0, 0.3), device="cuda")
+    bd = torch.as_tensor(d["newton_b"], device="cuda")
+    base = torch.zeros(n, dtype=torch.float64, device="cuda")
+    kr = _kr(n, 4)
+
+    def residual(x, y):
+        base.copy_(x)
+        torch.mv(Ad, x, out=y)
+        y.add_(c * x ** 3 - bd)
+
+    def jacobian(v, y):
+        torch.mv(Ad, v, out=y)
+        y.add_(3.0 * c * base ** 2 * v)
+
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    r = kr.newton(kr.python_map(jacobian), kr.python_map(residual), x, 1e-9, 60, 1e-11, 200)
+    assert (r["flag"], r["iterations"], r["linsolve_flag"]) == (flag, it, 0)
+    assert abs(r["tol"] - tol_out) < 1e-6 * tol_out + 1e-14
+    ref = d["newton_x"]
+    assert np.abs(x.cpu().numpy() - ref).max() < 1e-10 * np.abs(ref).max()
+    kr.close()
+
+
+def test_newton_finds_the_laminar_kolmogorov_flow(torch):
+    """F(u) = RHS(u) on reduced vectors (ns3d_map_rhs) with the linearised map
+    on the same base flow as the Jacobian: from a perturbed start, Newton
+    returns to the laminar fixed point u = (Re/16) sin(4y) x."""
+    from ns3dperiodic_b200 import Solver
+
+    g = O.Grid(16, 16, 16)
+    Re = 5.0
+    U0, F = O.kolmogorov_state(g, Re, 0, rel_amp=0.0)
+    P = O.random_perturbation(g, 4)
+    Ustart = [U0[i] + 0.05 * P[i] for i in range(3)]
+    S = Solver(16, 16, 16)
+    S.set_forcing(S.to_device(F))
+    n = S.krylov_length
+    kr = _kr(n, 4)
+    Ub = S.zeros()
+    Vs = S.zeros()
+    Fm = kr.rhs_map(S, Ub, Vs, Re)
+    Jm = kr.linearised_map(S, Ub, Re)
+    x = torch.as_tensor(O.pack_reduced(Ustart), device="cuda").clone()
+    r = kr.newton(Jm, Fm, x, 1e-10, 80, 1e-12, 300)
+    assert r["flag"] == 0 and Fm.status == 0 and Jm.status == 0
+    ref = O.pack_reduced(U0)
+    assert np.abs(x.cpu().numpy() - ref).max() < 1e-8 * np.abs(ref).max()
+    kr.close()
+    S.close()
+
+
+def test_bicgstabl_reports_nan_and_bad_arguments(torch):
+    from ns3dperiodic_b200 import Ns3dError
+
+    n = 500
+    kr = _kr(n, 4)
+    b = torch.ones(n, dtype=torch.float64, device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    nan_map = kr.python_map(lambda v, y: y.fill_(math.nan))
+    fl, its, err = kr.bicgstabl(nan_map, x, b, 2, 1e-8, 10)
+    assert fl == -3
+    with pytest.raises(Ns3dError) as e:
+        kr.bicgstabl(nan_map, x, b, 0, 1e-8, 10)
+    assert e.value.status == 1
+    kr.close()

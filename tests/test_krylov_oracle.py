@@ -154,3 +154,66 @@ def test_oracle_restart_keeps_a_k_step_factorisation():
 def test_oracle_arnoldi_rejects_zero_start():
     with pytest.raises(K.ArnoldiBreakdown):
         K.arnoldi_driver(K.laplace1d, np.zeros((4, 10)), np.zeros((4, 4)), np.zeros(10), 0, 4)
+
+
+def _linsolve_golden():
+    path = os.path.join(GOLDEN, "krylov_linsolve.npz")
+    if not os.path.exists(path):
+        pytest.fail("tests/golden/krylov_linsolve.npz is missing (make_golden_krylov.py)")
+    return np.load(path)
+
+
+def _lin_matrix(n, seed, diag, scale):
+    rng = np.random.default_rng(seed)
+    return diag * np.eye(n) + scale * rng.standard_normal((n, n)) / np.sqrt(n)
+
+
+@pytest.mark.parametrize("idx", range(3))
+def test_oracle_bicgstabl_matches_reference(idx):
+    d = _linsolve_golden()
+    n, L, seed, flag, it = (int(v) for v in d[f"bicg{idx}_meta"])
+    A = _lin_matrix(n, seed, 2.0, 0.5)
+    x = np.zeros(n)
+    fl, its, err = K.bicgstabl(lambda v: A @ v, x, d[f"bicg{idx}_b"], L, 1e-10, 200)
+    assert (fl, its) == (flag, it)
+    assert abs(err - float(d[f"bicg{idx}_err"][0])) < 1e-3 * float(d[f"bicg{idx}_err"][0])
+    assert np.abs(x - d[f"bicg{idx}_x"]).max() < 1e-10 * np.abs(d[f"bicg{idx}_x"]).max()
+
+
+def test_oracle_newton_matches_reference():
+    d = _linsolve_golden()
+    n, seed, flag, it = (int(v) for v in d["newton_meta"])
+    c, tol_out = (float(v) for v in d["newton_c_tol"])
+    A = _lin_matrix(n, seed, 3.0, 0.3)
+    b = d["newton_b"]
+    st = {"base": np.zeros(n)}
+
+    def F(x):
+        st["base"] = x.copy()
+        return A @ x + c * x ** 3 - b
+
+    x = np.zeros(n)
+    fl, its, t, lf = K.newton(lambda v: A @ v + 3 * c * st["base"] ** 2 * v, F, x, 1e-9, 60,
+                              1e-11, 200)
+    assert (fl, its, lf) == (flag, it, 0)
+    assert abs(t - tol_out) < 1e-6 * tol_out + 1e-14
+    assert np.abs(x - d["newton_x"]).max() < 1e-10 * np.abs(d["newton_x"]).max()
+
+
+def test_oracle_bicgstabl_solves_and_flags():
+    rng = np.random.default_rng(9)
+    n = 150
+    A = 2.0 * np.eye(n) + 0.5 * rng.standard_normal((n, n)) / np.sqrt(n)
+    b = rng.standard_normal(n)
+    for L in (1, 3, 6):
+        x = np.zeros(n)
+        fl, its, err = K.bicgstabl(lambda v: A @ v, x, b, L, 1e-12, 300)
+        assert fl == 0 and err < 1e-12
+        assert np.abs(A @ x - b).max() < 1e-10
+    # already solved: flag 0 without iterating
+    x = np.linalg.solve(A, b)
+    fl, its, err = K.bicgstabl(lambda v: A @ v, x, b, 2, 1e-8, 10)
+    assert fl == 0 and its == 0
+    # NaN in the map: flag -3
+    fl, its, err = K.bicgstabl(lambda v: v * np.nan, np.zeros(n), b, 2, 1e-8, 10)
+    assert fl == -3
