@@ -351,6 +351,15 @@ ns3d_status ns3d_ira_restart(ns3d_krylov* kr, double* V, double* f, double* Q, c
 ns3d_status ns3d_krylov_profile(ns3d_krylov* kr, const double* V, int ncols, const double* x,
                                 int reps, double* ms);
 
+/* W = V C: W(:, j) = sum_c V(:, c) C(c, j) for j < p, c < m; V and W DEVICE
+ * n x m and n x p column-major (leading dimension n, W not overlapping V),
+ * C HOST m x p column-major.  The basis products of the final eigenvector
+ * stage of the implicit restart (V1 = V Q_Schur and the eigenvector
+ * combinations, Source/Arnoldi/Implicit_restart_Arnoldi.cu:255-330,640-643):
+ * one pass over V, the outputs kept in registers.  Synchronous. */
+ns3d_status ns3d_krylov_combine(ns3d_krylov* kr, const double* V, int m, const double* C, int p,
+                                double* W);
+
 /* BiCGStabL (Source/Arnoldi/BiCGStabL.cu:18-185): solves A x = rhs with
  * BiCGStab(L), 1 <= L <= 16, x (device, length n) the initial guess on entry
  * and the solution on exit, rhs (device) unchanged.  *tol and *iter are the
@@ -424,8 +433,56 @@ typedef struct ns3d_laplace_context {
 void ns3d_map_laplace1d(void* user, void* in, void* out);
 
 /* ----------------------------------------------------------------------- */
+/* checkpoints in the reference's wire format (Source/file_operations.cu)   */
+/* ----------------------------------------------------------------------- */
+
+/* write_control_file_fourier / read_control_fourier
+ * (Source/file_operations.cu:196-228, 104-191) for the handle's DEVICE
+ * fields: one line per mode of [Nx][Ny][Mz], "%.16le" x 6 (Re, Im of ux, uy,
+ * uz).  Loading accepts the handle's own size or a coarser grid with the
+ * same aspect ratios, up-sampled the reference's way (see
+ * ns3d_read_control_fourier_host).  Synchronous. */
+ns3d_status ns3d_save_control_fourier(ns3d_solver* h, const char* path, const ns3d_complex* ux,
+                                      const ns3d_complex* uy, const ns3d_complex* uz);
+ns3d_status ns3d_load_control_fourier(ns3d_solver* h, const char* path, ns3d_complex* ux,
+                                      ns3d_complex* uy, ns3d_complex* uz);
+
+/* write_control_file / read_control_file (Source/file_operations.cu:4-45):
+ * the physical velocity, one line per point of [Nx][Ny][Nz],
+ * "%.16le %.16le %.16le".  Save transforms the spectral DEVICE fields to
+ * physical space (iFFTN_Device with the 1/N scale, as main does before
+ * writing); load reads the physical field and transforms it back (FFTN).
+ * Synchronous. */
+ns3d_status ns3d_save_control_file(ns3d_solver* h, const char* path, const ns3d_complex* ux,
+                                   const ns3d_complex* uy, const ns3d_complex* uz);
+ns3d_status ns3d_load_control_file(ns3d_solver* h, const char* path, ns3d_complex* ux,
+                                   ns3d_complex* uy, ns3d_complex* uz);
+
+/* ----------------------------------------------------------------------- */
 /* host-only helpers (no GPU needed)                                        */
 /* ----------------------------------------------------------------------- */
+
+/* The Fourier checkpoint of HOST fields [Nx][Ny][Nz/2+1] (Nz is the
+ * physical extent).  Reading a file of a coarser grid: its extents are
+ * found from its line count with the target's ratios Nx/Ny and (2Mz-1)/Ny,
+ * Ny_file = 4, 6, ... (get_control_fourier_size, Source/file_operations.cu:
+ * 48-101; the reference searches without a bound and writes out of range
+ * for a finer file, here the search stops at Ny and a finer or unmatched
+ * file is NS3D_ERR_BAD_ARG); modes are placed at the same signed x / y
+ * wavenumber and z index, the rest set to zero, and scaled by the integer
+ * ratio Nx Ny (2Mz-1) / (Nx_f Ny_f (2Mz_f-1)) the reference computes.
+ * Nx_file, Ny_file, Mz_file (may be null) receive the extents read. */
+ns3d_status ns3d_write_control_fourier_host(const char* path, int Nx, int Ny, int Nz,
+                                            const ns3d_complex* ux, const ns3d_complex* uy,
+                                            const ns3d_complex* uz);
+ns3d_status ns3d_read_control_fourier_host(const char* path, int Nx, int Ny, int Nz,
+                                           ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                                           int* Nx_file, int* Ny_file, int* Mz_file);
+/* The physical checkpoint of HOST fields [Nx][Ny][Nz]. */
+ns3d_status ns3d_write_control_file_host(const char* path, int Nx, int Ny, int Nz, const double* ux,
+                                         const double* uy, const double* uz);
+ns3d_status ns3d_read_control_file_host(const char* path, int Nx, int Ny, int Nz, double* ux,
+                                        double* uy, double* uz);
 
 /* The 2/3 mask as a kz cut-off per (x, y) column: mode (j,k,l) is kept iff
  * l < qcut[j*Ny + k] (and (j,k,l) != 0), evaluated with the arithmetic of

@@ -31,11 +31,14 @@ EXPORTS = (
     "ns3d_jvp_step", "ns3d_jvp_steps", "ns3d_linearised_rhs", "ns3d_implicit_tangent_step",
     "ns3d_krylov_length", "ns3d_pack_reduced", "ns3d_unpack_reduced", "ns3d_matvec_reduced",
     "ns3d_diagnostics", "ns3d_profile_passes", "ns3d_mask_cutoff", "ns3d_twiddles",
+    "ns3d_save_control_fourier", "ns3d_load_control_fourier", "ns3d_save_control_file",
+    "ns3d_load_control_file", "ns3d_write_control_fourier_host", "ns3d_read_control_fourier_host",
+    "ns3d_write_control_file_host", "ns3d_read_control_file_host",
     "ns3d_convolution_noalloc", "ns3d_fft_r2c", "ns3d_fft_c2r", "ns3d_fft_c2r_unscaled",
     "ns3d_tangent_euler_step",
     "ns3d_krylov_create", "ns3d_krylov_destroy", "ns3d_krylov_set_stream",
     "ns3d_krylov_last_error", "ns3d_arnoldi", "ns3d_krylov_stats", "ns3d_qr_shifts",
-    "ns3d_ira_restart", "ns3d_krylov_profile", "ns3d_bicgstabl", "ns3d_newton",
+    "ns3d_ira_restart", "ns3d_krylov_profile", "ns3d_krylov_combine", "ns3d_bicgstabl", "ns3d_newton",
     "ns3d_map_rhs", "ns3d_map_linearised", "ns3d_map_exponential", "ns3d_map_laplace1d",
 )
 
@@ -111,6 +114,18 @@ def _sig(lib):
         "ns3d_convolution_noalloc": ([c_int, c_int, c_int, c_double, c_double, c_double]
                                      + [_P] * 6 + [_P], c_int),
         "ns3d_fft_r2c": ([_P, _P, _P], c_int),
+        "ns3d_save_control_fourier": ([_P, ctypes.c_char_p, _P, _P, _P], c_int),
+        "ns3d_load_control_fourier": ([_P, ctypes.c_char_p, _P, _P, _P], c_int),
+        "ns3d_save_control_file": ([_P, ctypes.c_char_p, _P, _P, _P], c_int),
+        "ns3d_load_control_file": ([_P, ctypes.c_char_p, _P, _P, _P], c_int),
+        "ns3d_write_control_fourier_host": ([ctypes.c_char_p, c_int, c_int, c_int, _P, _P, _P],
+                                            c_int),
+        "ns3d_read_control_fourier_host": ([ctypes.c_char_p, c_int, c_int, c_int, _P, _P, _P,
+                                            _P, _P, _P], c_int),
+        "ns3d_write_control_file_host": ([ctypes.c_char_p, c_int, c_int, c_int, _P, _P, _P],
+                                         c_int),
+        "ns3d_read_control_file_host": ([ctypes.c_char_p, c_int, c_int, c_int, _P, _P, _P],
+                                        c_int),
         "ns3d_fft_c2r": ([_P, _P, _P], c_int),
         "ns3d_fft_c2r_unscaled": ([_P, _P, _P], c_int),
         "ns3d_tangent_euler_step": ([_P] + [_P] * 6 + [c_double, c_double], c_int),
@@ -123,6 +138,7 @@ def _sig(lib):
         "ns3d_qr_shifts": ([c_int, c_int, _P, _P, _P, _P, _P], c_int),
         "ns3d_ira_restart": ([_P, _P, _P, _P, _P, c_int, c_int, _P], c_int),
         "ns3d_krylov_profile": ([_P, _P, c_int, _P, c_int, _P], c_int),
+        "ns3d_krylov_combine": ([_P, _P, c_int, _P, c_int, _P], c_int),
         "ns3d_bicgstabl": ([_P, c_int, _P, _P, _P, _P, _P, _P, _P], c_int),
         "ns3d_newton": ([_P, _P, _P, _P, _P, _P, _P, _P, c_double, c_int, _P, _P], c_int),
         "ns3d_map_rhs": ([_P, _P, _P], None),

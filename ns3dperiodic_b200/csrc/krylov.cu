@@ -196,7 +196,8 @@ __global__ void __launch_bounds__(kThreads) gemv_n_sub(const double* __restrict_
 __global__ void __launch_bounds__(kRestartThreads) restart_rows(double* V, int64_t n, int m,
                                                                 int k0,
                                                                 const double* __restrict__ qc,
-                                                                double hl, double ql, double* f) {
+                                                                double hl, double ql, double* f,
+                                                                double* W) {
   extern __shared__ double row[];  // m * kRestartThreads
   const int t = threadIdx.x;
   const int64_t stride = (int64_t)gridDim.x * kRestartThreads;
@@ -205,9 +206,10 @@ __global__ void __launch_bounds__(kRestartThreads) restart_rows(double* V, int64
     for (int j = 0; j <= k0; ++j) {
       const double* q = qc + (size_t)j * m;
       double s = 0.0;
+      if (j == k0 && !f) break;
       for (int c = 0; c < m; ++c) s = fma(row[c * kRestartThreads + t], __ldg(q + c), s);
       if (j < k0)
-        V[(int64_t)j * n + r] = s;
+        W[(int64_t)j * n + r] = s;
       else
         f[r] = hl * s + ql * f[r];
     }
@@ -219,13 +221,15 @@ __global__ void __launch_bounds__(kRestartThreads) restart_rows(double* V, int64
 // streams its rows of V in chunks of 8 columns (coalesced across the warp)
 // and reads each coefficient, staged in shared memory, once per RR rows (a
 // broadcast).  The residual column Q(:, k0) has its own accumulator, so no
-// output is selected by a runtime index.
+// output is selected by a runtime index.  Outputs go to W (W = V: in place;
+// each thread reads its whole row before writing it); f = null skips the
+// residual.
 template <int KMAX, int RR>
 __global__ void __launch_bounds__(kRestartThreads) restart_rows_reg(double* V, int64_t n, int m,
                                                                     int k0,
                                                                     const double* __restrict__ qc,
                                                                     double hl, double ql,
-                                                                    double* f) {
+                                                                    double* f, double* W) {
   // sq: Q(:, 0..k0-1) column-major, zero-padded to KMAX columns, then
   // Q(:, k0); 8 words of zero padding after each part
   extern __shared__ double sq[];
@@ -234,7 +238,7 @@ __global__ void __launch_bounds__(kRestartThreads) restart_rows_reg(double* V, i
     double x = 0.0;
     if (i < m * k0)
       x = qc[i];
-    else if (i >= nb && i < nb + m)
+    else if (f && i >= nb && i < nb + m)
       x = qc[(size_t)k0 * m + (i - nb)];
     sq[i] = x;
   }
@@ -284,8 +288,8 @@ __global__ void __launch_bounds__(kRestartThreads) restart_rows_reg(double* V, i
       if (r < n) {
 #pragma unroll
         for (int j = 0; j < KMAX; ++j)
-          if (j < k0) V[(int64_t)j * n + r] = acc[rr][j];
-        f[r] = hl * accf[rr] + ql * f[r];
+          if (j < k0) W[(int64_t)j * n + r] = acc[rr][j];
+        if (f) f[r] = hl * accf[rr] + ql * f[r];
       }
     }
   }
@@ -293,22 +297,23 @@ __global__ void __launch_bounds__(kRestartThreads) restart_rows_reg(double* V, i
 
 // Launches the restart pass for the basis columns 0..k0-1 and the residual.
 cudaError_t launch_restart(double* V, int64_t n, int m, int k0, const double* qc, double hl,
-                           double ql, double* f, cudaStream_t st) {
+                           double ql, double* f, cudaStream_t st, double* W = nullptr) {
+  if (!W) W = V;
   const int kmax = k0 <= 8 ? 8 : k0 <= 16 ? 16 : k0 <= 32 ? 32 : 64;
   const size_t sq = sizeof(double) * ((size_t)m * kmax + 8 + m + 8);
   const int b2 = blocks_for(n, kRestartThreads * 2, 148 * 8);
   const int b1 = blocks_for(n, kRestartThreads, 148 * 8);
   if (k0 <= 8)
-    restart_rows_reg<8, 2><<<b2, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f);
+    restart_rows_reg<8, 2><<<b2, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f, W);
   else if (k0 <= 16)
-    restart_rows_reg<16, 2><<<b2, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f);
+    restart_rows_reg<16, 2><<<b2, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f, W);
   else if (k0 <= 32)
-    restart_rows_reg<32, 2><<<b2, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f);
+    restart_rows_reg<32, 2><<<b2, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f, W);
   else if (k0 <= 64)
-    restart_rows_reg<64, 1><<<b1, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f);
+    restart_rows_reg<64, 1><<<b1, kRestartThreads, sq, st>>>(V, n, m, k0, qc, hl, ql, f, W);
   else
     restart_rows<<<b1, kRestartThreads, sizeof(double) * (size_t)m * kRestartThreads, st>>>(
-        V, n, m, k0, qc, hl, ql, f);
+        V, n, m, k0, qc, hl, ql, f, W);
   return cudaGetLastError();
 }
 
@@ -805,6 +810,23 @@ ns3d_status ns3d_krylov_profile(ns3d_krylov* kr, const double* V, int ncols, con
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_krylov_combine(ns3d_krylov* kr, const double* V, int m, const double* C, int p,
+                                double* W) {
+  KR_TRY(enter(kr));
+  if (!V || !C || !W || m < 1 || m > kr->m_max || p < 1 || p > kr->m_max)
+    return kfail(kr, NS3D_ERR_BAD_ARG, "need 1 <= m, p <= m_max and non-null pointers");
+  const size_t nq = (size_t)m * p;
+  double* staged = kr->host + 2 + 2 * (size_t)kr->m_max;
+  std::memcpy(staged, C, sizeof(double) * nq);
+  KR_CHECK(kr, cudaMemcpyAsync(kr->qcoef, staged, sizeof(double) * nq, cudaMemcpyHostToDevice,
+                               kr->stream), "C upload");
+  KR_CHECK(kr, launch_restart(const_cast<double*>(V), kr->n, m, p, kr->qcoef, 0.0, 0.0, nullptr,
+                              kr->stream, W),
+           "combine");
+  KR_CHECK(kr, cudaStreamSynchronize(kr->stream), "combine sync");
   return NS3D_OK;
 }
 

@@ -584,6 +584,84 @@ ns3d_status ns3d_fft_c2r_unscaled(ns3d_solver* h, const ns3d_complex* in, double
   return fft_c2r(h, in, out, 1.0);
 }
 
+// Checkpoints of device fields through host buffers (the wire format is
+// written and parsed by the host functions of checkpoint.cpp).
+ns3d_status ns3d_save_control_fourier(ns3d_solver* h, const char* path, const ns3d_complex* ux,
+                                      const ns3d_complex* uy, const ns3d_complex* uz) {
+  NS3D_TRY(check_handle(h));
+  if (!path || !args_ok3(ux, uy, uz)) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  std::vector<ns3d_complex> b[3];
+  const ns3d_complex* d[3] = {ux, uy, uz};
+  for (int c = 0; c < 3; ++c) {
+    b[c].resize(h->nc);
+    NS3D_CHECK(h, cudaMemcpyAsync(b[c].data(), d[c], sizeof(ns3d_complex) * h->nc,
+                                  cudaMemcpyDeviceToHost, h->stream), "checkpoint copy");
+  }
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "checkpoint sync");
+  const ns3d_status s = ns3d_write_control_fourier_host(path, h->Nx, h->Ny, h->Nz, b[0].data(),
+                                                        b[1].data(), b[2].data());
+  return s == NS3D_OK ? s : fail(h, s, std::string("cannot write ") + path);
+}
+
+ns3d_status ns3d_load_control_fourier(ns3d_solver* h, const char* path, ns3d_complex* ux,
+                                      ns3d_complex* uy, ns3d_complex* uz) {
+  NS3D_TRY(check_handle(h));
+  if (!path || !args_ok3(ux, uy, uz)) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  std::vector<ns3d_complex> b[3];
+  for (int c = 0; c < 3; ++c) b[c].resize(h->nc);
+  const ns3d_status s = ns3d_read_control_fourier_host(path, h->Nx, h->Ny, h->Nz, b[0].data(),
+                                                       b[1].data(), b[2].data(), nullptr,
+                                                       nullptr, nullptr);
+  if (s != NS3D_OK) return fail(h, s, std::string("cannot read a matching state from ") + path);
+  ns3d_complex* d[3] = {ux, uy, uz};
+  for (int c = 0; c < 3; ++c)
+    NS3D_CHECK(h, cudaMemcpyAsync(d[c], b[c].data(), sizeof(ns3d_complex) * h->nc,
+                                  cudaMemcpyHostToDevice, h->stream), "checkpoint copy");
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "checkpoint sync");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_save_control_file(ns3d_solver* h, const char* path, const ns3d_complex* ux,
+                                   const ns3d_complex* uy, const ns3d_complex* uz) {
+  NS3D_TRY(check_handle(h));
+  if (!path || !args_ok3(ux, uy, uz)) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  const size_t nr = (size_t)h->Nx * h->Ny * h->Nz;
+  std::vector<double> b[3];
+  const ns3d_complex* d[3] = {ux, uy, uz};
+  double* phys = reinterpret_cast<double*>(h->B[0]);  // S_c bytes >= S_r bytes
+  for (int c = 0; c < 3; ++c) {
+    b[c].resize(nr);
+    NS3D_TRY(ns3d_fft_c2r(h, d[c], phys));
+    NS3D_CHECK(h, cudaMemcpyAsync(b[c].data(), phys, sizeof(double) * nr, cudaMemcpyDeviceToHost,
+                                  h->stream), "checkpoint copy");
+  }
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "checkpoint sync");
+  const ns3d_status s = ns3d_write_control_file_host(path, h->Nx, h->Ny, h->Nz, b[0].data(),
+                                                     b[1].data(), b[2].data());
+  return s == NS3D_OK ? s : fail(h, s, std::string("cannot write ") + path);
+}
+
+ns3d_status ns3d_load_control_file(ns3d_solver* h, const char* path, ns3d_complex* ux,
+                                   ns3d_complex* uy, ns3d_complex* uz) {
+  NS3D_TRY(check_handle(h));
+  if (!path || !args_ok3(ux, uy, uz)) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  const size_t nr = (size_t)h->Nx * h->Ny * h->Nz;
+  std::vector<double> b[3];
+  for (int c = 0; c < 3; ++c) b[c].resize(nr);
+  const ns3d_status s = ns3d_read_control_file_host(path, h->Nx, h->Ny, h->Nz, b[0].data(),
+                                                    b[1].data(), b[2].data());
+  if (s != NS3D_OK) return fail(h, s, std::string("cannot read a matching field from ") + path);
+  ns3d_complex* d[3] = {ux, uy, uz};
+  double* phys = reinterpret_cast<double*>(h->B[0]);
+  for (int c = 0; c < 3; ++c) {
+    NS3D_CHECK(h, cudaMemcpyAsync(phys, b[c].data(), sizeof(double) * nr, cudaMemcpyHostToDevice,
+                                  h->stream), "checkpoint copy");
+    NS3D_TRY(ns3d_fft_r2c(h, phys, d[c]));
+  }
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "checkpoint sync");
+  return NS3D_OK;
+}
+
 ns3d_status ns3d_convolution(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
                              const ns3d_complex* uz, ns3d_complex* Qx, ns3d_complex* Qy,
                              ns3d_complex* Qz) {

@@ -311,3 +311,58 @@ class Krylov:
             # vector_normC: max of fabsf (single precision), Products.cpp:23-31
             ritz_norm = float(np.max(np.abs(ritz[:k0]).astype(np.float32)))
         return eig, ritz_norm, it, V, H
+
+    # -- final stage of the implicit restart ----------------------------------
+    def combine(self, V, C: np.ndarray, out=None):
+        """W = V C on the device (ns3d_krylov_combine): V holds m basis
+        vectors as rows of an (m, n) tensor, C is (m, p); returns the (p, n)
+        tensor whose row j is sum_c C[c, j] V[c]."""
+        torch = self._torch
+        C = np.asfortranarray(C, dtype=np.float64)
+        m, p = C.shape
+        self._basis(V, m)
+        W = out if out is not None else torch.empty((p, self.n), dtype=torch.float64,
+                                                    device=self.device)
+        self._basis(W, p)
+        self._check(self._L.ns3d_krylov_combine(self._h, ctypes.c_void_p(V.data_ptr()), m,
+                                                C.ctypes.data, p,
+                                                ctypes.c_void_p(W.data_ptr())),
+                    "ns3d_krylov_combine")
+        return W
+
+    def apply(self, A: Map, x, y):
+        """y = A x through the map's C entry point (finished on return)."""
+        fn = MAP_FN(self._fnptr(A)) if isinstance(A.fn, int) else A.fn
+        fn(ctypes.c_void_p(A.ctx_ptr()), ctypes.c_void_p(x.data_ptr()),
+           ctypes.c_void_p(y.data_ptr()))
+        self._torch.cuda.synchronize(self.device)
+        return y
+
+    def eigenpairs(self, A: Map, V, H: np.ndarray, k: int, which: str = "LR"):
+        """The final stage of Implicit_restart_Arnoldi_GPU_data
+        (Implicit_restart_Arnoldi.cu:255-330, 589-664, no rotation): the real
+        Schur form H_k = Z T Z^T of the leading k x k block (dhseqr there,
+        scipy's LAPACK here), the Schur basis V1 = V_k Z, the Galerkin matrix
+        R = V1^T A V1, its eigenpairs (R y = lambda y, unit y) sorted by
+        ``which``, and the eigenvectors x = V1 y with the residuals
+        ||A v1_i - V1 R e_i|| of the Schur vectors.  Returns (eigenvalues,
+        eigenvectors as a complex (k, n) tensor, residuals).  The reference
+        permutes the eigenvector columns a second time after sorting; here
+        eigenvector i belongs to eigenvalue i."""
+        from scipy.linalg import schur
+
+        torch = self._torch
+        _, Z = schur(np.asarray(H[:k, :k], dtype=np.float64), output="real")
+        V1 = self.combine(V, Z)
+        AV1 = torch.empty_like(V1)
+        for i in range(k):
+            self.apply(A, V1[i], AV1[i])
+        R = (V1 @ AV1.T).cpu().numpy()               # R[i, j] = v1_i . A v1_j
+        res = torch.linalg.vector_norm(AV1 - (torch.as_tensor(R, device=self.device).T @ V1),
+                                       dim=1).cpu().numpy()
+        w, Y = np.linalg.eig(R)
+        key = -w.real if which == "LR" else -np.abs(w)
+        order = np.argsort(key, kind="stable")
+        w, Y = w[order], Y[:, order]
+        X = torch.complex(self.combine(V1, Y.real), self.combine(V1, Y.imag))
+        return w, X, res

@@ -217,6 +217,36 @@ class Solver:
         self._check(fn(self._h, p, _ptr(out)), "ns3d_fft_c2r")
         return out
 
+    # -- checkpoints (Source/file_operations.cu) -----------------------------
+    def save_control_fourier(self, path: str, U):
+        """write_control_file_fourier of device fields U."""
+        self._check(self._L.ns3d_save_control_fourier(self._h, str(path).encode(),
+                                                      *self._fields(U, "U")),
+                    "ns3d_save_control_fourier")
+
+    def load_control_fourier(self, path: str, out=None):
+        """read_control_fourier into device fields (a coarser file is
+        up-sampled the reference's way)."""
+        out = out if out is not None else self.zeros()
+        self._check(self._L.ns3d_load_control_fourier(self._h, str(path).encode(),
+                                                      *self._fields(out, "out")),
+                    "ns3d_load_control_fourier")
+        return out
+
+    def save_control_file(self, path: str, U):
+        """write_control_file of the physical velocity of device fields U."""
+        self._check(self._L.ns3d_save_control_file(self._h, str(path).encode(),
+                                                   *self._fields(U, "U")),
+                    "ns3d_save_control_file")
+
+    def load_control_file(self, path: str, out=None):
+        """read_control_file, transformed to spectral device fields."""
+        out = out if out is not None else self.zeros()
+        self._check(self._L.ns3d_load_control_file(self._h, str(path).encode(),
+                                                   *self._fields(out, "out")),
+                    "ns3d_load_control_file")
+        return out
+
     # -- Krylov adapters (Source/NS3D_periodic.cu:173-385) ------------------
     @property
     def krylov_length(self) -> int:
@@ -275,3 +305,55 @@ class Solver:
 
 def supported_extent(n: int) -> bool:
     return bool(lib().ns3d_supported_extent(int(n)))
+
+
+def write_control_fourier(path: str, U):
+    """Host form of write_control_file_fourier: U = 3 complex (Nx, Ny, Nz//2+1)
+    numpy arrays (Nz taken as 2 (Mz - 1))."""
+    import numpy as np
+
+    a = [np.ascontiguousarray(u, dtype=np.complex128) for u in U]
+    Nx, Ny, Mz = a[0].shape
+    rc = lib().ns3d_write_control_fourier_host(str(path).encode(), Nx, Ny, 2 * (Mz - 1),
+                                               *[x.ctypes.data for x in a])
+    if rc != 0:
+        raise Ns3dError(rc, "ns3d_write_control_fourier_host", str(path))
+
+
+def read_control_fourier(path: str, Nx: int, Ny: int, Nz: int):
+    """Host form of read_control_fourier for an Nx x Ny x Nz grid; returns
+    (U, (Nx_file, Ny_file, Mz_file))."""
+    import numpy as np
+
+    U = [np.zeros((Nx, Ny, Nz // 2 + 1), dtype=np.complex128) for _ in range(3)]
+    ext = [ctypes.c_int(0) for _ in range(3)]
+    rc = lib().ns3d_read_control_fourier_host(str(path).encode(), Nx, Ny, Nz,
+                                              *[u.ctypes.data for u in U],
+                                              *[ctypes.byref(e) for e in ext])
+    if rc != 0:
+        raise Ns3dError(rc, "ns3d_read_control_fourier_host", str(path))
+    return U, tuple(e.value for e in ext)
+
+
+def write_control_file(path: str, u):
+    """Host form of write_control_file: u = 3 real (Nx, Ny, Nz) arrays."""
+    import numpy as np
+
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in u]
+    Nx, Ny, Nz = a[0].shape
+    rc = lib().ns3d_write_control_file_host(str(path).encode(), Nx, Ny, Nz,
+                                            *[x.ctypes.data for x in a])
+    if rc != 0:
+        raise Ns3dError(rc, "ns3d_write_control_file_host", str(path))
+
+
+def read_control_file(path: str, Nx: int, Ny: int, Nz: int):
+    """Host form of read_control_file."""
+    import numpy as np
+
+    u = [np.zeros((Nx, Ny, Nz)) for _ in range(3)]
+    rc = lib().ns3d_read_control_file_host(str(path).encode(), Nx, Ny, Nz,
+                                           *[x.ctypes.data for x in u])
+    if rc != 0:
+        raise Ns3dError(rc, "ns3d_read_control_file_host", str(path))
+    return u

@@ -367,3 +367,41 @@ def test_bicgstabl_reports_nan_and_bad_arguments(torch):
         kr.bicgstabl(nan_map, x, b, 0, 1e-8, 10)
     assert e.value.status == 1
     kr.close()
+
+
+def test_combine_matches_numpy(torch):
+    n, m, p = 7001, 12, 9
+    rng = np.random.default_rng(21)
+    Vo = rng.standard_normal((m, n))
+    C = rng.standard_normal((m, p))
+    kr = _kr(n, m)
+    W = kr.combine(torch.as_tensor(Vo, device="cuda"), C)
+    assert np.abs(W.cpu().numpy() - C.T @ Vo).max() < 1e-12 * np.abs(C.T @ Vo).max()
+    kr.close()
+
+
+def test_eigenpairs_of_the_implicit_restart(torch):
+    """IRA to convergence, then the Schur / Galerkin stage: eigenvalues and
+    eigenvectors of a non-normal operator with a known spectrum (a complex
+    pair included) against numpy's dense eigen-decomposition."""
+    n = 400
+    rng = np.random.default_rng(13)
+    lam = np.concatenate([[2.0, 1.8, 1.7, 1.7], np.linspace(1.0, 0.01, n - 4)])
+    D = np.diag(lam)
+    D[2, 3], D[3, 2] = 0.3, -0.3
+    X = np.eye(n) + 0.05 * rng.standard_normal((n, n))
+    A = X @ D @ np.linalg.inv(X)
+    kr = _kr(n, 20)
+    Am = _torch_dense_map(torch, kr, A)
+    eig, rn, it, V, H = kr.implicit_restart_arnoldi(Am, "LR", k=4, m=20, tol=1e-11,
+                                                    max_iter=300, seed=1)
+    w, Xv, res = kr.eigenpairs(Am, V, H, 4, "LR")
+    want = np.array([2.0, 1.8, 1.7 + 0.3j, 1.7 - 0.3j])
+    assert np.abs(np.sort_complex(w) - np.sort_complex(want)).max() < 1e-8
+    assert res.max() < 1e-8
+    Xn = Xv.cpu().numpy()
+    for i in range(4):
+        x = Xn[i]
+        r = A @ x - w[i] * x
+        assert np.linalg.norm(r) < 1e-8 * np.linalg.norm(x)
+    kr.close()
