@@ -232,6 +232,93 @@ ns3d_status ns3d_diagnostics(ns3d_solver* h, const ns3d_complex* ux, const ns3d_
                              const ns3d_complex* uz, double* energy, double* dissipation,
                              double* div_max);
 
+/* ----------------------------------------------------------------------- */
+/* filters, curl and the main loop's diagnostics (Source/math_support.cu:    */
+/* 680-717, 819-987; Source/NS3D_periodic.cu:1291-1452, 1853;               */
+/* Source/Shapiro_test.cu:8-50)                                             */
+/* ----------------------------------------------------------------------- */
+
+/* Helmholz_Fourier_Filter's spectral step: f = u / (1 + eps^2 |k|^2), with
+ * signed x/y wave numbers (Nyquist -N/2) and the stored z index.  Follow it
+ * with ns3d_fft_c2r for the filtered physical field, as the reference does.
+ * f may alias u.  Asynchronous on the handle's stream. */
+ns3d_status ns3d_helmholtz_filter(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                  const ns3d_complex* uz, double eps, ns3d_complex* fx,
+                                  ns3d_complex* fy, ns3d_complex* fz);
+
+/* CutOff_Fourier_Filter's spectral step as main launches it (Mz in its Nz
+ * slot): keep the modes with m^2/Nx^2 + n^2/Ny^2 + q^2/Mz^2 <= radius^2,
+ * zero the rest.  f may alias u.  Asynchronous. */
+ns3d_status ns3d_cutoff_filter(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                               const ns3d_complex* uz, double radius, ns3d_complex* fx,
+                               ns3d_complex* fy, ns3d_complex* fz);
+
+/* get_curl on physical fields [Nx][Ny][Nz]: second-order central differences
+ * with periodic wrap, including the reference's rot_y term
+ * 0.5 (uz(j+1) - ux(j-1)) / dx (it mixes uz and ux; kept so that the numbers
+ * match the reference's output).  r must not alias u.  Asynchronous. */
+ns3d_status ns3d_curl(ns3d_solver* h, const double* ux, const double* uy, const double* uz,
+                      double* rx, double* ry, double* rz);
+
+/* One line of time_dependant.dat (Source/NS3D_periodic.cu:1324-1452) from
+ * the spectral state, into host rec[NS3D_RECORD_COLUMNS]:
+ *   rec[0]      total_time (the caller's TotalTime; main adds dt twice per
+ *               step before writing it)
+ *   rec[1..21]  at the three probe points IN(Nx/2-4,Ny/2-3,Nz/2-2),
+ *               IN(Nx/3,Ny/3,Nz/3), IN(Nx/8,Ny/8,Nz/8): ux uy uz, the curl
+ *               of ns3d_curl, then energy / dissipation / energy-dissipation/Re
+ *   rec[22..28] the same at the second point for the velocity cut-off
+ *               filtered at radius 0.1, then energy
+ *   rec[29..49] Re/Im reads of the spectral state at the reference's flat
+ *               indices, with dissipation at rec[35].
+ * energy and dissipation are those of ns3d_diagnostics.  The point values are
+ * evaluated from the spectrum directly (no transforms): the same numbers as
+ * the reference's transform-then-read, to rounding.  Synchronous; returns
+ * NS3D_ERR_NONFINITE, with rec filled, when a column is not finite (main
+ * prints "nans!" and carries on).  NS3D_ERR_BAD_ARG when the grid is too
+ * small for the reference's indices. */
+#define NS3D_RECORD_COLUMNS 50
+ns3d_status ns3d_record(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                        const ns3d_complex* uz, double total_time, double Re, double* rec);
+
+/* The sums of calculate_energy_spectrum as main calls it (Source/
+ * NS3D_periodic.cu:1853, Mz in its Nz slot): E[n] = sum over j < Nx/2,
+ * k < Ny/2, l < Mz with j + k + l = n of |u_hat|^2 / (Nx Ny Mz)^2, summed over
+ * the three components; nbins must be Nx/2 + Ny/2 + Nz/2 + 1.  Host E.
+ * Synchronous.  ns3d_write_energy_spectrum_host writes Ek.dat from it. */
+ns3d_status ns3d_energy_spectrum(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                 const ns3d_complex* uz, double* E, int nbins);
+
+/* Shapiro's exact Beltrami solution (Initial_Shapiro, Source/
+ * NS3D_periodic.cu:807-829) at time t, transformed to spectral fields.  The
+ * formula is the reference's for a 2 pi box.  Asynchronous. */
+ns3d_status ns3d_shapiro_state(ns3d_solver* h, double t, double Re, ns3d_complex* ux,
+                               ns3d_complex* uy, ns3d_complex* uz);
+
+/* Shapiro_test_case on physical fields: min_max[0..1] = min and max over
+ * the grid of |u - u_exact(t)|; the reference returns the max.  Synchronous. */
+ns3d_status ns3d_shapiro_error_physical(ns3d_solver* h, const double* ux, const double* uy,
+                                        const double* uz, double t, double Re, double* min_max);
+
+/* The same from the spectral state (inverse transform first): err = max. */
+ns3d_status ns3d_shapiro_error(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                               const ns3d_complex* uz, double t, double Re, double* err);
+
+/* Host-only writers of the two diagnostic files.  A series is the main
+ * loop's time_dependant.dat: ns3d_series_open truncates the file (fopen
+ * "w"), each ns3d_series_write appends one line of ncols "%le" fields
+ * separated by single spaces, ns3d_series_close flushes and closes. */
+typedef struct ns3d_series ns3d_series;
+ns3d_status ns3d_series_open(const char* path, ns3d_series** out);
+ns3d_status ns3d_series_write(ns3d_series* s, const double* rec, int ncols);
+ns3d_status ns3d_series_close(ns3d_series* s);
+
+/* Ek.dat as calculate_energy_spectrum writes it from E of
+ * ns3d_energy_spectrum: per bin "%i %.16le %.16le" of n, E[n]/2 and
+ * 0.25 n^(-5/3) (inf at n = 0); bins no mode reaches print "0 0 0". */
+ns3d_status ns3d_write_energy_spectrum_host(const char* path, int Nx, int Ny, int Nz,
+                                            const double* E);
+
 /* Times the five pass kernels of one RHS evaluation (the first RK3 stage:
  * inv_x, inv_y, z, fwd_y, fwd_x; u is read, handle scratch is written) with
  * CUDA events on the handle's stream, `reps` times after one warm-up, and

@@ -3,8 +3,8 @@
  *
  * libns3d_compat.so defines these functions with the exact signatures of
  * evstigneevnm/NS3DPeriodic's headers (RK_time_step.h:17-34,
- * advection_2_3.h:38-46, diffusion.h:12-24, math_support.h:15,29-37,49-63,
- * divergence.h:13-15, advection_WENO.h:22-23; `real` = double, `cudaComplex`
+ * advection_2_3.h:38-46, diffusion.h:12-24, math_support.h:15,29-37,45,49-73,
+ * divergence.h:13-15, advection_WENO.h:22-23, Shapiro_test.h:13; `real` = double, `cudaComplex`
  * = cufftDoubleComplex), so code written against those headers links
  * against this library unchanged.  Each function forwards to include/ns3d.h
  * (one ns3d_solver per grid and box, created on first use and kept until
@@ -251,6 +251,36 @@ double get_kinetic_energy(dim3 dimGrid, dim3 dimBlock, int Nx, int Ny, int Nz, d
 double get_dissipation(dim3 dimGrid, dim3 dimBlock, int Nx, int Ny, int Nz, double dx, double dy,
                        double dz, double* ux_d, double* uy_d, double* uz_d, double* dissipation,
                        double* energy_out, double* energy_out1);
+/* get_curl: on the handle of (Nx, Ny, Nz, dx*N...).  calculate_energy_spectrum
+ * runs on the host arrays it is given, in the reference's order, and writes
+ * the same text.  The two filters ignore Mz (it is Nz/2+1) and write the
+ * filtered spectra and their scaled inverse transforms, as the reference. */
+void get_curl(dim3 dimGrid, dim3 dimBlock, int Nx, int Ny, int Nz, double dx, double dy,
+              double dz, double* ux_d, double* uy_d, double* uz_d, double* rot_x_d,
+              double* rot_y_d, double* rot_z_d);
+void calculate_energy_spectrum(char* file_name, int Nx, int Ny, int Mz, double* ux_hat_Re,
+                               double* ux_hat_Im, double* uy_hat_Re, double* uy_hat_Im,
+                               double* uz_hat_Re, double* uz_hat_Im);
+void Helmholz_Fourier_Filter(dim3 dimGrid, dim3 dimBlock, dim3 dimGrid_C, dim3 dimBlock_C, int Nx,
+                             int Ny, int Nz, int Mz, double Lx, double Ly, double Lz,
+                             cufftDoubleComplex* ux_hat_d, cufftDoubleComplex* uy_hat_d,
+                             cufftDoubleComplex* uz_hat_d, cufftDoubleComplex* ux_filt_hat_d,
+                             cufftDoubleComplex* uy_filt_hat_d, cufftDoubleComplex* uz_filt_hat_d,
+                             double filter_eps, double* ux_filt_d, double* uy_filt_d,
+                             double* uz_filt_d);
+void CutOff_Fourier_Filter(dim3 dimGrid, dim3 dimBlock, dim3 dimGrid_C, dim3 dimBlock_C, int Nx,
+                           int Ny, int Nz, int Mz, double Lx, double Ly, double Lz,
+                           cufftDoubleComplex* ux_hat_d, cufftDoubleComplex* uy_hat_d,
+                           cufftDoubleComplex* uz_hat_d, cufftDoubleComplex* ux_filt_hat_d,
+                           cufftDoubleComplex* uy_filt_hat_d, cufftDoubleComplex* uz_filt_hat_d,
+                           double Radius_to_one, double* ux_filt_d, double* uy_filt_d,
+                           double* uz_filt_d);
+
+/* Shapiro_test.h: returns max |u - u_exact(t)| and stores (min, max) in
+ * ret[0..1]; the scratch arrays cfl_in / cfl_out are not written. */
+double Shapiro_test_case(dim3 dimGrid, dim3 dimBlock, double dx, double dy, double dz,
+                         double current_time, double Re, double* ux, double* uy, double* uz,
+                         int Nx, int Ny, int Nz, double* cfl_in, double* cfl_out, double* ret);
 
 /* divergence.h */
 void divergence_device(dim3 dimGrid_C, dim3 dimBlock_C, int Nx, int Ny, int Nz,

@@ -40,6 +40,10 @@ EXPORTS = (
     "ns3d_krylov_last_error", "ns3d_arnoldi", "ns3d_krylov_stats", "ns3d_qr_shifts",
     "ns3d_ira_restart", "ns3d_krylov_profile", "ns3d_krylov_combine", "ns3d_bicgstabl", "ns3d_newton",
     "ns3d_map_rhs", "ns3d_map_linearised", "ns3d_map_exponential", "ns3d_map_laplace1d",
+    "ns3d_helmholtz_filter", "ns3d_cutoff_filter", "ns3d_curl", "ns3d_record",
+    "ns3d_energy_spectrum", "ns3d_shapiro_state", "ns3d_shapiro_error_physical",
+    "ns3d_shapiro_error", "ns3d_series_open", "ns3d_series_write", "ns3d_series_close",
+    "ns3d_write_energy_spectrum_host",
 )
 
 # the matrix-vector callback type of ns3d_arnoldi: void (*)(void*, void*, void*)
@@ -145,6 +149,18 @@ def _sig(lib):
         "ns3d_map_linearised": ([_P, _P, _P], None),
         "ns3d_map_exponential": ([_P, _P, _P], None),
         "ns3d_map_laplace1d": ([_P, _P, _P], None),
+        "ns3d_helmholtz_filter": ([_P, _P, _P, _P, c_double, _P, _P, _P], c_int),
+        "ns3d_cutoff_filter": ([_P, _P, _P, _P, c_double, _P, _P, _P], c_int),
+        "ns3d_curl": ([_P] + [_P] * 6, c_int),
+        "ns3d_record": ([_P, _P, _P, _P, c_double, c_double, _P], c_int),
+        "ns3d_energy_spectrum": ([_P, _P, _P, _P, _P, c_int], c_int),
+        "ns3d_shapiro_state": ([_P, c_double, c_double, _P, _P, _P], c_int),
+        "ns3d_shapiro_error_physical": ([_P, _P, _P, _P, c_double, c_double, _P], c_int),
+        "ns3d_shapiro_error": ([_P, _P, _P, _P, c_double, c_double, _P], c_int),
+        "ns3d_series_open": ([ctypes.c_char_p, ctypes.POINTER(c_void_p)], c_int),
+        "ns3d_series_write": ([_P, _P, c_int], c_int),
+        "ns3d_series_close": ([_P], c_int),
+        "ns3d_write_energy_spectrum_host": ([ctypes.c_char_p, c_int, c_int, c_int, _P], c_int),
     }
     for name, (args, res) in S.items():
         f = getattr(lib, name)

@@ -23,7 +23,8 @@ COMPAT_LIB = os.path.join(HERE, "libns3d_compat.so")
 COMPAT_SOURCE = "compat.cu"
 
 SOURCES = ["k_xy.cu", "k_z.cu", "k_fwdx.cu", "k_fft3d.cu", "aux_kernels.cu", "solver.cu",
-           "noalloc.cu", "krylov.cu", "qr_shifts.cpp", "checkpoint.cpp"]
+           "noalloc.cu", "krylov.cu", "qr_shifts.cpp", "checkpoint.cpp",
+           "diag_kernels.cu", "series.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",

@@ -595,6 +595,77 @@ void all_double2Fourier(dim3, dim3, double* ux_re, double* ux_im, cplx* ux_hat, 
   merge_complex<<<grid_for(n), 256>>>(uz_re, uz_im, uz_hat, n);
 }
 
+void get_curl(dim3, dim3, int Nx, int Ny, int Nz, double dx, double dy, double dz, double* ux,
+              double* uy, double* uz, double* rx, double* ry, double* rz) {
+  Entry* e = entry_from_steps(Nx, Ny, Nz, dx, dy, dz);
+  report(ns3d_curl(e->h, ux, uy, uz, rx, ry, rz), e->h, "get_curl", false);
+}
+
+namespace {
+void filter_then_c2r(bool helmholtz, int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                     cplx* ux_hat, cplx* uy_hat, cplx* uz_hat, cplx* fx_hat, cplx* fy_hat,
+                     cplx* fz_hat, double p, double* fx, double* fy, double* fz) {
+  Entry* e = entry_for(Nx, Ny, Nz, Lx, Ly, Lz);
+  const ns3d_status s =
+      helmholtz ? ns3d_helmholtz_filter(e->h, C(ux_hat), C(uy_hat), C(uz_hat), p, C(fx_hat),
+                                        C(fy_hat), C(fz_hat))
+                : ns3d_cutoff_filter(e->h, C(ux_hat), C(uy_hat), C(uz_hat), p, C(fx_hat),
+                                     C(fy_hat), C(fz_hat));
+  report(s, e->h, helmholtz ? "Helmholz_Fourier_Filter" : "CutOff_Fourier_Filter", false);
+  report(ns3d_fft_c2r(e->h, C(fx_hat), fx), e->h, "*CUFFT C->R*", false);
+  report(ns3d_fft_c2r(e->h, C(fy_hat), fy), e->h, "*CUFFT C->R*", false);
+  report(ns3d_fft_c2r(e->h, C(fz_hat), fz), e->h, "*CUFFT C->R*", false);
+}
+}  // namespace
+
+void Helmholz_Fourier_Filter(dim3, dim3, dim3, dim3, int Nx, int Ny, int Nz, int, double Lx,
+                             double Ly, double Lz, cplx* ux_hat, cplx* uy_hat, cplx* uz_hat,
+                             cplx* fx_hat, cplx* fy_hat, cplx* fz_hat, double eps, double* fx,
+                             double* fy, double* fz) {
+  filter_then_c2r(true, Nx, Ny, Nz, Lx, Ly, Lz, ux_hat, uy_hat, uz_hat, fx_hat, fy_hat, fz_hat,
+                  eps, fx, fy, fz);
+}
+
+void CutOff_Fourier_Filter(dim3, dim3, dim3, dim3, int Nx, int Ny, int Nz, int, double Lx,
+                           double Ly, double Lz, cplx* ux_hat, cplx* uy_hat, cplx* uz_hat,
+                           cplx* fx_hat, cplx* fy_hat, cplx* fz_hat, double radius, double* fx,
+                           double* fy, double* fz) {
+  filter_then_c2r(false, Nx, Ny, Nz, Lx, Ly, Lz, ux_hat, uy_hat, uz_hat, fx_hat, fy_hat, fz_hat,
+                  radius, fx, fy, fz);
+}
+
+void calculate_energy_spectrum(char* file_name, int Nx, int Ny, int Mz, double* ux_re,
+                               double* ux_im, double* uy_re, double* uy_im, double* uz_re,
+                               double* uz_im) {
+  // host arrays, summed in the reference's loop order so the text is identical
+  const int size = Nx / 2 + Ny / 2 + Mz;
+  const int norm = Nx * Ny * Mz;
+  std::vector<double> E(size, 0.0);
+  for (int j = 0; j < Nx / 2; ++j)
+    for (int k = 0; k < Ny / 2; ++k)
+      for (int l = 0; l < Mz; ++l) {
+        const size_t i = ((size_t)j * Ny + k) * Mz + l;
+        const int n = j + k + l;
+        E[n] += ux_re[i] * ux_re[i] / norm / norm + ux_im[i] * ux_im[i] / norm / norm;
+        E[n] += uy_re[i] * uy_re[i] / norm / norm + uy_im[i] * uy_im[i] / norm / norm;
+        E[n] += uz_re[i] * uz_re[i] / norm / norm + uz_im[i] * uz_im[i] / norm / norm;
+      }
+  report(ns3d_write_energy_spectrum_host(file_name, Nx, Ny, 2 * (Mz - 1), E.data()), nullptr,
+         "calculate_energy_spectrum", false);
+}
+
+double Shapiro_test_case(dim3, dim3, double dx, double dy, double dz, double t, double Re,
+                         double* ux, double* uy, double* uz, int Nx, int Ny, int Nz, double*,
+                         double*, double* ret) {
+  Entry* e = entry_from_steps(Nx, Ny, Nz, dx, dy, dz);
+  double mm[2] = {0.0, 0.0};
+  report(ns3d_shapiro_error_physical(e->h, ux, uy, uz, t, Re, mm), e->h, "Shapiro_test_case",
+         false);
+  ret[0] = mm[0];
+  ret[1] = mm[1];
+  return mm[1];
+}
+
 namespace {
 // signed wavenumber index of the x / y tables (j >= N/2 -> j - N)
 inline int sidx(int j, int n) { return j >= n / 2 ? j - n : j; }

@@ -10,6 +10,7 @@
 
 #include "../../include/ns3d.h"
 #include "aux_kernels.cuh"
+#include "diag_kernels.cuh"
 #include "dispatch.h"
 
 using ns3d::FwdXArgs;
@@ -58,6 +59,12 @@ struct ns3d_solver {
   // diagnostics
   double* diag_partial = nullptr;
   double* diag_out = nullptr;
+  // record / spectrum / Shapiro buffers (allocated on first use)
+  double2* rec_tab = nullptr;
+  double* rec_partial = nullptr;  // kDiagBlocks x kRecordSums, then 2 x kDiagBlocks min/max
+  double* rec_out = nullptr;      // 50 record columns, then 2 min/max
+  ns3d::RecordReads rec_reads{};
+  long long rec_points[3] = {};
   // cached RK3 step graph
   cudaGraphExec_t rk3_exec = nullptr;
   const void* rk3_key[3] = {};
@@ -400,6 +407,9 @@ ns3d_status ns3d_destroy(ns3d_solver* h) {
   cudaFree(h->f_val);
   cudaFree(h->diag_partial);
   cudaFree(h->diag_out);
+  cudaFree(h->rec_tab);
+  cudaFree(h->rec_partial);
+  cudaFree(h->rec_out);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return NS3D_OK;
@@ -836,6 +846,255 @@ ns3d_status ns3d_diagnostics(ns3d_solver* h, const ns3d_complex* ux, const ns3d_
   if (div_max) *div_max = r[2];
   if (!std::isfinite(r[0]) || !std::isfinite(r[1]) || !std::isfinite(r[2]))
     return fail(h, NS3D_ERR_NONFINITE, "diagnostics are not finite");
+  return NS3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Filters, curl, the per-step record, the energy spectrum, Shapiro's solution
+// ---------------------------------------------------------------------------
+
+namespace {
+
+ns3d::GridGeom grid_geom(const ns3d_solver* h) {
+  ns3d::GridGeom g{};
+  g.Nx = h->Nx; g.Ny = h->Ny; g.Nz = h->Nz;
+  g.dx = h->Lx / (double)h->Nx;
+  g.dy = h->Ly / (double)h->Ny;
+  g.dz = h->Lz / (double)h->Nz;
+  return g;
+}
+
+int elementwise_blocks(long long n) {
+  const long long b = (n + kDiagThreads - 1) / kDiagThreads;
+  return (int)(b < 8 * kDiagBlocks ? (b > 0 ? b : 1) : 8 * kDiagBlocks);
+}
+
+// The probe points and spectral reads of the main loop's record
+// (Source/NS3D_periodic.cu:1357-1450, IN of Source/Macros.h:11 with the
+// physical Nz, then with Nz = Mz), and the phase tables of
+// record_partial_kernel.  Allocated on first use.
+ns3d_status ensure_record(ns3d_solver* h) {
+  if (h->rec_tab) return NS3D_OK;
+  const long long Nx = h->Nx, Ny = h->Ny, Nz = h->Nz, Mz = h->Mz;
+  auto in_r = [&](long long i, long long j, long long k) { return i * (Ny * Nz) + j * Nz + k; };
+  auto in_c = [&](long long i, long long j, long long k) { return i * (Ny * Mz) + j * Mz + k; };
+  const long long P[3] = {in_r(Nx / 2 - 4, Ny / 2 - 3, Nz / 2 - 2), in_r(Nx / 3, Ny / 3, Nz / 3),
+                          in_r(Nx / 8, Ny / 8, Nz / 8)};
+  const long long F[11] = {in_c(Nx - 6, Ny - 6, Mz - 6), in_c(Nx / 5, Ny / 4 - 3, Mz / 4 - 1),
+                           in_c(Nx / 5, Ny / 5, Mz / 5),  in_c(2, 2, 2),
+                           in_c(1, 0, 0),                 in_c(0, 0, 0),
+                           in_c(1, 1, 0),                 in_c(1, 1, 1),
+                           in_c(Nx - 1, 0, 0),            in_c(Nx - 1, Ny - 1, 0),
+                           in_c(Nx - 1, Ny - 1, Mz - 1)};
+  for (long long p : P)
+    if (p < 0 || p >= Nx * Ny * Nz)
+      return fail(h, NS3D_ERR_BAD_ARG, "grid too small for the record's probe points");
+  for (long long f : F)
+    if (f < 0 || f >= (long long)h->nc)
+      return fail(h, NS3D_ERR_BAD_ARG, "grid too small for the record's spectral reads");
+  const int nx = h->Nx, ny = h->Ny, mz = h->Mz;
+  std::vector<double2> tab((size_t)ns3d::record_table_size(nx, ny, mz));
+  auto phase = [](long long r, long long n) {
+    const double a = 2.0 * M_PI * (double)r / (double)n;
+    return make_double2(std::cos(a), std::sin(a));
+  };
+  size_t o = 0;
+  const long long ext[3] = {Nx, Ny, Mz};
+  for (int axis = 0; axis < 3; ++axis)
+    for (int s = 0; s < 3; ++s) {
+      const long long p = P[s];
+      const long long c[3] = {p / (Ny * Nz), (p / Nz) % Ny, p % Nz};
+      const long long n = axis == 0 ? Nx : axis == 1 ? Ny : Nz;
+      for (long long j = 0; j < ext[axis]; ++j) tab[o++] = phase((j * c[axis]) % n, n);
+    }
+  for (long long j = 0; j < Nx; ++j) tab[o++] = phase(j, Nx);
+  const double h3[3] = {h->Lx / Nx, h->Ly / Ny, h->Lz / Nz};
+  for (int axis = 0; axis < 3; ++axis) {
+    const long long n = axis == 0 ? Nx : axis == 1 ? Ny : Nz;
+    for (long long j = 0; j < ext[axis]; ++j)
+      tab[o++] = make_double2(std::sin(2.0 * M_PI * (double)j / (double)n) / h3[axis], 0.0);
+  }
+  for (int i = 0; i < 11; ++i) h->rec_reads.f[i] = F[i];
+  for (int i = 0; i < 3; ++i) h->rec_points[i] = P[i];
+  double2* t = nullptr;
+  double* part = nullptr;
+  double* out = nullptr;
+  cudaError_t e = cudaMalloc(&t, sizeof(double2) * tab.size());
+  if (e == cudaSuccess) e = cudaMalloc(&part, sizeof(double) * ns3d::kRecordSums * kDiagBlocks);
+  if (e == cudaSuccess) e = cudaMalloc(&out, sizeof(double) * 64);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(t, tab.data(), sizeof(double2) * tab.size(), cudaMemcpyHostToDevice,
+                        h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    cudaFree(t);
+    cudaFree(part);
+    cudaFree(out);
+    return cuda_fail(h, e, "record buffers");
+  }
+  h->rec_tab = t;
+  h->rec_partial = part;
+  h->rec_out = out;
+  return NS3D_OK;
+}
+
+ns3d_status spectral_filter(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                            const ns3d_complex* uz, int mode, double p, ns3d_complex* fx,
+                            ns3d_complex* fy, ns3d_complex* fz) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(ux, uy, uz) || !args_ok3(fx, fy, fz)) return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  if (!std::isfinite(p)) return fail(h, NS3D_ERR_BAD_ARG, "filter parameter not finite");
+  ns3d::FilterGeom g{h->Nx, h->Ny, h->Mz, h->Lx, h->Ly, h->Lz};
+  ns3d::spectral_filter_kernel<<<elementwise_blocks((long long)h->nc), kDiagThreads, 0,
+                                 h->stream>>>((const double2*)ux, (const double2*)uy,
+                                              (const double2*)uz, (double2*)fx, (double2*)fy,
+                                              (double2*)fz, g, mode, p);
+  NS3D_CHECK(h, cudaGetLastError(), "spectral_filter");
+  return NS3D_OK;
+}
+
+ns3d_status diag_sums(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                      const ns3d_complex* uz) {
+  ns3d::DiagGeom g{};
+  g.Nx = h->Nx; g.Ny = h->Ny; g.Nz = h->Nz; g.Mz = h->Mz;
+  g.kfx = h->geom.kfx; g.kfy = h->geom.kfy; g.kfz = h->geom.kfz;
+  g.dx = h->Lx / (double)h->Nx;
+  g.dy = h->Ly / (double)h->Ny;
+  g.dz = h->Lz / (double)h->Nz;
+  g.inv_vol = h->geom.inv_vol;
+  ns3d::diag_partial_kernel<<<kDiagBlocks, kDiagThreads, 0, h->stream>>>(
+      (const double2*)ux, (const double2*)uy, (const double2*)uz, g, h->diag_partial);
+  NS3D_CHECK(h, cudaGetLastError(), "diag_partial");
+  ns3d::diag_final_kernel<<<1, 1024, 0, h->stream>>>(h->diag_partial, kDiagBlocks, h->diag_out);
+  NS3D_CHECK(h, cudaGetLastError(), "diag_final");
+  return NS3D_OK;
+}
+
+ns3d_status shapiro_minmax(ns3d_solver* h, const double* ux, const double* uy, const double* uz,
+                           double t, double Re, double* mm) {
+  NS3D_TRY(ensure_record(h));
+  const double f = std::sqrt(3.0);
+  const double decay = std::exp(-(f * f) * t / Re);
+  ns3d::shapiro_error_kernel<<<kDiagBlocks, kDiagThreads, 0, h->stream>>>(
+      ux, uy, uz, grid_geom(h), decay, h->rec_partial);
+  NS3D_CHECK(h, cudaGetLastError(), "shapiro_error");
+  ns3d::minmax_final_kernel<<<1, 1024, 0, h->stream>>>(h->rec_partial, kDiagBlocks,
+                                                       h->rec_out + 50);
+  NS3D_CHECK(h, cudaGetLastError(), "minmax_final");
+  NS3D_CHECK(h, cudaMemcpyAsync(mm, h->rec_out + 50, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                h->stream), "shapiro copy");
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "shapiro sync");
+  return NS3D_OK;
+}
+
+}  // namespace
+
+ns3d_status ns3d_helmholtz_filter(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                  const ns3d_complex* uz, double eps, ns3d_complex* fx,
+                                  ns3d_complex* fy, ns3d_complex* fz) {
+  return spectral_filter(h, ux, uy, uz, 0, eps, fx, fy, fz);
+}
+
+ns3d_status ns3d_cutoff_filter(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                               const ns3d_complex* uz, double radius, ns3d_complex* fx,
+                               ns3d_complex* fy, ns3d_complex* fz) {
+  return spectral_filter(h, ux, uy, uz, 1, radius, fx, fy, fz);
+}
+
+ns3d_status ns3d_curl(ns3d_solver* h, const double* ux, const double* uy, const double* uz,
+                      double* rx, double* ry, double* rz) {
+  NS3D_TRY(check_handle(h));
+  if (!ux || !uy || !uz || !rx || !ry || !rz) return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  const long long n = (long long)h->Nx * h->Ny * h->Nz;
+  ns3d::curl_kernel<<<elementwise_blocks(n), kDiagThreads, 0, h->stream>>>(ux, uy, uz, rx, ry, rz,
+                                                                           grid_geom(h));
+  NS3D_CHECK(h, cudaGetLastError(), "curl");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_record(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                        const ns3d_complex* uz, double total_time, double Re, double* rec) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(ux, uy, uz) || !rec) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  if (!(Re > 0.0) || !std::isfinite(Re)) return fail(h, NS3D_ERR_BAD_ARG, "Re must be > 0");
+  NS3D_TRY(ensure_record(h));
+  NS3D_TRY(diag_sums(h, ux, uy, uz));
+  ns3d::RecordGeom g{};
+  g.Nx = h->Nx; g.Ny = h->Ny; g.Nz = h->Nz; g.Mz = h->Mz;
+  g.dx = h->Lx / (double)h->Nx;
+  g.dy = h->Ly / (double)h->Ny;
+  g.dz = h->Lz / (double)h->Nz;
+  g.cut2 = 0.1 * 0.1;  // CutOff_Fourier_Filter(..., 0.1, ...) of the main loop
+  ns3d::record_partial_kernel<<<kDiagBlocks, kDiagThreads, 0, h->stream>>>(
+      (const double2*)ux, (const double2*)uy, (const double2*)uz, g, h->rec_tab, h->rec_partial);
+  NS3D_CHECK(h, cudaGetLastError(), "record_partial");
+  ns3d::record_final_kernel<<<1, 32 * ns3d::kRecordSums, 0, h->stream>>>(
+      h->rec_partial, kDiagBlocks, h->diag_out, (const double2*)ux, (const double2*)uy,
+      (const double2*)uz, h->rec_reads, total_time, Re, h->geom.inv_vol, h->rec_out);
+  NS3D_CHECK(h, cudaGetLastError(), "record_final");
+  NS3D_CHECK(h, cudaMemcpyAsync(rec, h->rec_out, sizeof(double) * NS3D_RECORD_COLUMNS,
+                                cudaMemcpyDeviceToHost, h->stream), "record copy");
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "record sync");
+  for (int i = 0; i < NS3D_RECORD_COLUMNS; ++i)
+    if (!std::isfinite(rec[i])) return fail(h, NS3D_ERR_NONFINITE, "record is not finite");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_energy_spectrum(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                 const ns3d_complex* uz, double* E, int nbins) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(ux, uy, uz) || !E) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  const int size = h->Nx / 2 + h->Ny / 2 + h->Mz;
+  if (nbins != size) return fail(h, NS3D_ERR_BAD_ARG, "nbins must be Nx/2 + Ny/2 + Nz/2 + 1");
+  double* d = reinterpret_cast<double*>(h->B[0]);  // nc complex >= size doubles
+  const double norm = (double)h->Nx * (double)h->Ny * (double)h->Mz;
+  ns3d::spectrum_kernel<<<size, kDiagThreads, 0, h->stream>>>(
+      (const double2*)ux, (const double2*)uy, (const double2*)uz, h->Nx, h->Ny, h->Mz, norm, d);
+  NS3D_CHECK(h, cudaGetLastError(), "spectrum");
+  NS3D_CHECK(h, cudaMemcpyAsync(E, d, sizeof(double) * size, cudaMemcpyDeviceToHost, h->stream),
+             "spectrum copy");
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "spectrum sync");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_shapiro_state(ns3d_solver* h, double t, double Re, ns3d_complex* ux,
+                               ns3d_complex* uy, ns3d_complex* uz) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(ux, uy, uz)) return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  if (!(Re > 0.0) || !std::isfinite(t)) return fail(h, NS3D_ERR_BAD_ARG, "bad t or Re");
+  const double f = std::sqrt(3.0);
+  const double decay = std::exp(-(f * f) * t / Re);
+  double* p[3];
+  for (int c = 0; c < 3; ++c) p[c] = reinterpret_cast<double*>(h->B[c]);
+  const long long n = (long long)h->Nx * h->Ny * h->Nz;
+  ns3d::shapiro_field_kernel<<<elementwise_blocks(n), kDiagThreads, 0, h->stream>>>(
+      p[0], p[1], p[2], grid_geom(h), decay);
+  NS3D_CHECK(h, cudaGetLastError(), "shapiro_field");
+  ns3d_complex* out[3] = {ux, uy, uz};
+  for (int c = 0; c < 3; ++c) NS3D_TRY(ns3d_fft_r2c(h, p[c], out[c]));
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_shapiro_error_physical(ns3d_solver* h, const double* ux, const double* uy,
+                                        const double* uz, double t, double Re, double* min_max) {
+  NS3D_TRY(check_handle(h));
+  if (!ux || !uy || !uz || !min_max) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  if (!(Re > 0.0) || !std::isfinite(t)) return fail(h, NS3D_ERR_BAD_ARG, "bad t or Re");
+  return shapiro_minmax(h, ux, uy, uz, t, Re, min_max);
+}
+
+ns3d_status ns3d_shapiro_error(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                               const ns3d_complex* uz, double t, double Re, double* err) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(ux, uy, uz) || !err) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  if (!(Re > 0.0) || !std::isfinite(t)) return fail(h, NS3D_ERR_BAD_ARG, "bad t or Re");
+  double* p[3];
+  for (int c = 0; c < 3; ++c) p[c] = reinterpret_cast<double*>(h->B[c]);
+  const ns3d_complex* u[3] = {ux, uy, uz};
+  for (int c = 0; c < 3; ++c) NS3D_TRY(ns3d_fft_c2r(h, u[c], p[c]));
+  double mm[2];
+  NS3D_TRY(shapiro_minmax(h, p[0], p[1], p[2], t, Re, mm));
+  *err = mm[1];
   return NS3D_OK;
 }
 

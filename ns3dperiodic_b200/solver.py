@@ -295,6 +295,84 @@ class Solver:
         return e.value, d.value, dv.value
 
 
+    # -- filters, curl and the main loop's record (Source/math_support.cu,
+    #    Source/NS3D_periodic.cu:1291-1452, Source/Shapiro_test.cu) ----------
+    def _real_fields(self, F: Sequence, name: str):
+        t = self._torch
+        if len(F) != 3:
+            raise ValueError(f"{name}: need 3 components")
+        for f in F:
+            if (not isinstance(f, t.Tensor) or f.dtype != t.float64 or f.device != self.device
+                    or tuple(f.shape) != self.real_shape or not f.is_contiguous()):
+                raise ValueError(f"{name}: expected contiguous float64 {self.real_shape} tensors "
+                                 f"on {self.device}")
+        return [_ptr(f) for f in F]
+
+    def helmholtz_filter(self, U, eps: float, out=None):
+        """Helmholz_Fourier_Filter's spectral step: u / (1 + eps^2 |k|^2)."""
+        out = out if out is not None else self.zeros()
+        self._check(self._L.ns3d_helmholtz_filter(self._h, *self._fields(U, "U"), float(eps),
+                                                  *self._fields(out, "out")),
+                    "ns3d_helmholtz_filter")
+        return out
+
+    def cutoff_filter(self, U, radius: float, out=None):
+        """CutOff_Fourier_Filter's spectral step (Mz in its Nz slot)."""
+        out = out if out is not None else self.zeros()
+        self._check(self._L.ns3d_cutoff_filter(self._h, *self._fields(U, "U"), float(radius),
+                                               *self._fields(out, "out")),
+                    "ns3d_cutoff_filter")
+        return out
+
+    def curl(self, u, out=None):
+        """get_curl of physical (Nx, Ny, Nz) float64 fields."""
+        t = self._torch
+        out = out if out is not None else [t.empty(self.real_shape, dtype=t.float64,
+                                                   device=self.device) for _ in range(3)]
+        self._check(self._L.ns3d_curl(self._h, *self._real_fields(u, "u"),
+                                      *self._real_fields(out, "out")), "ns3d_curl")
+        return out
+
+    def record(self, U, total_time: float, Re: float):
+        """The 50 columns of one time_dependant.dat line (numpy array)."""
+        import numpy as np
+
+        rec = np.zeros(RECORD_COLUMNS)
+        rc = self._L.ns3d_record(self._h, *self._fields(U, "U"), float(total_time), float(Re),
+                                 rec.ctypes.data)
+        if rc == 5:  # non-finite: the record is filled, as main writes it anyway
+            return rec
+        self._check(rc, "ns3d_record")
+        return rec
+
+    def energy_spectrum(self, U):
+        """calculate_energy_spectrum's per-bin sums E[n] (numpy array)."""
+        import numpy as np
+
+        nb = self.Nx // 2 + self.Ny // 2 + self.Mz
+        E = np.zeros(nb)
+        self._check(self._L.ns3d_energy_spectrum(self._h, *self._fields(U, "U"), E.ctypes.data,
+                                                 nb), "ns3d_energy_spectrum")
+        return E
+
+    def write_energy_spectrum(self, path: str, U):
+        """Ek.dat of the state, as main writes it at the end of a run."""
+        write_energy_spectrum(path, self.Nx, self.Ny, self.Nz, self.energy_spectrum(U))
+
+    def shapiro_state(self, t: float, Re: float, out=None):
+        """Shapiro's exact Beltrami solution at time t, spectral."""
+        out = out if out is not None else self.zeros()
+        self._check(self._L.ns3d_shapiro_state(self._h, float(t), float(Re),
+                                               *self._fields(out, "out")), "ns3d_shapiro_state")
+        return out
+
+    def shapiro_error(self, U, t: float, Re: float) -> float:
+        """Shapiro_test_case: max |u - u_exact(t)| over the grid."""
+        e = ctypes.c_double()
+        self._check(self._L.ns3d_shapiro_error(self._h, *self._fields(U, "U"), float(t),
+                                               float(Re), ctypes.byref(e)), "ns3d_shapiro_error")
+        return e.value
+
     def profile_passes(self, U, dt: float, Re: float, reps: int = 10):
         """Mean ms per launch of (inv_x, inv_y, z, fwd_y, fwd_x), CUDA events."""
         ms = (ctypes.c_double * 5)()
@@ -357,3 +435,62 @@ def read_control_file(path: str, Nx: int, Ny: int, Nz: int):
     if rc != 0:
         raise Ns3dError(rc, "ns3d_read_control_file_host", str(path))
     return u
+
+
+RECORD_COLUMNS = 50
+
+
+class TimeSeries:
+    """time_dependant.dat of the main loop (ns3d_series_*): one line of 50
+    '%le' columns per ``write``.  ``step`` advances the time the reference's
+    way (TotalTime += dt twice per step, Source/NS3D_periodic.cu:1355,1374),
+    computes the record on the device and writes it."""
+
+    def __init__(self, path: str, total_time: float = 0.0):
+        self._L = lib()
+        h = ctypes.c_void_p()
+        rc = self._L.ns3d_series_open(str(path).encode(), ctypes.byref(h))
+        if rc != 0:
+            raise Ns3dError(rc, "ns3d_series_open", str(path))
+        self._s = h
+        self.total_time = float(total_time)
+
+    def write(self, rec):
+        import numpy as np
+
+        r = np.ascontiguousarray(rec, dtype=np.float64)
+        rc = self._L.ns3d_series_write(self._s, r.ctypes.data, int(r.size))
+        if rc != 0:
+            raise Ns3dError(rc, "ns3d_series_write", "")
+
+    def step(self, solver: "Solver", U, dt: float, Re: float):
+        self.total_time += dt
+        self.total_time += dt
+        rec = solver.record(U, self.total_time, Re)
+        self.write(rec)
+        return rec
+
+    def close(self):
+        if self._s:
+            rc = self._L.ns3d_series_close(self._s)
+            self._s = None
+            if rc != 0:
+                raise Ns3dError(rc, "ns3d_series_close", "")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def write_energy_spectrum(path: str, Nx: int, Ny: int, Nz: int, E):
+    """Ek.dat from the per-bin sums E (ns3d_write_energy_spectrum_host)."""
+    import numpy as np
+
+    e = np.ascontiguousarray(E, dtype=np.float64)
+    if e.size != Nx // 2 + Ny // 2 + Nz // 2 + 1:
+        raise ValueError("E must have Nx/2 + Ny/2 + Nz/2 + 1 bins")
+    rc = lib().ns3d_write_energy_spectrum_host(str(path).encode(), Nx, Ny, Nz, e.ctypes.data)
+    if rc != 0:
+        raise Ns3dError(rc, "ns3d_write_energy_spectrum_host", str(path))

@@ -515,3 +515,155 @@ def rel_l2(A, B) -> float:
     num = sum(float(np.vdot(A[i] - B[i], A[i] - B[i]).real) for i in range(len(A)))
     den = sum(float(np.vdot(B[i], B[i]).real) for i in range(len(B)))
     return math.sqrt(num / den) if den > 0 else math.sqrt(num)
+
+
+# ---------------------------------------------------------------------------
+# Filters, curl, the per-step diagnostic record and the energy spectrum
+# (Source/math_support.cu:680-717,819-987; Source/NS3D_periodic.cu:1291-1452,
+# 1853; Source/Shapiro_test.cu:8-50)
+# ---------------------------------------------------------------------------
+
+def helmholtz_filter(g: Grid, U, eps: float):
+    """Helmholz_Fourier_Filter_Device (math_support.cu:866-907): u/(1+eps^2|k|^2),
+    signed x/y indices (Nyquist -> -N/2), z index as stored."""
+    KX = (2.0 * PI / g.Lx * g.m)[:, None, None]
+    KY = (2.0 * PI / g.Ly * g.n)[None, :, None]
+    KZ = (2.0 * PI / g.Lz * g.q)[None, None, :]
+    filt = 1.0 / (1.0 + eps * eps * (KX * KX + KY * KY + KZ * KZ))
+    return [filt * u for u in U]
+
+
+def cutoff_mask(g: Grid, radius: float) -> np.ndarray:
+    """CutOff_Fourier_Filter_Device (math_support.cu:929-970), launched with Mz
+    in its Nz slot: keep m^2/Nx^2 + n^2/Ny^2 + q^2/Mz^2 <= radius^2."""
+    m = g.m[:, None, None].astype(np.float64)
+    n = g.n[None, :, None].astype(np.float64)
+    q = g.q[None, None, :].astype(np.float64)
+    r2 = (1.0 * m * m / (1.0 * g.Nx * g.Nx) + 1.0 * n * n / (1.0 * g.Ny * g.Ny)
+          + 1.0 * q * q / (1.0 * g.Mz * g.Mz))
+    return (r2 <= radius * radius).astype(np.float64)
+
+
+def cutoff_filter(g: Grid, U, radius: float):
+    mask = cutoff_mask(g, radius)
+    return [mask * u for u in U]
+
+
+def curl_fd(g: Grid, u):
+    """get_curl_device (math_support.cu:680-707) on physical fields: central
+    differences with periodic wrap, including the reference's rot_y term
+    0.5 (uz(j+1) - ux(j-1)) / dx (it mixes uz and ux)."""
+    ux, uy, uz = u
+
+    def sh(a, ax, s):  # a(index + s) with periodic wrap
+        return np.roll(a, -s, axis=ax)
+
+    dx, dy, dz = g.dx, g.dy, g.dz
+    rx = 0.5 * (sh(uz, 1, 1) - sh(uz, 1, -1)) / dy - 0.5 * (sh(uy, 2, 1) - sh(uy, 2, -1)) / dz
+    ry = 0.5 * (sh(ux, 2, 1) - sh(ux, 2, -1)) / dz - 0.5 * (sh(uz, 0, 1) - sh(ux, 0, -1)) / dx
+    rz = 0.5 * (sh(uy, 0, 1) - sh(uy, 0, -1)) / dx - 0.5 * (sh(ux, 1, 1) - sh(ux, 1, -1)) / dy
+    return [rx, ry, rz]
+
+
+def _flat_r(g: Grid, i, j, k) -> int:
+    """IN(i,j,k) of a physical field (Macros.h:11), as a flat index."""
+    return i * (g.Ny * g.Nz) + j * g.Nz + k
+
+
+def _flat_c(g: Grid, i, j, k) -> int:
+    """IN(i,j,k) with Nz = Mz: a spectral field's flat index."""
+    return i * (g.Ny * g.Mz) + j * g.Mz + k
+
+
+def record_points(g: Grid):
+    """Flat indices the time loop reads (NS3D_periodic.cu:1357-1450): three
+    physical probes and eleven spectral ones."""
+    Nx, Ny, Nz, Mz = g.Nx, g.Ny, g.Nz, g.Mz
+    phys = [_flat_r(g, Nx // 2 - 4, Ny // 2 - 3, Nz // 2 - 2),
+            _flat_r(g, Nx // 3, Ny // 3, Nz // 3),
+            _flat_r(g, Nx // 8, Ny // 8, Nz // 8)]
+    spec = [_flat_c(g, Nx - 6, Ny - 6, Mz - 6),
+            _flat_c(g, Nx // 5, Ny // 4 - 3, Mz // 4 - 1),
+            _flat_c(g, Nx // 5, Ny // 5, Mz // 5),
+            _flat_c(g, 2, 2, 2), _flat_c(g, 1, 0, 0), _flat_c(g, 0, 0, 0),
+            _flat_c(g, 1, 1, 0), _flat_c(g, 1, 1, 1), _flat_c(g, Nx - 1, 0, 0),
+            _flat_c(g, Nx - 1, Ny - 1, 0), _flat_c(g, Nx - 1, Ny - 1, Mz - 1)]
+    return phys, spec
+
+
+def series_record(g: Grid, U, total_time: float, Re: float) -> np.ndarray:
+    """The 50 columns the time loop writes to time_dependant.dat per step
+    (NS3D_periodic.cu:1324-1452), computed the reference's way: physical
+    velocity (Image_to_Domain), the cut-off filtered velocity (the Helmholtz
+    filter's output is overwritten by CutOff_Fourier_Filter with radius 0.1),
+    finite-difference curls, get_kinetic_energy / get_dissipation, point
+    reads by flat index, and Re/Im reads of the spectral state."""
+    phys, spec = record_points(g)
+    u = physical_velocity(g, U)
+    r = curl_fd(g, u)
+    uf = physical_velocity(g, cutoff_filter(g, U, 0.1))
+    rf = curl_fd(g, uf)
+    e = kinetic_energy(g, U)
+    d = dissipation(g, U)
+    flat = lambda a, i: float(a.reshape(-1)[i])  # noqa: E731
+    Ur = [x.reshape(-1) for x in U]
+    col = [total_time]
+    for p, tail in zip(phys, (e, d, e - d / Re)):
+        col += [flat(a, p) for a in u] + [flat(a, p) for a in r] + [tail]
+    p = phys[1]
+    col += [flat(a, p) for a in uf] + [flat(a, p) for a in rf] + [e]
+    s = spec[0]
+    col += [Ur[0][s].real, Ur[0][s].imag, Ur[1][s].real, Ur[1][s].imag,
+            Ur[2][s].real, Ur[2][s].imag, d]
+    a, b = spec[1], spec[2]
+    col += [Ur[0][a].imag, Ur[0][b].imag, Ur[1][a].imag, Ur[1][b].imag,
+            Ur[2][a].imag, Ur[2][b].imag, Ur[0][spec[3]].imag]
+    col += [Ur[0][i].imag for i in spec[4:]]
+    return np.array(col, dtype=np.float64)
+
+
+def format_series_line(rec) -> str:
+    """One time_dependant.dat line: 50 '%le' fields, single spaces."""
+    return " ".join("%e" % v for v in rec) + "\n"
+
+
+def energy_spectrum(g: Grid, U) -> np.ndarray:
+    """calculate_energy_spectrum (math_support.cu:819-860): bins n = j+k+l over
+    j < Nx/2, k < Ny/2, l < Mz; E[n] = sum |u_hat|^2 / norm^2 with norm =
+    Nx*Ny*Mz (the function receives Mz as Nz).  Returns the unhalved sums."""
+    Nx, Ny, Mz = g.Nx, g.Ny, g.Mz
+    size = Nx // 2 + Ny // 2 + Mz
+    norm = float(Nx * Ny * Mz)
+    E = np.zeros(size)
+    j = np.arange(Nx // 2)[:, None, None]
+    k = np.arange(Ny // 2)[None, :, None]
+    l = np.arange(Mz)[None, None, :]
+    n = np.broadcast_to(j + k + l, (Nx // 2, Ny // 2, Mz)).reshape(-1)
+    dens = sum((u[: Nx // 2, : Ny // 2, :].real ** 2 / norm / norm
+                + u[: Nx // 2, : Ny // 2, :].imag ** 2 / norm / norm) for u in U).reshape(-1)
+    np.add.at(E, n, dens)
+    return E
+
+
+def format_energy_spectrum(g: Grid, E) -> str:
+    """Ek.dat text: '%i %.16le %.16le' per bin; bins no mode reaches print 0."""
+    size = len(E)
+    nmax = (g.Nx // 2 - 1) + (g.Ny // 2 - 1) + (g.Mz - 1)
+    out = []
+    with np.errstate(divide="ignore"):
+        for n in range(size):
+            if n <= nmax:
+                out.append("%i %.16e %.16e\n" % (n, 0.5 * E[n], 0.5 * (0.5 * math.pow(n, -5.0 / 3.0)
+                                                                       if n else math.inf)))
+            else:
+                out.append("%i %.16e %.16e\n" % (0, 0.0, 0.0))
+    return "".join(out)
+
+
+def shapiro_error(g: Grid, U, t: float, Re: float) -> float:
+    """Shapiro_test_case (Shapiro_test.cu:8-50): max over the grid of
+    |u - u_exact(t)| (Euclidean norm per point) on the physical field."""
+    u = physical_velocity(g, U)
+    ex = shapiro_physical(g, t, Re)
+    err = np.sqrt(sum((a - b) ** 2 for a, b in zip(u, ex)))
+    return float(np.max(err))

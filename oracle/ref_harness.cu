@@ -26,6 +26,7 @@
 #include "diffusion.h"
 #include "math_support.h"
 #include "cuda_supp.h"
+#include "Shapiro_test.h"
 
 namespace {
 
@@ -291,6 +292,157 @@ int ref_diag(double* energy, double* diss) {
   *diss = get_dissipation(S.dimGrid, S.dimBlock, S.Nx, S.Ny, S.Nz, S.dx, S.dy, S.dz, S.phys[0],
                           S.phys[1], S.phys[2], S.red[0], S.red[1], S.red[2]);
   return check("diag");
+}
+
+// One step of the main loop's diagnostic block (Source/NS3D_periodic.cu:1325-1452)
+// on the state itself, in main's order and with main's index arithmetic:
+// Image_to_Domain of the state, the Helmholtz and then the cut-off filter, the
+// curls, get_kinetic_energy / get_dissipation, the point reads, and
+// all_Fourier2double.  rec[0] = total_time, rec[1..49] = columns 2..50 of
+// time_dependant.dat.  preserve = 0: as main, Image_to_Domain transforms the
+// state arrays themselves (cuFFT's out-of-place multi-dimensional
+// complex-to-real transform may overwrite its input, and on B200 with cuFFT
+// 12.9 it does, so the filters and the spectral reads that follow see what
+// the transform left there; ref_get_u shows it).  preserve = 1: Image_to_Domain
+// reads a copy, so everything after it sees the state.
+int ref_diag_record(double total_time, double Re, double* rec, int preserve) {
+  int Nx = S.Nx, Ny = S.Ny, Nz = S.Nz;
+  const int Mz = S.Mz;
+  const double dx = S.dx, dy = S.dy, dz = S.dz;
+  real *ux_d = S.phys[0], *uy_d = S.phys[1], *uz_d = S.phys[2];
+  real *filt[3], *rot[3], *reim[6], *div_pos_d;
+  cudaComplex* fh[3];
+  for (int i = 0; i < 3; ++i) {
+    filt[i] = alloc_r(nr());
+    rot[i] = alloc_r(nr());
+    fh[i] = alloc_c();
+  }
+  for (int i = 0; i < 6; ++i) reim[i] = alloc_r(nc());
+  div_pos_d = alloc_r(nr());
+  if (check("record alloc")) return -1;
+  auto rd = [](const real* p, long long i) {
+    real v = 0.0;
+    cudaMemcpy(&v, p + i, sizeof(real), cudaMemcpyDeviceToHost);
+    return v;
+  };
+  cudaComplex* src[3] = {S.u[0], S.u[1], S.u[2]};
+  if (preserve) {
+    for (int i = 0; i < 3; ++i) {
+      cudaMemcpy(S.u3[i], S.u[i], sizeof(cudaComplex) * nc(), cudaMemcpyDeviceToDevice);
+      src[i] = S.u3[i];
+    }
+  }
+  Image_to_Domain(S.dimGrid, S.dimBlock, Nx, Ny, Nz, ux_d, src[0], uy_d, src[1], uz_d, src[2]);
+  Helmholz_Fourier_Filter(S.dimGrid, S.dimBlock, S.dimGrid_C, S.dimBlock_C, Nx, Ny, Nz, Mz, S.Lx,
+                          S.Ly, S.Lz, S.u[0], S.u[1], S.u[2], fh[0], fh[1], fh[2], 1.0, filt[0],
+                          filt[1], filt[2]);
+  CutOff_Fourier_Filter(S.dimGrid, S.dimBlock, S.dimGrid_C, S.dimBlock_C, Nx, Ny, Nz, Mz, S.Lx,
+                        S.Ly, S.Lz, S.u[0], S.u[1], S.u[2], fh[0], fh[1], fh[2], 0.1, filt[0],
+                        filt[1], filt[2]);
+  get_curl(S.dimGrid, S.dimBlock, Nx, Ny, Nz, dx, dy, dz, ux_d, uy_d, uz_d, rot[0], rot[1], rot[2]);
+  const real energy = get_kinetic_energy(S.dimGrid, S.dimBlock, Nx, Ny, Nz, dx, dy, dz, ux_d, uy_d,
+                                         uz_d, S.red[0], S.red[1], S.red[2]);
+  const real dissipation = get_dissipation(S.dimGrid, S.dimBlock, Nx, Ny, Nz, dx, dy, dz, ux_d,
+                                           uy_d, uz_d, S.red[0], S.red[1], S.red[2]);
+  int c = 0;
+  rec[c++] = total_time;
+  const long long P[3] = {IN(Nx / 2 - 4, Ny / 2 - 3, Nz / 2 - 2), IN(Nx / 3, Ny / 3, Nz / 3),
+                          IN(Nx / 8, Ny / 8, Nz / 8)};
+  const real tail[3] = {energy, dissipation, energy - dissipation / Re};
+  for (int p = 0; p < 3; ++p) {
+    rec[c++] = rd(ux_d, P[p]); rec[c++] = rd(uy_d, P[p]); rec[c++] = rd(uz_d, P[p]);
+    rec[c++] = rd(rot[0], P[p]); rec[c++] = rd(rot[1], P[p]); rec[c++] = rd(rot[2], P[p]);
+    rec[c++] = tail[p];
+  }
+  get_curl(S.dimGrid, S.dimBlock, Nx, Ny, Nz, dx, dy, dz, filt[0], filt[1], filt[2], rot[0], rot[1],
+           rot[2]);
+  rec[c++] = rd(filt[0], P[1]); rec[c++] = rd(filt[1], P[1]); rec[c++] = rd(filt[2], P[1]);
+  rec[c++] = rd(rot[0], P[1]); rec[c++] = rd(rot[1], P[1]); rec[c++] = rd(rot[2], P[1]);
+  rec[c++] = energy;
+  Nz = Mz;  // main switches IN to the spectral layout here
+  all_Fourier2double(S.dimGrid_C, S.dimBlock_C, S.u[0], reim[0], reim[1], S.u[1], reim[2], reim[3],
+                     S.u[2], reim[4], reim[5], Nx, Ny, Mz);
+  const long long F1 = IN(Nx - 6, Ny - 6, Nz - 6);
+  for (int i = 0; i < 6; ++i) rec[c++] = rd(reim[i], F1);
+  rec[c++] = dissipation;
+  const long long F2 = IN(Nx / 5, Ny / 4 - 3, Nz / 4 - 1), F3 = IN(Nx / 5, Ny / 5, Nz / 5);
+  for (int i = 1; i < 6; i += 2) {
+    rec[c++] = rd(reim[i], F2);
+    rec[c++] = rd(reim[i], F3);
+  }
+  rec[c++] = rd(reim[1], IN(2, 2, 2));
+  const long long F[7] = {IN(1, 0, 0),      IN(0, 0, 0),           IN(1, 1, 0),
+                          IN(1, 1, 1),      IN(Nx - 1, 0, 0),      IN(Nx - 1, Ny - 1, 0),
+                          IN(Nx - 1, Ny - 1, Nz - 1)};
+  for (int i = 0; i < 7; ++i) rec[c++] = rd(reim[1], F[i]);
+  for (int i = 0; i < 3; ++i) {
+    cudaFree(filt[i]);
+    cudaFree(rot[i]);
+    cudaFree(fh[i]);
+  }
+  for (int i = 0; i < 6; ++i) cudaFree(reim[i]);
+  cudaFree(div_pos_d);
+  return check("record");
+}
+
+// The two spectral filters on a copy of the state, as main calls them:
+// Helmholz_Fourier_Filter(eps) and CutOff_Fourier_Filter(radius), each
+// followed by its scaled complex-to-real transform; phys_h / phys_c receive
+// the filtered physical velocities (3 host fields each).
+int ref_filters(double eps, double radius, double* phys_h, double* phys_c) {
+  cudaComplex* fh[3];
+  real* filt[3];
+  for (int i = 0; i < 3; ++i) {
+    fh[i] = alloc_c();
+    filt[i] = alloc_r(nr());
+    cudaMemcpy(S.u3[i], S.u[i], sizeof(cudaComplex) * nc(), cudaMemcpyDeviceToDevice);
+  }
+  if (check("filters alloc")) return -1;
+  Helmholz_Fourier_Filter(S.dimGrid, S.dimBlock, S.dimGrid_C, S.dimBlock_C, S.Nx, S.Ny, S.Nz, S.Mz,
+                          S.Lx, S.Ly, S.Lz, S.u3[0], S.u3[1], S.u3[2], fh[0], fh[1], fh[2], eps,
+                          filt[0], filt[1], filt[2]);
+  for (int i = 0; i < 3; ++i)
+    cudaMemcpy(phys_h + nr() * i, filt[i], sizeof(real) * nr(), cudaMemcpyDeviceToHost);
+  CutOff_Fourier_Filter(S.dimGrid, S.dimBlock, S.dimGrid_C, S.dimBlock_C, S.Nx, S.Ny, S.Nz, S.Mz,
+                        S.Lx, S.Ly, S.Lz, S.u3[0], S.u3[1], S.u3[2], fh[0], fh[1], fh[2], radius,
+                        filt[0], filt[1], filt[2]);
+  for (int i = 0; i < 3; ++i)
+    cudaMemcpy(phys_c + nr() * i, filt[i], sizeof(real) * nr(), cudaMemcpyDeviceToHost);
+  for (int i = 0; i < 3; ++i) {
+    cudaFree(fh[i]);
+    cudaFree(filt[i]);
+  }
+  return check("filters");
+}
+
+// get_curl on 3 physical host fields (rot: 3 physical host fields).
+int ref_curl(const double* u, double* rot) {
+  real* r[3];
+  for (int i = 0; i < 3; ++i) {
+    r[i] = alloc_r(nr());
+    cudaMemcpy(S.phys[i], u + nr() * i, sizeof(real) * nr(), cudaMemcpyHostToDevice);
+  }
+  get_curl(S.dimGrid, S.dimBlock, S.Nx, S.Ny, S.Nz, S.dx, S.dy, S.dz, S.phys[0], S.phys[1],
+           S.phys[2], r[0], r[1], r[2]);
+  if (check("curl")) return -1;
+  for (int i = 0; i < 3; ++i) {
+    cudaMemcpy(rot + nr() * i, r[i], sizeof(real) * nr(), cudaMemcpyDeviceToHost);
+    cudaFree(r[i]);
+  }
+  return check("curl copy");
+}
+
+// Shapiro_test_case (Source/Shapiro_test.cu:38-50) on the physical velocity of
+// a copy of the state.
+int ref_shapiro_error(double t, double Re, double* err) {
+  for (int i = 0; i < 3; ++i)
+    cudaMemcpy(S.u3[i], S.u[i], sizeof(cudaComplex) * nc(), cudaMemcpyDeviceToDevice);
+  Image_to_Domain(S.dimGrid, S.dimBlock, S.Nx, S.Ny, S.Nz, S.phys[0], S.u3[0], S.phys[1], S.u3[1],
+                  S.phys[2], S.u3[2]);
+  real ret[2] = {0.0, 0.0};
+  *err = Shapiro_test_case(S.dimGrid, S.dimBlock, S.dx, S.dy, S.dz, t, Re, S.phys[0], S.phys[1],
+                           S.phys[2], S.Nx, S.Ny, S.Nz, S.red[0], S.red[1], ret);
+  return check("shapiro");
 }
 
 // Device-resident timing of nsteps RK3_SSP calls with CUDA events (ms total).

@@ -61,6 +61,10 @@ class RefSolver:
             lib.ref_diag.argtypes = [_dp, _dp]
             lib.ref_time_rk3.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
             lib.ref_time_rk3.restype = ctypes.c_double
+            lib.ref_diag_record.argtypes = [ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int]
+            lib.ref_filters.argtypes = [ctypes.c_double, ctypes.c_double, _dp, _dp]
+            lib.ref_curl.argtypes = [_dp, _dp]
+            lib.ref_shapiro_error.argtypes = [ctypes.c_double, ctypes.c_double, _dp]
             lib.ref_u_ptr.argtypes = [ctypes.c_int]
             lib.ref_u_ptr.restype = ctypes.c_void_p
             RefSolver._libs[path] = lib
@@ -163,6 +167,34 @@ class RefSolver:
         d = np.zeros(1)
         self._check(self.lib.ref_diag(_ptr(e), _ptr(d)), "diag")
         return float(e[0]), float(d[0])
+
+    def record(self, total_time, Re, preserve=True):
+        """The main loop's 50-column record.  preserve=False transforms the
+        state arrays in place as main does (cuFFT may overwrite them; get_u
+        shows what is left); preserve=True transforms a copy."""
+        rec = np.zeros(50)
+        self._check(self.lib.ref_diag_record(total_time, Re, _ptr(rec), int(bool(preserve))),
+                    "record")
+        return rec
+
+    def filters(self, eps, radius):
+        """Physical velocities of the Helmholtz (eps) and cut-off (radius)
+        filtered state."""
+        ph = np.zeros((3, self.Nx, self.Ny, self.Nz))
+        pc = np.zeros((3, self.Nx, self.Ny, self.Nz))
+        self._check(self.lib.ref_filters(eps, radius, _ptr(ph), _ptr(pc)), "filters")
+        return ph, pc
+
+    def curl(self, u):
+        a = np.ascontiguousarray(np.stack([np.asarray(x, dtype=np.float64) for x in u]))
+        r = np.zeros_like(a)
+        self._check(self.lib.ref_curl(_ptr(a), _ptr(r)), "curl")
+        return r
+
+    def shapiro_error(self, t, Re):
+        e = np.zeros(1)
+        self._check(self.lib.ref_shapiro_error(t, Re, _ptr(e)), "shapiro_error")
+        return float(e[0])
 
     def time_rk3(self, nsteps, dt, Re):
         ms = self.lib.ref_time_rk3(nsteps, dt, Re)
