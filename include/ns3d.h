@@ -329,6 +329,41 @@ ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns
                                 double* ms);
 
 /* ----------------------------------------------------------------------- */
+/* ensembles: many independent instances of one grid stepped together       */
+/* ----------------------------------------------------------------------- */
+
+/* No reference counterpart (the reference steps one field per process).  An
+ * ensemble holds `batch` instances of one Nx x Ny x Nz grid and box, each
+ * with its own dt and Re, and advances all of them with the launches of one
+ * RK3 step (15 kernels for the whole batch, replayed from a captured CUDA
+ * graph), so small grids are not bound by launch latency.  Fields are
+ * [batch][Nx][Ny][Nz/2+1] per component: instance b of component c starts at
+ * u_c + b * Nx*Ny*(Nz/2+1).  Each instance's step is RK3_SSP exactly (the same
+ * arithmetic as ns3d_rk3_step, bit for bit).  Several ensembles of different
+ * grids overlap on the GPU when they run on different streams. */
+typedef struct ns3d_ensemble ns3d_ensemble;
+
+ns3d_status ns3d_ensemble_create(int batch, int Nx, int Ny, int Nz, double Lx, double Ly,
+                                 double Lz, ns3d_ensemble** out);
+ns3d_status ns3d_ensemble_destroy(ns3d_ensemble* e);
+ns3d_status ns3d_ensemble_set_stream(ns3d_ensemble* e, void* stream);
+const char* ns3d_ensemble_last_error(const ns3d_ensemble* e);
+size_t ns3d_ensemble_device_bytes(const ns3d_ensemble* e);
+/* One instance-sized forcing, shared by every instance (as ns3d_set_forcing). */
+ns3d_status ns3d_ensemble_set_forcing(ns3d_ensemble* e, const ns3d_complex* fx,
+                                      const ns3d_complex* fy, const ns3d_complex* fz);
+/* Host arrays of `batch` entries; synchronous.  Required before stepping. */
+ns3d_status ns3d_ensemble_set_params(ns3d_ensemble* e, const double* dt, const double* Re);
+/* nsteps RK3 steps of every instance, in place.  Asynchronous. */
+ns3d_status ns3d_ensemble_rk3_steps(ns3d_ensemble* e, ns3d_complex* ux, ns3d_complex* uy,
+                                    ns3d_complex* uz, int nsteps);
+/* ns3d_diagnostics' energy and dissipation per instance (host arrays of
+ * `batch` entries).  Synchronous. */
+ns3d_status ns3d_ensemble_diagnostics(ns3d_ensemble* e, const ns3d_complex* ux,
+                                      const ns3d_complex* uy, const ns3d_complex* uz,
+                                      double* energy, double* dissipation);
+
+/* ----------------------------------------------------------------------- */
 /* allocation-free nonlinear term                                           */
 /* ----------------------------------------------------------------------- */
 

@@ -2,12 +2,13 @@
 time-stepping / Jacobian / Krylov entry points of NS3DPeriodic.
 
 The compute path is the CUDA library libns3d_b200.so (C ABI in
-include/ns3d.h); :class:`Solver` (time stepping) and :class:`Krylov`
-(Arnoldi / implicit restart) are the Python host mirrors over it.
+include/ns3d.h); :class:`Solver` (time stepping), :class:`Ensemble` (many instances of one
+grid stepped together) and :class:`Krylov` (Arnoldi / implicit restart) are
+the Python host mirrors over it.
 """
 from ._lib import Ns3dError, Ns3dLibraryError, LIB_PATH  # noqa: F401
-from .solver import Solver, supported_extent  # noqa: F401
+from .solver import Ensemble, Solver, TimeSeries, supported_extent  # noqa: F401
 from .krylov import Krylov, qr_shifts, select_shifts  # noqa: F401
 
-__all__ = ["Solver", "supported_extent", "Krylov", "qr_shifts", "select_shifts", "Ns3dError",
+__all__ = ["Solver", "Ensemble", "TimeSeries", "supported_extent", "Krylov", "qr_shifts", "select_shifts", "Ns3dError",
            "Ns3dLibraryError", "LIB_PATH"]

@@ -44,6 +44,9 @@ EXPORTS = (
     "ns3d_energy_spectrum", "ns3d_shapiro_state", "ns3d_shapiro_error_physical",
     "ns3d_shapiro_error", "ns3d_series_open", "ns3d_series_write", "ns3d_series_close",
     "ns3d_write_energy_spectrum_host",
+    "ns3d_ensemble_create", "ns3d_ensemble_destroy", "ns3d_ensemble_set_stream",
+    "ns3d_ensemble_last_error", "ns3d_ensemble_device_bytes", "ns3d_ensemble_set_forcing",
+    "ns3d_ensemble_set_params", "ns3d_ensemble_rk3_steps", "ns3d_ensemble_diagnostics",
 )
 
 # the matrix-vector callback type of ns3d_arnoldi: void (*)(void*, void*, void*)
@@ -161,6 +164,16 @@ def _sig(lib):
         "ns3d_series_write": ([_P, _P, c_int], c_int),
         "ns3d_series_close": ([_P], c_int),
         "ns3d_write_energy_spectrum_host": ([ctypes.c_char_p, c_int, c_int, c_int, _P], c_int),
+        "ns3d_ensemble_create": ([c_int, c_int, c_int, c_int, c_double, c_double, c_double,
+                                  ctypes.POINTER(c_void_p)], c_int),
+        "ns3d_ensemble_destroy": ([_P], c_int),
+        "ns3d_ensemble_set_stream": ([_P, _P], c_int),
+        "ns3d_ensemble_last_error": ([_P], ctypes.c_char_p),
+        "ns3d_ensemble_device_bytes": ([_P], ctypes.c_size_t),
+        "ns3d_ensemble_set_forcing": ([_P, _P, _P, _P], c_int),
+        "ns3d_ensemble_set_params": ([_P, _P, _P], c_int),
+        "ns3d_ensemble_rk3_steps": ([_P, _P, _P, _P, c_int], c_int),
+        "ns3d_ensemble_diagnostics": ([_P, _P, _P, _P, _P, _P], c_int),
     }
     for name, (args, res) in S.items():
         f = getattr(lib, name)

@@ -89,7 +89,7 @@ inline unsigned persistent_grid(Kern kern, size_t smem, long long groups) {
 template <int NF>
 cudaError_t launch_inv_x(const InvXArgs<NF>& a, const PassGeom& g, cudaStream_t st,
                          bool prepare_only = false) {
-  const long long lines = (long long)g.Ny * g.Mz;
+  const long long lines = (long long)g.Ny * g.Mz * nbatch(g);
   switch (g.Nx) {
 #define NS3D_CASE(N)                                                                    \
   case N: {                                                                             \
@@ -109,8 +109,9 @@ cudaError_t launch_inv_x(const InvXArgs<NF>& a, const PassGeom& g, cudaStream_t 
 }
 
 template <int NF>
-cudaError_t launch_inv_y(const InvYArgs<NF>& a, const PassGeom& g, cudaStream_t st,
+cudaError_t launch_inv_y(const InvYArgs<NF>& a, const PassGeom& gi, cudaStream_t st,
                          bool prepare_only = false) {
+  const PassGeom g = planes_geom(gi);
   const long long lines = (long long)g.Nx * g.Mz;
   switch (g.Ny) {
 #define NS3D_CASE(N)                                                                    \
@@ -131,7 +132,8 @@ cudaError_t launch_inv_y(const InvYArgs<NF>& a, const PassGeom& g, cudaStream_t 
 }
 
 template <bool UV>
-cudaError_t launch_z(const ZArgs<UV ? 6 : 3>& a, const PassGeom& g, cudaStream_t st) {
+cudaError_t launch_z(const ZArgs<UV ? 6 : 3>& a, const PassGeom& gi, cudaStream_t st) {
+  const PassGeom g = planes_geom(gi);
   const long long lines = (long long)g.Nx * g.Ny;
   switch (g.Nz) {
 #define NS3D_CASE(N)                                                               \
@@ -151,7 +153,7 @@ cudaError_t launch_z(const ZArgs<UV ? 6 : 3>& a, const PassGeom& g, cudaStream_t
 template <int MODE, bool COMBINE>
 cudaError_t launch_fwd_x(const FwdXArgs& a, const PassGeom& g, cudaStream_t st,
                          bool prepare_only = false) {
-  const long long lines = (long long)g.Ny * g.Mz;
+  const long long lines = (long long)g.Ny * g.Mz * nbatch(g);
   switch (g.Nx) {
 #define NS3D_CASE(N)                                                                    \
   case N: {                                                                             \
@@ -170,8 +172,9 @@ cudaError_t launch_fwd_x(const FwdXArgs& a, const PassGeom& g, cudaStream_t st,
   }
 }
 
-inline cudaError_t launch_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream_t st,
+inline cudaError_t launch_fwd_y(const FwdYArgs& a, const PassGeom& gi, cudaStream_t st,
                                 bool prepare_only = false) {
+  const PassGeom g = planes_geom(gi);
   const long long lines = (long long)g.Nx * g.Mz;
   switch (g.Ny) {
 #define NS3D_CASE(N)                                                                    \

@@ -43,7 +43,22 @@ struct PassGeom {
   int Nx, Ny, Nz, Mz;
   double kfx, kfy, kfz;  // 2*pi/L per direction (Source/math_support.cu:350-370)
   double inv_vol;        // 1/(Nx*Ny*Nz), the scale_double factor
+  // Independent instances of one grid stored back to back ([batch][Nx][Ny][Mz]
+  // per field).  The y and z passes see them as one grid of batch*Nx planes;
+  // the x passes split their line index into (instance, y*Mz + z).  0 or 1:
+  // a single instance.
+  int batch;
 };
+__host__ __device__ __forceinline__ int nbatch(const PassGeom& g) {
+  return g.batch > 1 ? g.batch : 1;
+}
+// The geometry the y and z passes use: the instances as extra x planes.
+__host__ __device__ __forceinline__ PassGeom planes_geom(const PassGeom& g) {
+  PassGeom p = g;
+  p.Nx = g.Nx * nbatch(g);
+  p.batch = 1;
+  return p;
+}
 
 // signed wavenumber index: j < N/2 -> j, else j - N (x and y; the Nyquist
 // index N/2 is stored as -N/2, Source/math_support.cu:354-357)
@@ -191,8 +206,14 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF
   LM::get(li, t);
   double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
   double2* pf = dsm + S::PF + threadIdx.x;
-  const int nlines = g.Ny * g.Mz;
-  const int groups = (nlines + LM::LPC - 1) / LM::LPC;
+  const int nlines = g.Ny * g.Mz;               // lines of one instance
+  const int tlines = nlines * nbatch(g);        // lines of all instances
+  const int groups = (tlines + LM::LPC - 1) / LM::LPC;
+  // line G of the batch: instance G / nlines, line G % nlines of it
+  auto line_off = [&](int G) -> size_t {
+    const int b = G / nlines;
+    return (size_t)b * NX * nlines + (size_t)(G - b * nlines);
+  };
   // each CTA takes a contiguous range of groups, so neighbouring lines (which
   // share partially covered 32-byte sectors) are handled back to back
   const GroupRange gr = group_range(groups);
@@ -201,23 +222,26 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF
   if (grp >= g_end) return;  // uniform across the CTA
   uint32_t keep;             // bit s: mode (t + T s, y, z) survives the 2/3 mask
   {
-    const int L = grp * LM::LPC + li;
-    const bool valid = L < nlines;
-    const int Lc = valid ? L : 0;
+    const int G = grp * LM::LPC + li;
+    const bool valid = G < tlines;
+    const int Gc = valid ? G : 0;
+    const int Lc = Gc % nlines;
     const int y = Lc / g.Mz, z = Lc - y * g.Mz;
     keep = mask_bits<NX>(a.qcut, g.Ny, y, z, Lc, valid, t, T, P);
-    issue_line<P, T>(pf, a.in[0], (size_t)Lc, (size_t)nlines, t, keep);
+    issue_line<P, T>(pf, a.in[0], line_off(Gc), (size_t)nlines, t, keep);
     cp_async_commit();
   }
   int ub = 0;
   for (; grp < g_end; grp += gr.step) {
-    const int L = grp * LM::LPC + li;
-    const bool valid = L < nlines;
-    const int Lc = valid ? L : 0;
+    const int G = grp * LM::LPC + li;
+    const bool valid = G < tlines;
+    const int Gc = valid ? G : 0;
+    const size_t off = line_off(Gc);
     const int gn = grp + gr.step;
-    const int Ln = gn * LM::LPC + li;
-    const bool validn = Ln < nlines;
-    const int Lnc = validn ? Ln : 0;
+    const int Gn = gn * LM::LPC + li;
+    const bool validn = Gn < tlines;
+    const int Gnc = validn ? Gn : 0;
+    const int Lnc = Gnc % nlines;
     uint32_t keep_next = 0;
     if (gn < g_end) {
       const int yn = Lnc / g.Mz, zn = Lnc - yn * g.Mz;
@@ -228,9 +252,9 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF
       const double2* cur = pf + ub * (P * kThreads);
       double2* nxt = pf + (ub ^ 1) * (P * kThreads);
       if (f + 1 < NF) {
-        issue_line<P, T>(nxt, a.in[f + 1], (size_t)Lc, (size_t)nlines, t, keep);
+        issue_line<P, T>(nxt, a.in[f + 1], off, (size_t)nlines, t, keep);
       } else if (gn < g_end) {
-        issue_line<P, T>(nxt, a.in[0], (size_t)Lnc, (size_t)nlines, t, keep_next);
+        issue_line<P, T>(nxt, a.in[0], line_off(Gnc), (size_t)nlines, t, keep_next);
       }
       cp_async_commit();
       cp_async_wait<1>();
@@ -241,7 +265,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF
       F::template run<+1>(v, t, sbuf, tw_s);
       if (valid) {
 #pragma unroll
-        for (int s = 0; s < P; ++s) a.A[f][(size_t)(t + T * s) * nlines + L] = v[s];
+        for (int s = 0; s < P; ++s) a.A[f][off + (size_t)(t + T * s) * nlines] = v[s];
       }
 #pragma unroll
       for (int s = 0; s < P; ++s) {
@@ -252,7 +276,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF
       F::template run<+1>(v, t, sbuf, tw_s);
       if (valid) {
 #pragma unroll
-        for (int s = 0; s < P; ++s) a.B[f][(size_t)(t + T * s) * nlines + L] = v[s];
+        for (int s = 0; s < P; ++s) a.B[f][off + (size_t)(t + T * s) * nlines] = v[s];
       }
       ub ^= 1;
     }
@@ -828,6 +852,7 @@ struct FwdXArgs {
   const double2* fval;      // sparse forcing values, 3 per entry
   int fnnz;
   double dt, Re, ca, cb;    // out = ca * un + cb * base  (COMBINE), else out = base
+  const double* dtRe;       // per instance (dt, Re) of a batch, replacing dt and Re; or null
   const double2* tw;
 };
 
@@ -835,13 +860,13 @@ struct FwdXArgs {
 // prefetch slots), then the pointwise update of Source/diffusion.cu.
 template <int NX, int P, int MODE, bool COMBINE>
 __device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g, int t, int L,
-                                           int Lc, bool valid, double2* sbuf,
+                                           size_t off, int inst, bool valid, double2* sbuf,
                                            const double2* tw_s, double2* pf, int& ub,
-                                           bool more, size_t Lnc) {
+                                           bool more, size_t offn) {
   constexpr int T = NX / P;
   using F = LineFFT<NX, P>;
   const int nlines = g.Ny * g.Mz;
-  const int y = Lc / g.Mz, z = Lc - y * g.Mz;
+  const int y = L / g.Mz, z = L - y * g.Mz;
   // Re(Qh) is set to zero (set_to_zero_real), so only the imaginary part of
   // each transformed component is kept
   double qi[3][P];
@@ -850,9 +875,9 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g,
     const double2* cur = pf + ub * (P * kThreads);
     double2* nxt = pf + (ub ^ 1) * (P * kThreads);
     if (c + 1 < 3) {
-      issue_line<P, T>(nxt, a.Qh[c + 1], (size_t)Lc, (size_t)nlines, t);
+      issue_line<P, T>(nxt, a.Qh[c + 1], off, (size_t)nlines, t);
     } else if (more) {
-      issue_line<P, T>(nxt, a.Qh[0], Lnc, (size_t)nlines, t);
+      issue_line<P, T>(nxt, a.Qh[0], offn, (size_t)nlines, t);
     }
     cp_async_commit();
     cp_async_wait<1>();
@@ -869,7 +894,7 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g,
 #pragma unroll
     for (int s = 0; s < P; ++s) {
       const int x = t + T * s;
-      const size_t idx = (size_t)x * nlines + L;
+      const size_t idx = off + (size_t)x * nlines;
       const bool origin = (x == 0) && (L == 0);
 #pragma unroll
       for (int c = 0; c < 3; ++c) a.out[c][idx] = make_double2(0.0, origin ? 0.0 : qi[c][s]);
@@ -879,10 +904,13 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g,
   const double ky = g.kfy * (double)signed_idx(y, g.Ny);
   const double kz = g.kfz * (double)z;
   const bool dense_f = a.fd[0] != nullptr;
+  const double dt = a.dtRe ? __ldg(a.dtRe + 2 * inst) : a.dt;
+  const double Re = a.dtRe ? __ldg(a.dtRe + 2 * inst + 1) : a.Re;
 #pragma unroll
   for (int s = 0; s < P; ++s) {
     const int x = t + T * s;
-    const size_t idx = (size_t)x * nlines + L;
+    const size_t fi = (size_t)x * nlines + L;  // index inside the instance (forcing)
+    const size_t idx = off + (size_t)x * nlines;
     const double kx = g.kfx * (double)signed_idx(x, NX);
     const double kk = kx * kx + ky * ky + kz * kz;
     // set_to_zero_real: Re(Qh) = 0 everywhere, Qh(0,0,0) = 0
@@ -897,10 +925,10 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g,
     if constexpr (MODE != kImplicit) {
       if (dense_f) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) f[c] = __ldg(a.fd[c] + idx);
+        for (int c = 0; c < 3; ++c) f[c] = __ldg(a.fd[c] + fi);
       } else {
         for (int e = 0; e < a.fnnz; ++e) {
-          if (__ldg(a.fidx + e) == (int)idx) {
+          if (__ldg(a.fidx + e) == (int)fi) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) f[c] = cadd(f[c], __ldg(a.fval + 3 * e + c));
           }
@@ -912,14 +940,14 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g,
       const double2 u = __ldg(a.us[c] + idx);
       double2 r;
       if constexpr (MODE == kExplicit) {
-        const double G = 1.0 - kk * a.dt / a.Re;
-        r = make_double2(G * u.x + a.dt * f[c].x, a.dt * p[c] + G * u.y + a.dt * f[c].y);
+        const double G = 1.0 - kk * dt / Re;
+        r = make_double2(G * u.x + dt * f[c].x, dt * p[c] + G * u.y + dt * f[c].y);
       } else if constexpr (MODE == kRhs) {
-        const double G = -kk / a.Re;
+        const double G = -kk / Re;
         r = make_double2(G * u.x + f[c].x, p[c] + G * u.y + f[c].y);
       } else {
-        const double G = 1.0 + kk * a.dt / a.Re;
-        r = make_double2(u.x / G, (a.dt * p[c] + u.y) / G);
+        const double G = 1.0 + kk * dt / Re;
+        r = make_double2(u.x / G, (dt * p[c] + u.y) / G);
       }
       if constexpr (COMBINE) {
         const double2 n = __ldg(a.un[c] + idx);
@@ -944,25 +972,32 @@ __global__ void __launch_bounds__(kThreads, kMinCtasFwdX) fwd_x_kernel(FwdXArgs 
   double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
   double2* pf = dsm + S::PF + threadIdx.x;
   const int nlines = g.Ny * g.Mz;
-  const int groups = (nlines + LM::LPC - 1) / LM::LPC;
+  const int tlines = nlines * nbatch(g);
+  const int groups = (tlines + LM::LPC - 1) / LM::LPC;
+  auto line_off = [&](int G) -> size_t {
+    const int b = G / nlines;
+    return (size_t)b * NX * nlines + (size_t)(G - b * nlines);
+  };
   const GroupRange gr = group_range(groups);
   const int g_end = gr.end;
   int grp = gr.grp;
   if (grp >= g_end) return;
   {
-    const int L0 = grp * LM::LPC + li;
-    issue_line<P, T>(pf, a.Qh[0], (size_t)(L0 < nlines ? L0 : 0), (size_t)nlines, t);
+    const int G0 = grp * LM::LPC + li;
+    issue_line<P, T>(pf, a.Qh[0], line_off(G0 < tlines ? G0 : 0), (size_t)nlines, t);
     cp_async_commit();
   }
   int ub = 0;
   for (; grp < g_end; grp += gr.step) {
-    const int L = grp * LM::LPC + li;
-    const bool valid = L < nlines;
-    const int Lc = valid ? L : 0;
+    const int G = grp * LM::LPC + li;
+    const bool valid = G < tlines;
+    const int Gc = valid ? G : 0;
+    const int inst = Gc / nlines;
     const int gn = grp + gr.step;
-    const int Ln = gn * LM::LPC + li;
-    const size_t Lnc = (size_t)(Ln < nlines ? Ln : 0);
-    fwd_x_line<NX, P, MODE, COMBINE>(a, g, t, L, Lc, valid, sbuf, tw_s, pf, ub, gn < g_end, Lnc);
+    const int Gn = gn * LM::LPC + li;
+    fwd_x_line<NX, P, MODE, COMBINE>(a, g, t, Gc - inst * nlines, line_off(Gc), inst, valid,
+                                     sbuf, tw_s, pf, ub, gn < g_end,
+                                     line_off(Gn < tlines ? Gn : 0));
   }
   cp_async_wait<0>();
 }

@@ -31,7 +31,11 @@ constexpr int kDiagThreads = 256;
 struct ns3d_solver {
   int Nx = 0, Ny = 0, Nz = 0, Mz = 0;
   double Lx = 0, Ly = 0, Lz = 0;
-  size_t nc = 0;  // complex points per field
+  size_t nc = 0;  // complex points per field (one instance)
+  int batch = 1;  // instances stepped together (ns3d_ensemble); scratch is batch x nc
+  double* dtRe = nullptr;  // per instance (dt, Re) of a batch, device
+  double ens_dt = 0.0, ens_Re = 0.0;  // the same for an ensemble of one
+  bool ens_params = false;            // ns3d_ensemble_set_params was called
   int device = 0;
   PassGeom geom{};
   cudaStream_t stream = nullptr;
@@ -238,6 +242,7 @@ ns3d_status finish(ns3d_solver* h, int mode, bool forcing, const double2* const 
   a.fnnz = (forcing && !h->f_dense[0]) ? h->f_nnz : 0;
   a.dt = dt;
   a.Re = Re;
+  a.dtRe = h->batch > 1 ? h->dtRe : nullptr;
   a.ca = ca;
   a.cb = cb;
   a.tw = h->tw[0];
@@ -328,19 +333,26 @@ ns3d_status ns3d_twiddles(int N, double* tw) {
   return NS3D_OK;
 }
 
-ns3d_status ns3d_create(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
-                        ns3d_solver** out) {
+namespace {
+ns3d_status create_solver(int batch, int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                          ns3d_solver** out) {
   if (!out) return NS3D_ERR_BAD_ARG;
   *out = nullptr;
-  if (Nx <= 0 || Ny <= 0 || Nz <= 0 || !(Lx > 0) || !(Ly > 0) || !(Lz > 0))
+  if (Nx <= 0 || Ny <= 0 || Nz <= 0 || !(Lx > 0) || !(Ly > 0) || !(Lz > 0) || batch < 1)
     return NS3D_ERR_BAD_ARG;
   if (!valid_extents(Nx, Ny, Nz)) return NS3D_ERR_UNSUPPORTED;
+  // the x passes index lines of the whole batch with 32-bit integers
+  if ((long long)batch * Ny * (Nz / 2 + 1) >= (1LL << 31) ||
+      (long long)batch * Nx * Ny >= (1LL << 31))
+    return NS3D_ERR_BAD_ARG;
   ns3d_solver* h = new ns3d_solver();
   h->Nx = Nx; h->Ny = Ny; h->Nz = Nz; h->Mz = Nz / 2 + 1;
   h->Lx = Lx; h->Ly = Ly; h->Lz = Lz;
   h->nc = (size_t)Nx * Ny * h->Mz;
+  h->batch = batch;
   cudaGetDevice(&h->device);
   h->geom.Nx = Nx; h->geom.Ny = Ny; h->geom.Nz = Nz; h->geom.Mz = h->Mz;
+  h->geom.batch = batch;
   // 2.0*M_PI/L as in build_Nabla_Wavenumbers (Source/math_support.cu:398-413)
   h->geom.kfx = 2.0 * M_PI / Lx;
   h->geom.kfy = 2.0 * M_PI / Ly;
@@ -366,31 +378,43 @@ ns3d_status ns3d_create(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
     if (cudaMalloc(&h->tw[d], sizeof(double2) * t.size()) != cudaSuccess) return bail(NS3D_ERR_OOM);
     cudaMemcpy(h->tw[d], t.data(), sizeof(double2) * t.size(), cudaMemcpyHostToDevice);
   }
-  const size_t base_bytes = sizeof(double2) * h->nc * 21;
+  const size_t field = h->nc * (size_t)batch;  // one scratch field of the whole batch
+  const size_t base_bytes = sizeof(double2) * field * 21;
   if (cudaMalloc(&h->pool_base, base_bytes) != cudaSuccess) return bail(NS3D_ERR_OOM);
   h->bytes = base_bytes + sizeof(uint16_t) * qc.size() + sizeof(double2) * (Nx + Ny + Nz);
   double2* p = h->pool_base;
   for (int i = 0; i < 3; ++i) {
-    h->A[i] = p; p += h->nc;
-    h->B[i] = p; p += h->nc;
-    h->C[i] = p; p += h->nc;
-    h->D[i] = p; p += h->nc;
-    h->E[i] = p; p += h->nc;
-    h->u1[i] = p; p += h->nc;
-    h->u2[i] = p; p += h->nc;
+    h->A[i] = p; p += field;
+    h->B[i] = p; p += field;
+    h->C[i] = p; p += field;
+    h->D[i] = p; p += field;
+    h->E[i] = p; p += field;
+    h->u1[i] = p; p += field;
+    h->u2[i] = p; p += field;
   }
   if (cudaMalloc(&h->f_count, sizeof(int)) != cudaSuccess ||
       cudaMalloc(&h->f_idx, sizeof(int) * kForcingCap) != cudaSuccess ||
       cudaMalloc(&h->f_val, sizeof(double2) * 3 * kForcingCap) != cudaSuccess ||
       cudaMalloc(&h->diag_partial, sizeof(double) * 3 * kDiagBlocks) != cudaSuccess ||
-      cudaMalloc(&h->diag_out, sizeof(double) * 3) != cudaSuccess)
+      cudaMalloc(&h->diag_out, sizeof(double) * 3 * batch) != cudaSuccess)
     return bail(NS3D_ERR_OOM);
+  if (batch > 1) {
+    if (cudaMalloc(&h->dtRe, sizeof(double) * 2 * batch) != cudaSuccess) return bail(NS3D_ERR_OOM);
+    std::vector<double> ones(2 * batch, 1.0);
+    cudaMemcpy(h->dtRe, ones.data(), sizeof(double) * 2 * batch, cudaMemcpyHostToDevice);
+  }
   if ((e = ns3d::prepare_xy(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   if ((e = ns3d::prepare_fwdx(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   if ((e = ns3d::prepare_fft3d(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   *out = h;
   return NS3D_OK;
+}
+}  // namespace
+
+ns3d_status ns3d_create(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                        ns3d_solver** out) {
+  return create_solver(1, Nx, Ny, Nz, Lx, Ly, Lz, out);
 }
 
 ns3d_status ns3d_destroy(ns3d_solver* h) {
@@ -407,6 +431,7 @@ ns3d_status ns3d_destroy(ns3d_solver* h) {
   cudaFree(h->f_val);
   cudaFree(h->diag_partial);
   cudaFree(h->diag_out);
+  cudaFree(h->dtRe);
   cudaFree(h->rec_tab);
   cudaFree(h->rec_partial);
   cudaFree(h->rec_out);
@@ -471,11 +496,11 @@ ns3d_status ns3d_rk3_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns
   return ns3d_rk3_steps(h, ux, uy, uz, dt, Re, 1);
 }
 
-ns3d_status ns3d_rk3_steps(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+namespace {
+// nsteps RK3 steps, through a captured graph where the stream allows it.  A
+// batch reads its per-instance dt and Re from h->dtRe (dt, Re here are 0).
+ns3d_status rk3_steps_impl(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
                            double dt, double Re, int nsteps) {
-  NS3D_TRY(check_handle(h));
-  NS3D_TRY(check_step(h, dt, Re));
-  if (!args_ok3(ux, uy, uz) || nsteps < 0) return fail(h, NS3D_ERR_BAD_ARG, "null field");
   double2* u[3] = {(double2*)ux, (double2*)uy, (double2*)uz};
   if (nsteps == 0) return NS3D_OK;
   // The legacy default stream cannot be captured: launch directly there.
@@ -518,6 +543,15 @@ ns3d_status ns3d_rk3_steps(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, n
   for (int s = 0; s < nsteps; ++s)
     NS3D_CHECK(h, cudaGraphLaunch(h->rk3_exec, h->stream), "graph launch");
   return NS3D_OK;
+}
+}  // namespace
+
+ns3d_status ns3d_rk3_steps(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                           double dt, double Re, int nsteps) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, dt, Re));
+  if (!args_ok3(ux, uy, uz) || nsteps < 0) return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  return rk3_steps_impl(h, ux, uy, uz, dt, Re, nsteps);
 }
 
 ns3d_status ns3d_euler_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
@@ -1157,3 +1191,118 @@ ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ensembles: `batch` independent instances of one grid stepped together
+// ---------------------------------------------------------------------------
+struct ns3d_ensemble {
+  ns3d_solver* h = nullptr;
+};
+
+ns3d_status ns3d_ensemble_create(int batch, int Nx, int Ny, int Nz, double Lx, double Ly,
+                                 double Lz, ns3d_ensemble** out) {
+  if (!out) return NS3D_ERR_BAD_ARG;
+  *out = nullptr;
+  ns3d_solver* h = nullptr;
+  const ns3d_status s = create_solver(batch, Nx, Ny, Nz, Lx, Ly, Lz, &h);
+  if (s != NS3D_OK) return s;
+  *out = new ns3d_ensemble{h};
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_ensemble_destroy(ns3d_ensemble* e) {
+  if (!e) return NS3D_ERR_BAD_ARG;
+  const ns3d_status s = ns3d_destroy(e->h);
+  delete e;
+  return s;
+}
+
+ns3d_status ns3d_ensemble_set_stream(ns3d_ensemble* e, void* stream) {
+  return e ? ns3d_set_stream(e->h, stream) : NS3D_ERR_BAD_ARG;
+}
+
+const char* ns3d_ensemble_last_error(const ns3d_ensemble* e) {
+  return e ? ns3d_last_error(e->h) : "null ensemble";
+}
+
+size_t ns3d_ensemble_device_bytes(const ns3d_ensemble* e) {
+  return e ? ns3d_device_bytes(e->h) : 0;
+}
+
+ns3d_status ns3d_ensemble_set_forcing(ns3d_ensemble* e, const ns3d_complex* fx,
+                                      const ns3d_complex* fy, const ns3d_complex* fz) {
+  return e ? ns3d_set_forcing(e->h, fx, fy, fz) : NS3D_ERR_BAD_ARG;
+}
+
+ns3d_status ns3d_ensemble_set_params(ns3d_ensemble* e, const double* dt, const double* Re) {
+  if (!e) return NS3D_ERR_BAD_ARG;
+  ns3d_solver* h = e->h;
+  if (!dt || !Re) return fail(h, NS3D_ERR_BAD_ARG, "null parameter array");
+  std::vector<double> p(2 * (size_t)h->batch);
+  for (int b = 0; b < h->batch; ++b) {
+    if (!(dt[b] > 0.0) || !std::isfinite(dt[b]) || !(Re[b] > 0.0) || !std::isfinite(Re[b]))
+      return fail(h, NS3D_ERR_BAD_ARG, "dt and Re must be finite and > 0");
+    p[2 * b] = dt[b];
+    p[2 * b + 1] = Re[b];
+  }
+  if (h->batch == 1) {  // a single instance keeps them on the host
+    h->ens_dt = dt[0];
+    h->ens_Re = Re[0];
+    h->ens_params = true;
+    return NS3D_OK;
+  }
+  NS3D_CHECK(h, cudaMemcpyAsync(h->dtRe, p.data(), sizeof(double) * p.size(),
+                                cudaMemcpyHostToDevice, h->stream), "parameter copy");
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "parameter sync");
+  h->ens_params = true;
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_ensemble_rk3_steps(ns3d_ensemble* e, ns3d_complex* ux, ns3d_complex* uy,
+                                    ns3d_complex* uz, int nsteps) {
+  if (!e) return NS3D_ERR_BAD_ARG;
+  ns3d_solver* h = e->h;
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(ux, uy, uz) || nsteps < 0) return fail(h, NS3D_ERR_BAD_ARG, "null field");
+  if (!h->ens_params) return fail(h, NS3D_ERR_BAD_ARG, "ns3d_ensemble_set_params first");
+  if (h->batch == 1) return rk3_steps_impl(h, ux, uy, uz, h->ens_dt, h->ens_Re, nsteps);
+  return rk3_steps_impl(h, ux, uy, uz, 0.0, 0.0, nsteps);
+}
+
+ns3d_status ns3d_ensemble_diagnostics(ns3d_ensemble* e, const ns3d_complex* ux,
+                                      const ns3d_complex* uy, const ns3d_complex* uz,
+                                      double* energy, double* dissipation) {
+  if (!e) return NS3D_ERR_BAD_ARG;
+  ns3d_solver* h = e->h;
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(ux, uy, uz) || !energy || !dissipation)
+    return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  ns3d::DiagGeom g{};
+  g.Nx = h->Nx; g.Ny = h->Ny; g.Nz = h->Nz; g.Mz = h->Mz;
+  g.kfx = h->geom.kfx; g.kfy = h->geom.kfy; g.kfz = h->geom.kfz;
+  g.dx = h->Lx / (double)h->Nx;
+  g.dy = h->Ly / (double)h->Ny;
+  g.dz = h->Lz / (double)h->Nz;
+  g.inv_vol = h->geom.inv_vol;
+  for (int b = 0; b < h->batch; ++b) {
+    const size_t o = (size_t)b * h->nc;
+    ns3d::diag_partial_kernel<<<kDiagBlocks, kDiagThreads, 0, h->stream>>>(
+        (const double2*)ux + o, (const double2*)uy + o, (const double2*)uz + o, g,
+        h->diag_partial);
+    NS3D_CHECK(h, cudaGetLastError(), "diag_partial");
+    ns3d::diag_final_kernel<<<1, 1024, 0, h->stream>>>(h->diag_partial, kDiagBlocks,
+                                                       h->diag_out + 3 * b);
+    NS3D_CHECK(h, cudaGetLastError(), "diag_final");
+  }
+  std::vector<double> r(3 * (size_t)h->batch);
+  NS3D_CHECK(h, cudaMemcpyAsync(r.data(), h->diag_out, sizeof(double) * r.size(),
+                                cudaMemcpyDeviceToHost, h->stream), "diag copy");
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "diag sync");
+  bool finite = true;
+  for (int b = 0; b < h->batch; ++b) {
+    energy[b] = r[3 * b];
+    dissipation[b] = r[3 * b + 1];
+    finite = finite && std::isfinite(r[3 * b]) && std::isfinite(r[3 * b + 1]);
+  }
+  return finite ? NS3D_OK : fail(h, NS3D_ERR_NONFINITE, "diagnostics are not finite");
+}

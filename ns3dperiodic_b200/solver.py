@@ -494,3 +494,122 @@ def write_energy_spectrum(path: str, Nx: int, Ny: int, Nz: int, E):
     rc = lib().ns3d_write_energy_spectrum_host(str(path).encode(), Nx, Ny, Nz, e.ctypes.data)
     if rc != 0:
         raise Ns3dError(rc, "ns3d_write_energy_spectrum_host", str(path))
+
+
+class Ensemble:
+    """ns3d_ensemble: `batch` independent instances of one grid, each with its
+    own dt and Re, advanced together by the launches of one RK3 step.  Fields
+    are complex128 tensors of shape (batch, Nx, Ny, Nz//2+1) per component."""
+
+    def __init__(self, batch: int, Nx: int, Ny: int, Nz: int, Lx: float = _PI2,
+                 Ly: float = _PI2, Lz: float = _PI2, device=None):
+        import torch
+
+        self._torch = torch
+        dev = torch.device(device if device is not None else "cuda")
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        self.batch = int(batch)
+        self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)
+        self.Mz = self.Nz // 2 + 1
+        self._L = lib()
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            torch.cuda.init()
+            rc = self._L.ns3d_ensemble_create(self.batch, self.Nx, self.Ny, self.Nz, float(Lx),
+                                              float(Ly), float(Lz), ctypes.byref(h))
+        if rc != 0:
+            raise Ns3dError(rc, "ns3d_ensemble_create")
+        self._h = h
+        self._forcing = None
+
+    @property
+    def shape(self):
+        return (self.batch, self.Nx, self.Ny, self.Mz)
+
+    def _check(self, rc: int, where: str):
+        if rc != 0:
+            detail = self._L.ns3d_ensemble_last_error(self._h)
+            raise Ns3dError(rc, where, detail.decode() if detail else "")
+
+    def _fields(self, F, shape, name):
+        t = self._torch
+        if len(F) != 3:
+            raise ValueError(f"{name}: need 3 components")
+        for f in F:
+            if (not isinstance(f, t.Tensor) or f.dtype != t.complex128 or f.device != self.device
+                    or tuple(f.shape) != shape or not f.is_contiguous()):
+                raise ValueError(f"{name}: expected contiguous complex128 {shape} tensors")
+        return [_ptr(f) for f in F]
+
+    def zeros(self):
+        t = self._torch
+        return [t.zeros(self.shape, dtype=t.complex128, device=self.device) for _ in range(3)]
+
+    def to_device(self, F):
+        t = self._torch
+        return [t.as_tensor(f).to(device=self.device, dtype=t.complex128).contiguous() for f in F]
+
+    def set_stream(self, stream):
+        raw = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        self._check(self._L.ns3d_ensemble_set_stream(self._h, ctypes.c_void_p(raw)),
+                    "ns3d_ensemble_set_stream")
+
+    def set_forcing(self, F):
+        """One instance-sized forcing (Nx, Ny, Nz//2+1) shared by all instances."""
+        if F is None:
+            self._check(self._L.ns3d_ensemble_set_forcing(self._h, None, None, None),
+                        "ns3d_ensemble_set_forcing")
+            return
+        Fd = self.to_device(F)
+        p = self._fields(Fd, (self.Nx, self.Ny, self.Mz), "F")
+        self._check(self._L.ns3d_ensemble_set_forcing(self._h, *p), "ns3d_ensemble_set_forcing")
+        self._forcing = Fd
+
+    def set_params(self, dt, Re):
+        import numpy as np
+
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float64), (self.batch,)))
+        r = np.ascontiguousarray(np.broadcast_to(np.asarray(Re, np.float64), (self.batch,)))
+        self._check(self._L.ns3d_ensemble_set_params(self._h, d.ctypes.data, r.ctypes.data),
+                    "ns3d_ensemble_set_params")
+
+    def rk3_steps(self, U, nsteps: int = 1):
+        self._check(self._L.ns3d_ensemble_rk3_steps(self._h, *self._fields(U, self.shape, "U"),
+                                                    int(nsteps)), "ns3d_ensemble_rk3_steps")
+        return U
+
+    def diagnostics(self, U):
+        """(energy, dissipation) per instance; an instance whose values are
+        not finite has diverged (the call still returns)."""
+        import numpy as np
+
+        e = np.zeros(self.batch)
+        d = np.zeros(self.batch)
+        rc = self._L.ns3d_ensemble_diagnostics(self._h, *self._fields(U, self.shape, "U"),
+                                               e.ctypes.data, d.ctypes.data)
+        if rc != 5:  # non-finite: the arrays are filled, NaN/Inf marks diverged instances
+            self._check(rc, "ns3d_ensemble_diagnostics")
+        return e, d
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._L.ns3d_ensemble_device_bytes(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._L.ns3d_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
