@@ -54,10 +54,14 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
-    ap.add_argument("--workload", choices=["rk3", "arnoldi", "ensemble"], default="rk3",
+    ap.add_argument("--workload", choices=["rk3", "arnoldi", "ensemble", "serving"],
+                    default="rk3",
                     help="rk3: the RK3 step (default); arnoldi: the Krylov factorisation; "
                          "ensemble: mixed-N Kolmogorov instances stepped as batches")
     ap.add_argument("--instances", type=int, default=64, help="ensemble size")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: mean arrivals per s")
+    ap.add_argument("--window", type=float, default=45.0, help="serving: seconds of arrivals")
+    ap.add_argument("--slots", default="16,8,4", help="serving: slots for N = 64,96,128")
     ap.add_argument("--n-arnoldi", type=int, default=2300000)
     ap.add_argument("--m-arnoldi", type=int, default=30)
     return ap.parse_args()
@@ -779,7 +783,8 @@ def run_ours_ensemble(args, world, rank, local, pg):
                    "diverged_note": "under-resolved high-Re instances overflow within the "
                                     "200 steps; the reference's RK3_SSP does the same "
                                     "arithmetic (the timing covers them all)",
-                   "energy_first": {str(N): float(e[0]) for N, e in energies.items()}},
+                   "energy_first": {str(N): (float(e[0]) if math.isfinite(e[0]) else None)
+                                    for N, e in energies.items()}},
         "roofline": {"bound": "hbm", "kernel": "all passes (P3L bytes of every instance)",
                      "achieved": round(B / (ms / 1e3) / 1e9, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(B / (ms / 1e3) / 1e9 / peak, 4), "traffic": None,
@@ -838,11 +843,159 @@ def run_reference_ensemble(args, world, rank, local, pg):
             "clocks": clocks}
 
 
+# ---------------------------------------------------------------------------
+# serving: Poisson arrivals of tangent-integration (JVP) requests
+# ---------------------------------------------------------------------------
+SERVE_NS = (64, 96, 128)
+
+
+def serving_requests(rate, window, seed=0):
+    """(N, Re, T, seed, arrival): N in {64,96,128}, Re in {100,200,400},
+    T ~ U[1, 5], Poisson arrivals of mean `rate` per second over `window` s."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out, t, i = [], 0.0, 0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t > window:
+            return out
+        out.append((int(rng.choice(SERVE_NS)), float(rng.choice((100.0, 200.0, 400.0))),
+                    float(rng.uniform(1.0, 5.0)), i, t))
+        i += 1
+
+
+def latency_stats(res):
+    import numpy as np
+
+    done = [r for r in res if r["done"] >= 0.0]
+    if not done:
+        return {"completed": 0}
+    lat = np.array([r["done"] - r["arrival"] for r in done])
+    wait = np.array([r["admitted"] - r["arrival"] for r in done])
+    return {"completed": len(done),
+            "p50_s": round(float(np.percentile(lat, 50)), 4),
+            "p99_s": round(float(np.percentile(lat, 99)), 4),
+            "mean_wait_s": round(float(wait.mean()), 4),
+            "per_N": {str(N): sum(1 for r in done if r["N"] == N) for N in SERVE_NS}}
+
+
+def jvp_bytes(N):
+    _, Sc, Sr = sizes(N)
+    return 330 * Sc + 30 * Sr
+
+
+def run_ours_serving(args, world, rank, local, pg):
+    import torch
+
+    from ns3dperiodic_b200 import Server, Solver, request_steps
+    from ns3dperiodic_b200 import workload as W
+
+    slots = [int(x) for x in args.slots.split(",")]
+    reqs = serving_requests(args.rate, args.window, seed=rank)
+    peak, peak_src = peaks()
+
+    # 1. the offered load (far beyond one GPU at 200/s): completions in the window
+    sampler = ClockSampler(local)
+    sampler.start()
+    with Server(SERVE_NS, capacity=slots, hbm_fraction=0.8) as srv:
+        caps = {N: srv.capacity(N) for N in SERVE_NS}
+        srv.submit([(N, Re, T, sd, a, 0) for N, Re, T, sd, a in reqs])
+        t0 = time.perf_counter()
+        srv.run(args.window)
+        wall = time.perf_counter() - t0
+        res = srv.results()
+        work = {N: srv.instance_steps(N) for N in SERVE_NS}
+    clocks = sampler.stop()
+    done = [r for r in res if r["done"] >= 0.0]
+    wall = max_over_ranks(wall, pg)
+    thr = world * len(done) / wall
+    step_bytes = sum(jvp_bytes(N) * k for N, k in work.items())
+    sat = latency_stats(res)
+
+    # 2. below saturation: 60% of the measured completion rate, drained
+    sub_rate = max(0.6 * len(done) / wall, 0.05)
+    reqs2 = serving_requests(sub_rate, args.window, seed=1000 + rank)
+    with Server(SERVE_NS, capacity=slots, hbm_fraction=0.8) as srv:
+        if reqs2:
+            srv.submit([(N, Re, T, sd, a, 0) for N, Re, T, sd, a in reqs2])
+            srv.run()
+        sub = latency_stats(srv.results())
+    sub["offered_rate_per_s"] = round(sub_rate, 3)
+    sub["offered"] = len(reqs2)
+
+    # 3. plain FP64 serial: the first requests of the stream, one at a time
+    sample = reqs[:6]
+    serial_s = 0.0
+    st = torch.cuda.Stream()
+    for N, Re, T, sd, _ in sample:
+        with Solver(N, N, N) as S:
+            S.set_stream(st)
+            S.set_forcing(S.to_device(W.kolmogorov_forcing(N, N, N)))
+            with torch.cuda.stream(st):
+                U, V = S.request_fields(Re, sd)
+                a = torch.cuda.Event(enable_timing=True)
+                z = torch.cuda.Event(enable_timing=True)
+                a.record()
+                S.rk3_ssp_uv(U, V, W.kolmogorov_dt(N, Re), Re,
+                             nsteps=request_steps(N, Re, T))
+                z.record()
+            z.synchronize()
+            serial_s += a.elapsed_time(z) / 1e3
+    serial = len(sample) / serial_s
+    return {
+        "metric": "JVP-request serving: completions/s with p50/p99 latency (Poisson "
+                  f"{args.rate:g}/s, N in {{64,96,128}}, Re in {{100,200,400}}, T ~ U[1,5], FP64)",
+        "value": round(thr, 4),
+        "unit": "completions/s",
+        "n_gpus": world,
+        "steps": len(done),
+        "warmup": 0,
+        "ms_per_step": round(1e3 / thr, 3) if thr > 0 else None,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "serving_jvp_poisson",
+                   "offered": len(reqs), "window_s": args.window,
+                   "slots": {str(N): caps[N] for N in SERVE_NS},
+                   "admission": "slots reserved from 80% of the free HBM, capped per grid; "
+                                "first come first served per grid; continuous batching "
+                                "per step",
+                   "saturated": sat, "sub_saturation": sub,
+                   "instance_steps": {str(N): k for N, k in work.items()},
+                   "serial_completions_per_s": round(serial, 4),
+                   "serial_protocol": "the first 6 requests one at a time through "
+                                      "ns3d_jvp_steps of a single-grid handle (plain FP64), "
+                                      "CUDA events",
+                   "speedup_vs_serial": round(thr / world / serial, 3)},
+        "roofline": {"bound": "hbm", "kernel": "all passes of every JVP step the server ran "
+                                               "in the window (330 S_c + 30 S_r per step)",
+                     "achieved": round(step_bytes / wall / 1e9, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(step_bytes / wall / 1e9 / peak, 4),
+                     "traffic": None, "peak_source": peak_src},
+        "e2e": {"value": round(thr, 4), "unit": "completions/s", "h2d_bytes_per_step": 48,
+                "d2h_bytes_per_step": 8,
+                "protocol": "requests (N, Re, T, seed) from the host, fields made on the "
+                            "device, |v(T)| back per request; wall clock"},
+        "gpu_launches": None,
+        "clocks": clocks,
+    }
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
     try:
-        if args.workload == "ensemble":
+        if args.workload == "serving":
+            if args.impl == "reference":
+                line = {"impl": "reference", "unavailable": "the reference has no request "
+                                                            "server; its one-at-a-time JVP is "
+                                                            "the serial figure of our line"}
+            else:
+                line = run_ours_serving(args, world, rank, local, pg)
+        elif args.workload == "ensemble":
             if args.impl == "reference":
                 line = run_reference_ensemble(args, world, rank, local, pg)
             else:

@@ -364,6 +364,74 @@ ns3d_status ns3d_ensemble_diagnostics(ns3d_ensemble* e, const ns3d_complex* ux,
                                       double* energy, double* dissipation);
 
 /* ----------------------------------------------------------------------- */
+/* request server: tangent integrations with continuous batching            */
+/* ----------------------------------------------------------------------- */
+
+/* No reference counterpart.  A request asks for the tangent (Jacobian-vector
+ * product) integration that NSCallMatrixVector_exponential performs
+ * (Source/NS3D_periodic.cu:444-470: RK3_SSP_UV steps, Source/RK_time_step.cu:
+ * 342-355) on an N^3 2 pi box: base state u = Kolmogorov laminar profile
+ * (Re/16) sin(4y) x plus a seeded 1e-3 perturbation, forcing sin(4y) x,
+ * tangent v = a seeded unit perturbation (both pure-imaginary,
+ * divergence-free, |k|^-2 on 1 <= |k| <= 8, made on the device from `seed`;
+ * ns3d_request_fields gives the same fields on a single-grid handle),
+ * steps = ceil(T / dt) with dt = 0.3 (2 pi / N) / (Re / 16).  The result is
+ * |v(T)| (L2 over the stored half spectrum) and, with keep = 1, v(T).
+ *
+ * The server reserves, per grid N, as many instance slots as hbm_fraction of
+ * the free device memory (split evenly over the grids) holds, at most
+ * capacity[i] when `capacity` is given (hbm_fraction outside (0, 1) with a
+ * capacity: exactly capacity[i]), and serves requests with continuous
+ * batching: whenever a grid's step finishes, finished requests leave,
+ * requests that have arrived take the free slots (first come, first served
+ * per grid), and the next step runs all active slots in one batch.  Grids
+ * run on their own streams and overlap.  A result does not depend on the mix
+ * it ran in (bit for bit).  Times are seconds on the server clock, which
+ * starts at the first ns3d_server_run. */
+typedef struct ns3d_server ns3d_server;
+typedef struct ns3d_request {
+  int N;
+  double Re, T;
+  unsigned long long seed;
+  double arrival; /* server-clock seconds; requests are submitted in arrival order */
+  int keep;       /* keep v(T) for ns3d_server_result_field */
+} ns3d_request;
+typedef struct ns3d_result {
+  long long id;
+  int N;
+  double Re, T;
+  int steps;
+  double arrival, admitted, done; /* -1: not yet */
+  double v_norm;
+  int status; /* -1 pending, NS3D_OK, NS3D_ERR_NONFINITE */
+} ns3d_result;
+
+ns3d_status ns3d_server_create(const int* Ns, int nN, const int* capacity, double hbm_fraction,
+                               ns3d_server** out);
+ns3d_status ns3d_server_destroy(ns3d_server* s);
+const char* ns3d_server_last_error(const ns3d_server* s);
+ns3d_status ns3d_server_capacity(const ns3d_server* s, int N, int* slots);
+/* JVP steps the grid N has launched so far, summed over its active slots
+ * (the work done, finished requests or not). */
+ns3d_status ns3d_server_stats(const ns3d_server* s, int N, long long* instance_steps);
+/* Queues n requests (ids first_id .. first_id + n - 1). */
+ns3d_status ns3d_server_submit(ns3d_server* s, const ns3d_request* r, int n, long long* first_id);
+/* Runs the engine on the calling thread until every submitted request is
+ * done or max_seconds have passed (then nothing more is admitted or launched
+ * and the steps in flight are finished; unfinished requests keep their slots
+ * for the next call); *completed = requests finished in this call. */
+ns3d_status ns3d_server_run(ns3d_server* s, double max_seconds, int* completed);
+/* All requests so far, in id order (*n = their count; up to cap copied). */
+ns3d_status ns3d_server_results(const ns3d_server* s, ns3d_result* out, int cap, int* n);
+ns3d_status ns3d_server_result_field(const ns3d_server* s, long long id, ns3d_complex* vx,
+                                     ns3d_complex* vy, ns3d_complex* vz);
+/* The request's initial (u, v) on a cubic single-grid handle, and its step count. */
+ns3d_status ns3d_request_fields(ns3d_solver* h, double Re, unsigned long long seed,
+                                ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
+                                ns3d_complex* vx, ns3d_complex* vy, ns3d_complex* vz);
+int ns3d_request_steps(int N, double Re, double T);
+
+/* ----------------------------------------------------------------------- */
 /* allocation-free nonlinear term                                           */
 /* ----------------------------------------------------------------------- */
 

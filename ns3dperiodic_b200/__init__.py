@@ -7,8 +7,9 @@ grid stepped together) and :class:`Krylov` (Arnoldi / implicit restart) are
 the Python host mirrors over it.
 """
 from ._lib import Ns3dError, Ns3dLibraryError, LIB_PATH  # noqa: F401
-from .solver import Ensemble, Solver, TimeSeries, supported_extent  # noqa: F401
+from .solver import (Ensemble, Server, Solver, TimeSeries, request_steps,  # noqa: F401
+                     supported_extent)
 from .krylov import Krylov, qr_shifts, select_shifts  # noqa: F401
 
-__all__ = ["Solver", "Ensemble", "TimeSeries", "supported_extent", "Krylov", "qr_shifts", "select_shifts", "Ns3dError",
+__all__ = ["Solver", "Ensemble", "Server", "TimeSeries", "request_steps", "supported_extent", "Krylov", "qr_shifts", "select_shifts", "Ns3dError",
            "Ns3dLibraryError", "LIB_PATH"]

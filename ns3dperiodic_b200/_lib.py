@@ -47,7 +47,25 @@ EXPORTS = (
     "ns3d_ensemble_create", "ns3d_ensemble_destroy", "ns3d_ensemble_set_stream",
     "ns3d_ensemble_last_error", "ns3d_ensemble_device_bytes", "ns3d_ensemble_set_forcing",
     "ns3d_ensemble_set_params", "ns3d_ensemble_rk3_steps", "ns3d_ensemble_diagnostics",
+    "ns3d_server_create", "ns3d_server_destroy", "ns3d_server_last_error",
+    "ns3d_server_capacity", "ns3d_server_stats", "ns3d_server_submit", "ns3d_server_run", "ns3d_server_results",
+    "ns3d_server_result_field", "ns3d_request_fields", "ns3d_request_steps",
 )
+
+class Request(ctypes.Structure):
+    """ns3d_request of include/ns3d.h."""
+    _fields_ = [("N", ctypes.c_int), ("Re", ctypes.c_double), ("T", ctypes.c_double),
+                ("seed", ctypes.c_ulonglong), ("arrival", ctypes.c_double),
+                ("keep", ctypes.c_int)]
+
+
+class Result(ctypes.Structure):
+    """ns3d_result of include/ns3d.h."""
+    _fields_ = [("id", ctypes.c_longlong), ("N", ctypes.c_int), ("Re", ctypes.c_double),
+                ("T", ctypes.c_double), ("steps", ctypes.c_int), ("arrival", ctypes.c_double),
+                ("admitted", ctypes.c_double), ("done", ctypes.c_double),
+                ("v_norm", ctypes.c_double), ("status", ctypes.c_int)]
+
 
 # the matrix-vector callback type of ns3d_arnoldi: void (*)(void*, void*, void*)
 MAP_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
@@ -174,6 +192,17 @@ def _sig(lib):
         "ns3d_ensemble_set_params": ([_P, _P, _P], c_int),
         "ns3d_ensemble_rk3_steps": ([_P, _P, _P, _P, c_int], c_int),
         "ns3d_ensemble_diagnostics": ([_P, _P, _P, _P, _P, _P], c_int),
+        "ns3d_server_create": ([_P, c_int, _P, c_double, ctypes.POINTER(c_void_p)], c_int),
+        "ns3d_server_destroy": ([_P], c_int),
+        "ns3d_server_last_error": ([_P], ctypes.c_char_p),
+        "ns3d_server_capacity": ([_P, c_int, _P], c_int),
+        "ns3d_server_stats": ([_P, c_int, _P], c_int),
+        "ns3d_server_submit": ([_P, _P, c_int, _P], c_int),
+        "ns3d_server_run": ([_P, c_double, _P], c_int),
+        "ns3d_server_results": ([_P, _P, c_int, _P], c_int),
+        "ns3d_server_result_field": ([_P, ctypes.c_longlong, _P, _P, _P], c_int),
+        "ns3d_request_fields": ([_P, c_double, ctypes.c_ulonglong] + [_P] * 6, c_int),
+        "ns3d_request_steps": ([c_int, c_double, c_double], c_int),
     }
     for name, (args, res) in S.items():
         f = getattr(lib, name)

@@ -24,7 +24,7 @@ COMPAT_SOURCE = "compat.cu"
 
 SOURCES = ["k_xy.cu", "k_z.cu", "k_fwdx.cu", "k_fft3d.cu", "aux_kernels.cu", "solver.cu",
            "noalloc.cu", "krylov.cu", "qr_shifts.cpp", "checkpoint.cpp",
-           "diag_kernels.cu", "series.cpp"]
+           "diag_kernels.cu", "series.cpp", "server.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",

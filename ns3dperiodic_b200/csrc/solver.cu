@@ -12,6 +12,7 @@
 #include "aux_kernels.cuh"
 #include "diag_kernels.cuh"
 #include "dispatch.h"
+#include "solver_internal.h"
 
 using ns3d::FwdXArgs;
 using ns3d::FwdYArgs;
@@ -19,68 +20,11 @@ using ns3d::InvXArgs;
 using ns3d::InvYArgs;
 using ns3d::PassGeom;
 using ns3d::ZArgs;
+using namespace ns3d_detail;
 
-namespace {
 
-constexpr int kForcingCap = 4096;
-constexpr int kDiagBlocks = 592;  // 4 x 148 SMs
-constexpr int kDiagThreads = 256;
 
-}  // namespace
-
-struct ns3d_solver {
-  int Nx = 0, Ny = 0, Nz = 0, Mz = 0;
-  double Lx = 0, Ly = 0, Lz = 0;
-  size_t nc = 0;  // complex points per field (one instance)
-  int batch = 1;  // instances stepped together (ns3d_ensemble); scratch is batch x nc
-  double* dtRe = nullptr;  // per instance (dt, Re) of a batch, device
-  double ens_dt = 0.0, ens_Re = 0.0;  // the same for an ensemble of one
-  bool ens_params = false;            // ns3d_ensemble_set_params was called
-  int device = 0;
-  PassGeom geom{};
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  // tables
-  uint16_t* qcut = nullptr;
-  double2* tw[3] = {};
-  // scratch: base pool (21 fields) and tangent pool (18 fields, lazily)
-  double2* pool_base = nullptr;
-  double2* pool_uv = nullptr;
-  double2* A[6] = {};
-  double2* B[6] = {};
-  double2* C[6] = {};
-  double2* D[6] = {};
-  double2* E[6] = {};
-  double2* u1[3] = {};
-  double2* u2[3] = {};
-  double2* v1[3] = {};
-  // forcing
-  int* f_count = nullptr;
-  int* f_idx = nullptr;
-  double2* f_val = nullptr;
-  int f_nnz = 0;
-  const double2* f_dense[3] = {};
-  // diagnostics
-  double* diag_partial = nullptr;
-  double* diag_out = nullptr;
-  // record / spectrum / Shapiro buffers (allocated on first use)
-  double2* rec_tab = nullptr;
-  double* rec_partial = nullptr;  // kDiagBlocks x kRecordSums, then 2 x kDiagBlocks min/max
-  double* rec_out = nullptr;      // 50 record columns, then 2 min/max
-  ns3d::RecordReads rec_reads{};
-  long long rec_points[3] = {};
-  // cached RK3 step graph
-  cudaGraphExec_t rk3_exec = nullptr;
-  const void* rk3_key[3] = {};
-  double rk3_dt = 0.0, rk3_Re = 0.0;
-  cudaStream_t rk3_stream = nullptr;
-  int f_version = 0, rk3_fversion = -1;
-  bool graphs_off = false;
-  size_t bytes = 0;
-  std::string err;
-};
-
-namespace {
+namespace ns3d_detail {
 
 ns3d_status fail(ns3d_solver* h, ns3d_status s, const std::string& msg) {
   if (h) h->err = msg;
@@ -92,11 +36,6 @@ ns3d_status cuda_fail(ns3d_solver* h, cudaError_t e, const char* where) {
               std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-#define NS3D_CHECK(h, call, where)                 \
-  do {                                             \
-    cudaError_t e_ = (call);                       \
-    if (e_ != cudaSuccess) return cuda_fail(h, e_, where); \
-  } while (0)
 
 void build_twiddles(int N, std::vector<double2>& out) {
   out.resize(N);
@@ -161,18 +100,19 @@ bool valid_extents(int Nx, int Ny, int Nz) {
 
 ns3d_status ensure_uv_pool(ns3d_solver* h) {
   if (h->pool_uv) return NS3D_OK;
-  const size_t bytes = sizeof(double2) * h->nc * 18;
+  const size_t field = h->nc * (size_t)h->batch;
+  const size_t bytes = sizeof(double2) * field * 18;
   NS3D_CHECK(h, cudaMalloc(&h->pool_uv, bytes), "cudaMalloc(tangent scratch)");
   h->bytes += bytes;
   double2* p = h->pool_uv;
   for (int i = 3; i < 6; ++i) {
-    h->A[i] = p; p += h->nc;
-    h->B[i] = p; p += h->nc;
-    h->C[i] = p; p += h->nc;
-    h->D[i] = p; p += h->nc;
-    h->E[i] = p; p += h->nc;
+    h->A[i] = p; p += field;
+    h->B[i] = p; p += field;
+    h->C[i] = p; p += field;
+    h->D[i] = p; p += field;
+    h->E[i] = p; p += field;
   }
-  for (int i = 0; i < 3; ++i) { h->v1[i] = p; p += h->nc; }
+  for (int i = 0; i < 3; ++i) { h->v1[i] = p; p += field; }
   return NS3D_OK;
 }
 
@@ -242,7 +182,7 @@ ns3d_status finish(ns3d_solver* h, int mode, bool forcing, const double2* const 
   a.fnnz = (forcing && !h->f_dense[0]) ? h->f_nnz : 0;
   a.dt = dt;
   a.Re = Re;
-  a.dtRe = h->batch > 1 ? h->dtRe : nullptr;
+  a.dtRe = h->dtRe;  // allocated for batches (and server grids) only
   a.ca = ca;
   a.cb = cb;
   a.tw = h->tw[0];
@@ -250,11 +190,6 @@ ns3d_status finish(ns3d_solver* h, int mode, bool forcing, const double2* const 
   return NS3D_OK;
 }
 
-#define NS3D_TRY(expr)                 \
-  do {                                 \
-    ns3d_status s_ = (expr);           \
-    if (s_ != NS3D_OK) return s_;      \
-  } while (0)
 
 // RK3_SSP (Source/RK_time_step.cu:310-327) with every stage fused:
 //   u1 = u + dt L(u); u2 = 3/4 u + 1/4 (u1 + dt L(u1)); u = 1/3 u + 2/3 (u2 + dt L(u2))
@@ -333,7 +268,8 @@ ns3d_status ns3d_twiddles(int N, double* tw) {
   return NS3D_OK;
 }
 
-namespace {
+extern "C++" {
+namespace ns3d_detail {
 ns3d_status create_solver(int batch, int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
                           ns3d_solver** out) {
   if (!out) return NS3D_ERR_BAD_ARG;
@@ -410,7 +346,8 @@ ns3d_status create_solver(int batch, int Nx, int Ny, int Nz, double Lx, double L
   *out = h;
   return NS3D_OK;
 }
-}  // namespace
+}  // namespace ns3d_detail
+}  // extern "C++"
 
 ns3d_status ns3d_create(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
                         ns3d_solver** out) {
@@ -496,7 +433,8 @@ ns3d_status ns3d_rk3_step(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns
   return ns3d_rk3_steps(h, ux, uy, uz, dt, Re, 1);
 }
 
-namespace {
+extern "C++" {
+namespace ns3d_detail {
 // nsteps RK3 steps, through a captured graph where the stream allows it.  A
 // batch reads its per-instance dt and Re from h->dtRe (dt, Re here are 0).
 ns3d_status rk3_steps_impl(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
@@ -544,7 +482,8 @@ ns3d_status rk3_steps_impl(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, n
     NS3D_CHECK(h, cudaGraphLaunch(h->rk3_exec, h->stream), "graph launch");
   return NS3D_OK;
 }
-}  // namespace
+}  // namespace ns3d_detail
+}  // extern "C++"
 
 ns3d_status ns3d_rk3_steps(ns3d_solver* h, ns3d_complex* ux, ns3d_complex* uy, ns3d_complex* uz,
                            double dt, double Re, int nsteps) {
@@ -597,7 +536,8 @@ ns3d_status ns3d_fft_r2c(ns3d_solver* h, const double* in, ns3d_complex* out) {
   return NS3D_OK;
 }
 
-namespace {
+extern "C++" {
+namespace ns3d_detail {
 ns3d_status fft_c2r(ns3d_solver* h, const ns3d_complex* in, double* out, double scale) {
   NS3D_TRY(check_handle(h));
   if (!in || !out) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
@@ -618,7 +558,8 @@ ns3d_status fft_c2r(ns3d_solver* h, const ns3d_complex* in, double* out, double 
   NS3D_CHECK(h, ns3d::run_z_c2r(z, g, h->stream), "z_c2r");
   return NS3D_OK;
 }
-}  // namespace
+}  // namespace ns3d_detail
+}  // extern "C++"
 
 ns3d_status ns3d_fft_c2r(ns3d_solver* h, const ns3d_complex* in, double* out) {
   return h ? fft_c2r(h, in, out, h->geom.inv_vol) : NS3D_ERR_BAD_ARG;
@@ -887,7 +828,8 @@ ns3d_status ns3d_diagnostics(ns3d_solver* h, const ns3d_complex* ux, const ns3d_
 // Filters, curl, the per-step record, the energy spectrum, Shapiro's solution
 // ---------------------------------------------------------------------------
 
-namespace {
+extern "C++" {
+namespace ns3d_detail {
 
 ns3d::GridGeom grid_geom(const ns3d_solver* h) {
   ns3d::GridGeom g{};
@@ -1021,7 +963,8 @@ ns3d_status shapiro_minmax(ns3d_solver* h, const double* ux, const double* uy, c
   return NS3D_OK;
 }
 
-}  // namespace
+}  // namespace ns3d_detail
+}  // extern "C++"
 
 ns3d_status ns3d_helmholtz_filter(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
                                   const ns3d_complex* uz, double eps, ns3d_complex* fx,

@@ -12,7 +12,7 @@ import ctypes
 import math
 from typing import Sequence
 
-from ._lib import Ns3dError, lib
+from ._lib import Ns3dError, Request, Result, lib
 
 _PI2 = 2.0 * math.pi
 
@@ -373,6 +373,14 @@ class Solver:
                                                float(Re), ctypes.byref(e)), "ns3d_shapiro_error")
         return e.value
 
+    def request_fields(self, Re: float, seed: int):
+        """The initial (u, v) of a server request on this (cubic) grid."""
+        U, V = self.zeros(), self.zeros()
+        self._check(self._L.ns3d_request_fields(self._h, float(Re), int(seed),
+                                                *self._fields(U, "U"), *self._fields(V, "V")),
+                    "ns3d_request_fields")
+        return U, V
+
     def profile_passes(self, U, dt: float, Re: float, reps: int = 10):
         """Mean ms per launch of (inv_x, inv_y, z, fwd_y, fwd_x), CUDA events."""
         ms = (ctypes.c_double * 5)()
@@ -600,6 +608,118 @@ class Ensemble:
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             self._L.ns3d_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def request_steps(N: int, Re: float, T: float) -> int:
+    """JVP steps of a server request: ceil(T / dt), dt = 0.3 (2 pi/N) / (Re/16)."""
+    return int(lib().ns3d_request_steps(int(N), float(Re), float(T)))
+
+
+class Server:
+    """ns3d_server: tangent-integration requests served with continuous
+    batching, one batched slot pool per grid N (see include/ns3d.h)."""
+
+    def __init__(self, Ns, capacity=None, hbm_fraction: float = 0.0, device=None):
+        """capacity: slots per grid (at most, with hbm_fraction in (0, 1));
+        without it, hbm_fraction (default 0.5) of the free device memory sets
+        them."""
+        import torch
+
+        if capacity is None and not 0.0 < hbm_fraction < 1.0:
+            hbm_fraction = 0.5
+        self._L = lib()
+        dev = torch.device(device if device is not None else "cuda")
+        Ns = [int(n) for n in Ns]
+        arr = (ctypes.c_int * len(Ns))(*Ns)
+        cap = (ctypes.c_int * len(Ns))(*[int(c) for c in capacity]) if capacity else None
+        h = ctypes.c_void_p()
+        with torch.cuda.device(dev):
+            torch.cuda.init()
+            rc = self._L.ns3d_server_create(arr, len(Ns), cap, float(hbm_fraction),
+                                            ctypes.byref(h))
+        if rc != 0:
+            raise Ns3dError(rc, "ns3d_server_create")
+        self._h = h
+        self.Ns = Ns
+
+    def _check(self, rc, where):
+        if rc != 0:
+            d = self._L.ns3d_server_last_error(self._h)
+            raise Ns3dError(rc, where, d.decode() if d else "")
+
+    def capacity(self, N: int) -> int:
+        c = ctypes.c_int()
+        self._check(self._L.ns3d_server_capacity(self._h, int(N), ctypes.byref(c)),
+                    "ns3d_server_capacity")
+        return c.value
+
+    def instance_steps(self, N: int) -> int:
+        """JVP steps grid N has run so far, summed over its slots."""
+        c = ctypes.c_longlong()
+        self._check(self._L.ns3d_server_stats(self._h, int(N), ctypes.byref(c)),
+                    "ns3d_server_stats")
+        return c.value
+
+    def submit(self, requests):
+        """requests: iterable of dicts or tuples (N, Re, T, seed[, arrival[, keep]]),
+        in arrival order.  Returns the first id."""
+        rs = []
+        for r in requests:
+            if isinstance(r, dict):
+                rs.append(Request(int(r["N"]), float(r["Re"]), float(r["T"]), int(r["seed"]),
+                                  float(r.get("arrival", 0.0)), int(r.get("keep", 0))))
+            else:
+                rs.append(Request(int(r[0]), float(r[1]), float(r[2]), int(r[3]),
+                                  float(r[4]) if len(r) > 4 else 0.0,
+                                  int(r[5]) if len(r) > 5 else 0))
+        arr = (Request * max(len(rs), 1))(*rs)
+        first = ctypes.c_longlong()
+        self._check(self._L.ns3d_server_submit(self._h, arr, len(rs), ctypes.byref(first)),
+                    "ns3d_server_submit")
+        return first.value
+
+    def run(self, max_seconds: float = 1e30) -> int:
+        n = ctypes.c_int()
+        self._check(self._L.ns3d_server_run(self._h, float(max_seconds), ctypes.byref(n)),
+                    "ns3d_server_run")
+        return n.value
+
+    def results(self):
+        n = ctypes.c_int()
+        self._check(self._L.ns3d_server_results(self._h, None, 0, ctypes.byref(n)),
+                    "ns3d_server_results")
+        arr = (Result * max(n.value, 1))()
+        self._check(self._L.ns3d_server_results(self._h, arr, n.value, ctypes.byref(n)),
+                    "ns3d_server_results")
+        return [{f: getattr(arr[i], f) for f, _ in Result._fields_} for i in range(n.value)]
+
+    def result_field(self, rid: int, N: int):
+        """v(T) of a request submitted with keep = 1 (host numpy arrays)."""
+        import numpy as np
+
+        Mz = N // 2 + 1
+        v = [np.zeros((N, N, Mz), np.complex128) for _ in range(3)]
+        self._check(self._L.ns3d_server_result_field(self._h, int(rid),
+                                                     *[x.ctypes.data for x in v]),
+                    "ns3d_server_result_field")
+        return v
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._L.ns3d_server_destroy(self._h)
             self._h = None
 
     def __del__(self):
