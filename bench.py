@@ -59,6 +59,8 @@ def parse():
                     help="rk3: the RK3 step (default); arnoldi: the Krylov factorisation; "
                          "ensemble: mixed-N Kolmogorov instances stepped as batches")
     ap.add_argument("--instances", type=int, default=64, help="ensemble size")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
+                    help="fp32: transforms and products in FP32, state and update in FP64")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: mean arrivals per s")
     ap.add_argument("--window", type=float, default=45.0, help="serving: seconds of arrivals")
     ap.add_argument("--slots", default="16,8,4", help="serving: slots for N = 64,96,128")
@@ -265,6 +267,8 @@ def run_ours(args, world, rank, local, pg):
     S = Solver(N, N, N)
     stream = torch.cuda.Stream()
     S.set_stream(stream)
+    S.precision = args.precision
+    fp32 = args.precision == "fp32"
     U = S.to_device(U0)
     F = S.to_device(F0)
     torch.cuda.synchronize()
@@ -293,7 +297,9 @@ def run_ours(args, world, rank, local, pg):
 
     # per-pass timing (CUDA events on the launching stream), dominant kernel
     names = ["inv_x", "inv_y", "z", "fwd_y", "fwd_x"]
-    alg = [9 * Sc, 15 * Sc, 12 * Sc, 6 * Sc, 9 * Sc]  # algorithmic bytes per launch
+    # algorithmic bytes per launch; FP32 scratch halves every field but the state
+    alg = ([6 * Sc, 7.5 * Sc, 6 * Sc, 3 * Sc, 7.5 * Sc] if fp32 else
+           [9 * Sc, 15 * Sc, 12 * Sc, 6 * Sc, 9 * Sc])
     with torch.cuda.stream(stream):
         pm = S.profile_passes(U, dt, Re, reps=20)
     dom = max(range(5), key=lambda i: pm[i])
@@ -339,10 +345,27 @@ def run_ours(args, world, rank, local, pg):
            "steps": K,
            "protocol": "pinned host state+forcing -> device, K x (ns3d_rk3_step + "
                        "ns3d_diagnostics read-back), final state -> host; wall clock"}
+    accuracy = None
+    if fp32:
+        # the FP32 mode against FP64 from the same state over the timed steps
+        with torch.cuda.stream(stream):
+            U32 = S.rk3_ssp(S.to_device(U0), dt, Re, nsteps=args.steps)
+            e32 = S.diagnostics(U32)[0]
+            S.precision = "fp64"
+            U64 = S.rk3_ssp(S.to_device(U0), dt, Re, nsteps=args.steps)
+            e64 = S.diagnostics(U64)[0]
+            num = sum(float(torch.linalg.vector_norm(a - b)) ** 2 for a, b in zip(U32, U64))
+            den = sum(float(torch.linalg.vector_norm(b)) ** 2 for b in U64)
+        stream.synchronize()
+        accuracy = {"steps": args.steps, "rel_l2_u_vs_fp64": math.sqrt(num / den),
+                    "energy_rel_diff_vs_fp64": abs(e32 - e64) / abs(e64),
+                    "tolerance": 1e-5}
     S.close()
-    p3l = 159 * Sc + 18 * Sr
+    # P3L bytes; FP32 mode: 3 RHS of 30 S_c (6 + 7.5 + 6 + 3 + 7.5) plus the
+    # FP64 partners u^n of stages 2 and 3 (6 S_c)
+    p3l = (90 + 6) * Sc + 9 * Sr if fp32 else 159 * Sc + 18 * Sr
     line = {
-        "metric": f"RK3 steps/s (Kolmogorov {N}^3 FP64)",
+        "metric": f"RK3 steps/s (Kolmogorov {N}^3 {'FP32 mode' if fp32 else 'FP64'})",
         "value": round(value, 3),
         "unit": "steps/s",
         "n_gpus": world,
@@ -352,9 +375,9 @@ def run_ours(args, world, rank, local, pg):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f32 (transforms, products); f64 (state, update)" if fp32 else "f64",
         "data": "synthetic",
-        "config": {"workload": f"kolmogorov_{N}^3_fp64", "N": N, "Re": Re, "dt": dt,
+        "config": {"workload": f"kolmogorov_{N}^3_{args.precision}", "N": N, "Re": Re, "dt": dt,
                    "forcing": "sin(4y) x", "perturbation": "seeded 1e-3, |k|^-2 on 1<=|k|<=8",
                    "parallelism": f"replicas x{world}",
                    "l2": f"working set {(24 * Sc) / 1e6:.0f} MB (state + scratch) > 126 MB L2",
@@ -362,7 +385,8 @@ def run_ours(args, world, rank, local, pg):
                    "p3l_bytes_per_step": p3l,
                    "p3l_gbs": round(p3l / (ms_step * 1e-3) / 1e9, 1),
                    "p3l_frac": round(p3l / (ms_step * 1e-3) / 1e9 / peak, 4),
-                   "diag_last": diag},
+                   "diag_last": diag,
+                   "fp32_accuracy": accuracy},
         "roofline": roofline,
         "e2e": e2e,
         "gpu_launches": 15 * args.steps,
@@ -655,6 +679,7 @@ def run_ours_ensemble(args, world, rank, local, pg):
     for N, members in sorted(groups.items()):
         states = [W.kolmogorov_state(N, Re, seed) for seed, Re in members]
         E = Ensemble(len(members), N, N, N)
+        E.set_precision(args.precision)
         st = torch.cuda.Stream()
         E.set_stream(st)
         E.set_forcing(states[0][1])
@@ -709,6 +734,7 @@ def run_ours_ensemble(args, world, rank, local, pg):
     one = {N: [S.zeros() for _ in range(1)] for N, S in solo.items()}
     torch.cuda.synchronize()
     t_serial = 0.0
+    rel_err = []
     cm = torch.cuda.stream(solo_st)
     cm.__enter__()
     for N, members in sorted(groups.items()):
@@ -729,6 +755,13 @@ def run_ours_ensemble(args, world, rank, local, pg):
             z.synchronize()
             t_serial += a.elapsed_time(z)
             # identical to the batched result, instance by instance
+            if args.precision == "fp32":  # error of the FP32 ensemble against FP64 alone
+                num = sum(float(torch.linalg.vector_norm(fields[N][c][b] - U[c])) ** 2
+                          for c in range(3))
+                den = sum(float(torch.linalg.vector_norm(U[c])) ** 2 for c in range(3))
+                if math.isfinite(num) and math.isfinite(den) and den > 0:
+                    rel_err.append(math.sqrt(num / den))
+                continue
             for c in range(3):  # (diverged instances hold NaN in the same places)
                 if not torch.equal(torch.nan_to_num(U[c]), torch.nan_to_num(fields[N][c][b])):
                     raise AssertionError(f"ensemble instance {seed} (N={N}) differs from its solo run")
@@ -756,7 +789,7 @@ def run_ours_ensemble(args, world, rank, local, pg):
     serial = len(inst) / (t_serial / 1e3)
     return {
         "metric": "mixed-N ensemble solves/s (64 Kolmogorov instances, N in {32,48,64,96,128}, "
-                  "Re in [50,500], 200 RK3 steps each, FP64)",
+                  f"Re in [50,500], 200 RK3 steps each, {args.precision.upper()})",
         "value": round(value, 3),
         "unit": "solves/s",
         "n_gpus": world,
@@ -766,9 +799,14 @@ def run_ours_ensemble(args, world, rank, local, pg):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": ("f32 (transforms, products); f64 (state, update)"
+                  if args.precision == "fp32" else "f64"),
         "data": "synthetic",
-        "config": {"workload": f"ensemble_{len(inst)}x_mixedN_fp64",
+        "config": {"workload": f"ensemble_{len(inst)}x_mixedN_{args.precision}",
+                   "fp32_rel_l2_vs_fp64": ({"max": max(rel_err), "median":
+                                            statistics.median(rel_err),
+                                            "instances": len(rel_err), "tolerance": 1e-5}
+                                           if rel_err else None),
                    "instances_per_N": {str(N): len(m) for N, m in sorted(groups.items())},
                    "dt": "CFL 0.3 of the laminar peak Re/16 per instance",
                    "parallelism": f"replicas x{world}; one batched ensemble per N, each on its "
@@ -777,7 +815,7 @@ def run_ours_ensemble(args, world, rank, local, pg):
                    "serial_solves_per_s": round(serial, 3),
                    "serial_protocol": "the same instances one by one, ns3d_rk3_steps of a "
                                       "single-instance handle (plain FP64), CUDA events; "
-                                      "results identical to the batched ones",
+                                      "FP64 batched results identical to them",
                    "speedup_vs_serial": round(value / world / serial, 3),
                    "diverged_instances": diverged,
                    "diverged_note": "under-resolved high-Re instances overflow within the "

@@ -329,6 +329,25 @@ ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns
                                 double* ms);
 
 /* ----------------------------------------------------------------------- */
+/* precision mode                                                           */
+/* ----------------------------------------------------------------------- */
+
+/* No reference counterpart (the reference is FP64 throughout).  In the FP32
+ * mode the nonlinear term is formed in single precision: the inverse and
+ * forward transforms of the RHS pipeline and the physical-space products
+ * run on float2 scratch, while the state, the forcing, the projection,
+ * diffusion and RK combination of the update, and every diagnostic stay in
+ * FP64 (the state is read in FP64 and rounded once per stage; the FP32
+ * products are widened before the update).  It applies to every stepper of
+ * the handle (RK3, Euler, RHS, the tangent steppers) until changed; the
+ * plain transforms (ns3d_fft_*) and diagnostics stay FP64.  The default is
+ * FP64, the reference's arithmetic.  Synchronises the handle's stream. */
+#define NS3D_PRECISION_FP64 0
+#define NS3D_PRECISION_FP32 1
+ns3d_status ns3d_set_precision(ns3d_solver* h, int precision);
+int ns3d_get_precision(const ns3d_solver* h);
+
+/* ----------------------------------------------------------------------- */
 /* ensembles: many independent instances of one grid stepped together       */
 /* ----------------------------------------------------------------------- */
 
@@ -352,6 +371,8 @@ size_t ns3d_ensemble_device_bytes(const ns3d_ensemble* e);
 /* One instance-sized forcing, shared by every instance (as ns3d_set_forcing). */
 ns3d_status ns3d_ensemble_set_forcing(ns3d_ensemble* e, const ns3d_complex* fx,
                                       const ns3d_complex* fy, const ns3d_complex* fz);
+/* ns3d_set_precision for the whole ensemble. */
+ns3d_status ns3d_ensemble_set_precision(ns3d_ensemble* e, int precision);
 /* Host arrays of `batch` entries; synchronous.  Required before stepping. */
 ns3d_status ns3d_ensemble_set_params(ns3d_ensemble* e, const double* dt, const double* Re);
 /* nsteps RK3 steps of every instance, in place.  Asynchronous. */
@@ -411,6 +432,8 @@ ns3d_status ns3d_server_create(const int* Ns, int nN, const int* capacity, doubl
 ns3d_status ns3d_server_destroy(ns3d_server* s);
 const char* ns3d_server_last_error(const ns3d_server* s);
 ns3d_status ns3d_server_capacity(const ns3d_server* s, int N, int* slots);
+/* ns3d_set_precision for every grid of the server (between runs). */
+ns3d_status ns3d_server_set_precision(ns3d_server* s, int precision);
 /* JVP steps the grid N has launched so far, summed over its active slots
  * (the work done, finished requests or not). */
 ns3d_status ns3d_server_stats(const ns3d_server* s, int N, long long* instance_steps);

@@ -47,8 +47,9 @@ EXPORTS = (
     "ns3d_ensemble_create", "ns3d_ensemble_destroy", "ns3d_ensemble_set_stream",
     "ns3d_ensemble_last_error", "ns3d_ensemble_device_bytes", "ns3d_ensemble_set_forcing",
     "ns3d_ensemble_set_params", "ns3d_ensemble_rk3_steps", "ns3d_ensemble_diagnostics",
+    "ns3d_set_precision", "ns3d_get_precision", "ns3d_ensemble_set_precision",
     "ns3d_server_create", "ns3d_server_destroy", "ns3d_server_last_error",
-    "ns3d_server_capacity", "ns3d_server_stats", "ns3d_server_submit", "ns3d_server_run", "ns3d_server_results",
+    "ns3d_server_capacity", "ns3d_server_stats", "ns3d_server_set_precision", "ns3d_server_submit", "ns3d_server_run", "ns3d_server_results",
     "ns3d_server_result_field", "ns3d_request_fields", "ns3d_request_steps",
 )
 
@@ -192,11 +193,15 @@ def _sig(lib):
         "ns3d_ensemble_set_params": ([_P, _P, _P], c_int),
         "ns3d_ensemble_rk3_steps": ([_P, _P, _P, _P, c_int], c_int),
         "ns3d_ensemble_diagnostics": ([_P, _P, _P, _P, _P, _P], c_int),
+        "ns3d_set_precision": ([_P, c_int], c_int),
+        "ns3d_get_precision": ([_P], c_int),
+        "ns3d_ensemble_set_precision": ([_P, c_int], c_int),
         "ns3d_server_create": ([_P, c_int, _P, c_double, ctypes.POINTER(c_void_p)], c_int),
         "ns3d_server_destroy": ([_P], c_int),
         "ns3d_server_last_error": ([_P], ctypes.c_char_p),
         "ns3d_server_capacity": ([_P, c_int, _P], c_int),
         "ns3d_server_stats": ([_P, c_int, _P], c_int),
+        "ns3d_server_set_precision": ([_P, c_int], c_int),
         "ns3d_server_submit": ([_P, _P, c_int, _P], c_int),
         "ns3d_server_run": ([_P, c_double, _P], c_int),
         "ns3d_server_results": ([_P, _P, c_int, _P], c_int),

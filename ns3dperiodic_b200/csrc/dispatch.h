@@ -11,13 +11,21 @@ namespace ns3d {
 
 bool extent_supported(int n);
 
+// FP64 scratch (double2) and the FP32 precision mode (float2 scratch).
 cudaError_t run_inv_x(const InvXArgs<3>& a, const PassGeom& g, cudaStream_t st);
 cudaError_t run_inv_x(const InvXArgs<6>& a, const PassGeom& g, cudaStream_t st);
 cudaError_t run_inv_y(const InvYArgs<3>& a, const PassGeom& g, cudaStream_t st);
 cudaError_t run_inv_y(const InvYArgs<6>& a, const PassGeom& g, cudaStream_t st);
-cudaError_t run_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_fwd_y(const FwdYArgs<>& a, const PassGeom& g, cudaStream_t st);
 cudaError_t run_z(const ZArgs<3>& a, const PassGeom& g, cudaStream_t st);
 cudaError_t run_z(const ZArgs<6>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_x(const InvXArgs<3, float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_x(const InvXArgs<6, float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_y(const InvYArgs<3, float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_y(const InvYArgs<6, float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_fwd_y(const FwdYArgs<float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_z(const ZArgs<3, float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_z(const ZArgs<6, float2>& a, const PassGeom& g, cudaStream_t st);
 // Launch attributes of the pipelined passes for this geometry on the current
 // device; called when a handle is created (outside any stream capture).
 cudaError_t prepare_xy(const PassGeom& g);
@@ -29,7 +37,9 @@ cudaError_t run_z_c2r(const ZPlainArgs& a, const PassGeom& g, cudaStream_t st);
 cudaError_t run_z_r2c(const ZPlainArgs& a, const PassGeom& g, cudaStream_t st);
 cudaError_t prepare_fft3d(const PassGeom& g);
 // mode: UpdateMode; combine: out = ca*un + cb*base
-cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs& a, const PassGeom& g,
+cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs<>& a, const PassGeom& g,
+                      cudaStream_t st);
+cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs<float2>& a, const PassGeom& g,
                       cudaStream_t st);
 
 }  // namespace ns3d

@@ -1,4 +1,4 @@
-// FP64 line-FFT engine for sm_100a.
+// Line-FFT engine for sm_100a (FP64 and FP32 lines).
 //
 // One line of N complex points is owned by T = N/P threads of ONE warp (or of
 // the whole CTA when T > 32); thread t keeps the P points at positions
@@ -16,7 +16,8 @@
 // tw[e] = (cos 2*pi*e/N, sin 2*pi*e/N), e in [0, N).
 //
 // DIR = +1 is the inverse (e^{+i}) transform, DIR = -1 the forward one; both
-// unnormalised.
+// unnormalised.  Lines are double2 (FP64) or float2 (FP32, the precision
+// mode); the twiddle tables are FP64 in global memory and rounded on load.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -26,19 +27,52 @@
 namespace ns3d {
 
 // ---------------------------------------------------------------------------
-// complex helpers
+// complex helpers, for double2 (FP64) and float2 (FP32) lines
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
-__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+template <typename C>
+struct CTraits;
+template <>
+struct CTraits<double2> {
+  using R = double;
+  __host__ __device__ __forceinline__ static double2 make(double x, double y) {
+    return make_double2(x, y);
+  }
+};
+template <>
+struct CTraits<float2> {
+  using R = float;
+  __host__ __device__ __forceinline__ static float2 make(float x, float y) {
+    return make_float2(x, y);
+  }
+};
+template <typename C>
+using RealOf = typename CTraits<C>::R;
+template <typename C>
+__device__ __forceinline__ C mkc(RealOf<C> x, RealOf<C> y) {
+  return CTraits<C>::make(x, y);
+}
+// a complex value of another precision (FP64 state <-> FP32 scratch)
+template <typename C, typename D>
+__device__ __forceinline__ C cvt(D a) {
+  return mkc<C>((RealOf<C>)a.x, (RealOf<C>)a.y);
+}
+
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) { return mkc<C>(a.x + b.x, a.y + b.y); }
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) { return mkc<C>(a.x - b.x, a.y - b.y); }
+template <typename C>
+__device__ __forceinline__ C cscale(C a, RealOf<C> s) { return mkc<C>(a.x * s, a.y * s); }
+template <typename C>
+__device__ __forceinline__ C cconj(C a) { return mkc<C>(a.x, -a.y); }
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  return mkc<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 // a * (DIR * i)
-template <int DIR>
-__device__ __forceinline__ double2 cmul_i(double2 a) {
-  return DIR > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+template <int DIR, typename C>
+__device__ __forceinline__ C cmul_i(C a) {
+  return DIR > 0 ? mkc<C>(-a.y, a.x) : mkc<C>(a.y, -a.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -61,23 +95,24 @@ __host__ __device__ constexpr double cos48(int a) {
 __host__ __device__ constexpr double sin48(int a) { return cos48(a - 12); }
 
 // v * exp(DIR * 2*pi*i * E / R)
-template <int R, int E, int DIR>
-__device__ __forceinline__ double2 rot(double2 v) {
+template <int R, int E, int DIR, typename C>
+__device__ __forceinline__ C rot(C v) {
+  using Rt = RealOf<C>;
   constexpr int a = ((E % R) * (48 / R)) % 48;
   static_assert(48 % R == 0, "radix must divide 48");
   static_assert(cos48(a) > -1.5 || a % 12 == 0, "angle not in table");
   if constexpr (a == 0) {
     return v;
   } else if constexpr (a == 24) {
-    return make_double2(-v.x, -v.y);
+    return mkc<C>(-v.x, -v.y);
   } else if constexpr (a == 12) {
     return cmul_i<DIR>(v);
   } else if constexpr (a == 36) {
     return cmul_i<-DIR>(v);
   } else {
-    constexpr double c = cos48(a);
-    constexpr double s = DIR * sin48(a);
-    return make_double2(v.x * c - v.y * s, v.x * s + v.y * c);
+    constexpr Rt c = (Rt)cos48(a);
+    constexpr Rt s = (Rt)(DIR * sin48(a));
+    return mkc<C>(v.x * c - v.y * s, v.x * s + v.y * c);
   }
 }
 
@@ -89,13 +124,15 @@ struct DFT;
 
 template <int DIR>
 struct DFT<1, DIR> {
-  __device__ __forceinline__ static void run(double2*) {}
+  template <typename C>
+  __device__ __forceinline__ static void run(C*) {}
 };
 
 template <int DIR>
 struct DFT<2, DIR> {
-  __device__ __forceinline__ static void run(double2* v) {
-    double2 a = cadd(v[0], v[1]);
+  template <typename C>
+  __device__ __forceinline__ static void run(C* v) {
+    C a = cadd(v[0], v[1]);
     v[1] = csub(v[0], v[1]);
     v[0] = a;
   }
@@ -103,10 +140,12 @@ struct DFT<2, DIR> {
 
 template <int DIR>
 struct DFT<3, DIR> {
-  __device__ __forceinline__ static void run(double2* v) {
-    double2 t = cadd(v[1], v[2]);
-    double2 d = cmul_i<DIR>(cscale(csub(v[1], v[2]), kR3H));
-    double2 m = make_double2(v[0].x - 0.5 * t.x, v[0].y - 0.5 * t.y);
+  template <typename C>
+  __device__ __forceinline__ static void run(C* v) {
+    using Rt = RealOf<C>;
+    C t = cadd(v[1], v[2]);
+    C d = cmul_i<DIR>(cscale(csub(v[1], v[2]), (Rt)kR3H));
+    C m = mkc<C>(v[0].x - (Rt)0.5 * t.x, v[0].y - (Rt)0.5 * t.y);
     v[0] = cadd(v[0], t);
     v[1] = cadd(m, d);
     v[2] = csub(m, d);
@@ -115,9 +154,10 @@ struct DFT<3, DIR> {
 
 template <int DIR>
 struct DFT<4, DIR> {
-  __device__ __forceinline__ static void run(double2* v) {
-    double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-    double2 b0 = cadd(v[1], v[3]), b1 = cmul_i<DIR>(csub(v[1], v[3]));
+  template <typename C>
+  __device__ __forceinline__ static void run(C* v) {
+    C a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    C b0 = cadd(v[1], v[3]), b1 = cmul_i<DIR>(csub(v[1], v[3]));
     v[0] = cadd(a0, b0);
     v[2] = csub(a0, b0);
     v[1] = cadd(a1, b1);
@@ -129,11 +169,12 @@ struct DFT<4, DIR> {
 template <int A, int B, int DIR>
 struct DFT_CT {
   static constexpr int R = A * B;
-  __device__ __forceinline__ static void run(double2* v) {
-    double2 y[R];
+  template <typename C>
+  __device__ __forceinline__ static void run(C* v) {
+    C y[R];
 #pragma unroll
     for (int n2 = 0; n2 < B; ++n2) {
-      double2 t[A];
+      C t[A];
 #pragma unroll
       for (int n1 = 0; n1 < A; ++n1) t[n1] = v[B * n1 + n2];
       DFT<A, DIR>::run(t);
@@ -143,7 +184,7 @@ struct DFT_CT {
     twiddle_all(y, std::make_integer_sequence<int, A * B>{});
 #pragma unroll
     for (int k1 = 0; k1 < A; ++k1) {
-      double2 t[B];
+      C t[B];
 #pragma unroll
       for (int n2 = 0; n2 < B; ++n2) t[n2] = y[n2 * A + k1];
       DFT<B, DIR>::run(t);
@@ -151,8 +192,8 @@ struct DFT_CT {
       for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = t[k2];
     }
   }
-  template <int... I>
-  __device__ __forceinline__ static void twiddle_all(double2* y, std::integer_sequence<int, I...>) {
+  template <typename C, int... I>
+  __device__ __forceinline__ static void twiddle_all(C* y, std::integer_sequence<int, I...>) {
     ((y[I] = rot<R, (I / A) * (I % A), DIR>(y[I])), ...);
   }
 };
@@ -203,15 +244,16 @@ struct Stages {
   static constexpr int U = P / R;
   static_assert(P % R == 0, "radix must divide the points per thread");
 
-  __device__ __forceinline__ static void run(double2 (&x)[P], int t, double2* sbuf,
-                                             const double2* __restrict__ tw) {
+  template <typename C>
+  __device__ __forceinline__ static void run(C (&x)[P], int t, C* sbuf,
+                                             const C* __restrict__ tw) {
     constexpr bool last = sizeof...(Rest) == 0;
     static_assert(!last || NS * R == N, "radices must multiply to N");
     if constexpr (!last) line_sync<T>();  // previous readers of sbuf are done
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int b = t + T * u;
-      double2 v[R];
+      C v[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = x[u + r * U];
       if constexpr (NS > 1) {
@@ -219,7 +261,7 @@ struct Stages {
         // lanes read consecutive entries.  For R > 4 only w, w^2, w^4, w^8 are
         // read and the other powers composed (at most 3 products deep).
         const int jm = b % NS;
-        double2 W[R];
+        C W[R];
 #pragma unroll
         for (int r = 1; r < R; ++r) {
           if (!kComposeTwiddles || R <= 4 || r == 1 || r == 2 || r == 4 || r == 8) {
@@ -231,7 +273,7 @@ struct Stages {
           }
         }
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], make_double2(W[r].x, DIR * W[r].y));
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], mkc<C>(W[r].x, DIR * W[r].y));
       }
       DFT<R, DIR>::run(v);
       if constexpr (last) {
@@ -294,8 +336,9 @@ template <int N, int T, int DIR, int PADW, typename L>
 struct RunPlan;
 template <int N, int T, int DIR, int PADW, int... Rs>
 struct RunPlan<N, T, DIR, PADW, RadixList<Rs...>> {
-  __device__ __forceinline__ static void run(double2 (&x)[N / T], int t, double2* sbuf,
-                                             const double2* __restrict__ tw) {
+  template <typename C>
+  __device__ __forceinline__ static void run(C (&x)[N / T], int t, C* sbuf,
+                                             const C* __restrict__ tw) {
     Stages<N, T, DIR, PADW, 1, Rs...>::run(x, t, sbuf, tw);
   }
 };
@@ -315,19 +358,21 @@ struct StageTw;
 template <int N, int NS>
 struct StageTw<N, NS, RadixList<>> {
   static constexpr int len = 0;
-  __device__ __forceinline__ static void fill(double2*, const double2* __restrict__) {}
+  template <typename C>
+  __device__ __forceinline__ static void fill(C*, const double2* __restrict__) {}
 };
 template <int N, int NS, int R, int... Rest>
 struct StageTw<N, NS, RadixList<R, Rest...>> {
   static constexpr int own = NS > 1 ? (R - 1) * NS : 0;
   using Next = StageTw<N, NS * R, RadixList<Rest...>>;
   static constexpr int len = own + Next::len;
-  __device__ __forceinline__ static void fill(double2* tws, const double2* __restrict__ tw_g) {
+  template <typename C>
+  __device__ __forceinline__ static void fill(C* tws, const double2* __restrict__ tw_g) {
     if constexpr (NS > 1) {
       constexpr int step = N / (NS * R);
       for (int e = threadIdx.x; e < own; e += blockDim.x) {
         const int r = e / NS + 1, jm = e - (r - 1) * NS;
-        tws[e] = tw_g[jm * r * step];
+        tws[e] = cvt<C>(tw_g[jm * r * step]);  // FP64 table, rounded for FP32 lines
       }
     }
     Next::fill(tws + own, tw_g);
@@ -344,13 +389,14 @@ struct LineFFT {
   static constexpr int TWLEN = StageTw<N, 1, L>::len > 0 ? StageTw<N, 1, L>::len : 1;
   // fills the per-stage table from the global table tw_g[e] = exp(2 pi i e / N);
   // ends with a CTA barrier
-  __device__ __forceinline__ static void load_tw(double2* tws, const double2* __restrict__ tw_g) {
+  template <typename C>
+  __device__ __forceinline__ static void load_tw(C* tws, const double2* __restrict__ tw_g) {
     StageTw<N, 1, L>::fill(tws, tw_g);
     __syncthreads();
   }
-  template <int DIR>
-  __device__ __forceinline__ static void run(double2 (&x)[P], int t, double2* sbuf,
-                                             const double2* __restrict__ tw) {
+  template <int DIR, typename C>
+  __device__ __forceinline__ static void run(C (&x)[P], int t, C* sbuf,
+                                             const C* __restrict__ tw) {
     RunPlan<N, T, DIR, PADW, L>::run(x, t, sbuf, tw);
   }
 };

@@ -4,8 +4,10 @@
 
 namespace ns3d {
 
-cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs& a, const PassGeom& g,
-                      cudaStream_t st) {
+namespace {
+template <typename C>
+cudaError_t fwd_x_mode(int mode, bool combine, const FwdXArgs<C>& a, const PassGeom& g,
+                       cudaStream_t st) {
   switch (mode) {
     case kExplicit:
       return combine ? launch_fwd_x<kExplicit, true>(a, g, st)
@@ -21,14 +23,30 @@ cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs& a, const PassGeom&
   }
 }
 
-cudaError_t prepare_fwdx(const PassGeom& g) {
-  const FwdXArgs a{};
+template <typename C>
+cudaError_t prepare_fwdx_prec(const PassGeom& g) {
+  const FwdXArgs<C> a{};
   cudaError_t e;
   if ((e = launch_fwd_x<kExplicit, false>(a, g, nullptr, true)) != cudaSuccess) return e;
   if ((e = launch_fwd_x<kExplicit, true>(a, g, nullptr, true)) != cudaSuccess) return e;
   if ((e = launch_fwd_x<kRhs, false>(a, g, nullptr, true)) != cudaSuccess) return e;
   if ((e = launch_fwd_x<kImplicit, false>(a, g, nullptr, true)) != cudaSuccess) return e;
   return launch_fwd_x<kConvOut, false>(a, g, nullptr, true);
+}
+}  // namespace
+
+cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs<>& a, const PassGeom& g,
+                      cudaStream_t st) {
+  return fwd_x_mode(mode, combine, a, g, st);
+}
+cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs<float2>& a, const PassGeom& g,
+                      cudaStream_t st) {
+  return fwd_x_mode(mode, combine, a, g, st);
+}
+
+cudaError_t prepare_fwdx(const PassGeom& g) {
+  const cudaError_t e = prepare_fwdx_prec<double2>(g);
+  return e != cudaSuccess ? e : prepare_fwdx_prec<float2>(g);
 }
 
 }  // namespace ns3d

@@ -18,17 +18,40 @@ cudaError_t run_inv_y(const InvYArgs<3>& a, const PassGeom& g, cudaStream_t st) 
 cudaError_t run_inv_y(const InvYArgs<6>& a, const PassGeom& g, cudaStream_t st) {
   return launch_inv_y<6>(a, g, st);
 }
-cudaError_t run_fwd_y(const FwdYArgs& a, const PassGeom& g, cudaStream_t st) {
+cudaError_t run_fwd_y(const FwdYArgs<>& a, const PassGeom& g, cudaStream_t st) {
+  return launch_fwd_y(a, g, st);
+}
+cudaError_t run_inv_x(const InvXArgs<3, float2>& a, const PassGeom& g, cudaStream_t st) {
+  return launch_inv_x<3>(a, g, st);
+}
+cudaError_t run_inv_x(const InvXArgs<6, float2>& a, const PassGeom& g, cudaStream_t st) {
+  return launch_inv_x<6>(a, g, st);
+}
+cudaError_t run_inv_y(const InvYArgs<3, float2>& a, const PassGeom& g, cudaStream_t st) {
+  return launch_inv_y<3>(a, g, st);
+}
+cudaError_t run_inv_y(const InvYArgs<6, float2>& a, const PassGeom& g, cudaStream_t st) {
+  return launch_inv_y<6>(a, g, st);
+}
+cudaError_t run_fwd_y(const FwdYArgs<float2>& a, const PassGeom& g, cudaStream_t st) {
   return launch_fwd_y(a, g, st);
 }
 
-cudaError_t prepare_xy(const PassGeom& g) {
+namespace {
+template <typename C>
+cudaError_t prepare_xy_prec(const PassGeom& g) {
   cudaError_t e;
-  if ((e = launch_inv_x<3>(InvXArgs<3>{}, g, nullptr, true)) != cudaSuccess) return e;
-  if ((e = launch_inv_x<6>(InvXArgs<6>{}, g, nullptr, true)) != cudaSuccess) return e;
-  if ((e = launch_inv_y<3>(InvYArgs<3>{}, g, nullptr, true)) != cudaSuccess) return e;
-  if ((e = launch_inv_y<6>(InvYArgs<6>{}, g, nullptr, true)) != cudaSuccess) return e;
-  return launch_fwd_y(FwdYArgs{}, g, nullptr, true);
+  if ((e = launch_inv_x<3>(InvXArgs<3, C>{}, g, nullptr, true)) != cudaSuccess) return e;
+  if ((e = launch_inv_x<6>(InvXArgs<6, C>{}, g, nullptr, true)) != cudaSuccess) return e;
+  if ((e = launch_inv_y<3>(InvYArgs<3, C>{}, g, nullptr, true)) != cudaSuccess) return e;
+  if ((e = launch_inv_y<6>(InvYArgs<6, C>{}, g, nullptr, true)) != cudaSuccess) return e;
+  return launch_fwd_y(FwdYArgs<C>{}, g, nullptr, true);
+}
+}  // namespace
+
+cudaError_t prepare_xy(const PassGeom& g) {
+  const cudaError_t e = prepare_xy_prec<double2>(g);
+  return e != cudaSuccess ? e : prepare_xy_prec<float2>(g);
 }
 
 }  // namespace ns3d

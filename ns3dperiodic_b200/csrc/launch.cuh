@@ -86,19 +86,23 @@ inline unsigned persistent_grid(Kern kern, size_t smem, long long groups) {
   return (unsigned)(groups < cap ? (groups > 0 ? groups : 1) : cap);
 }
 
-template <int NF>
-cudaError_t launch_inv_x(const InvXArgs<NF>& a, const PassGeom& g, cudaStream_t st,
+// KTag's last argument separates the FP64 and FP32 instantiations.
+template <typename C>
+constexpr int prec_tag() { return sizeof(C) == 16 ? 0 : 100; }
+
+template <int NF, typename C>
+cudaError_t launch_inv_x(const InvXArgs<NF, C>& a, const PassGeom& g, cudaStream_t st,
                          bool prepare_only = false) {
   const long long lines = (long long)g.Ny * g.Mz * nbatch(g);
   switch (g.Nx) {
 #define NS3D_CASE(N)                                                                    \
   case N: {                                                                             \
     constexpr int P = p_xy(N);                                                          \
-    using S = PassSmem<N, P>;                                                           \
-    const unsigned grid = persistent_grid<KTag<0, N, P, NF>>(                           \
-        inv_x_kernel<N, P, NF>, S::BYTES, (lines + S::LPC - 1) / S::LPC);                \
+    using S = PassSmem<N, P, C, double2>;                                               \
+    const unsigned grid = persistent_grid<KTag<0, N, P, NF + prec_tag<C>()>>(           \
+        inv_x_kernel<N, P, NF, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);             \
     if (prepare_only) return cudaGetLastError();                                        \
-    inv_x_kernel<N, P, NF><<<grid, kThreads, S::BYTES, st>>>(a, g);                      \
+    inv_x_kernel<N, P, NF, C><<<grid, kThreads, S::BYTES, st>>>(a, g);                   \
     return cudaGetLastError();                                                          \
   }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
@@ -108,8 +112,8 @@ cudaError_t launch_inv_x(const InvXArgs<NF>& a, const PassGeom& g, cudaStream_t 
   }
 }
 
-template <int NF>
-cudaError_t launch_inv_y(const InvYArgs<NF>& a, const PassGeom& gi, cudaStream_t st,
+template <int NF, typename C>
+cudaError_t launch_inv_y(const InvYArgs<NF, C>& a, const PassGeom& gi, cudaStream_t st,
                          bool prepare_only = false) {
   const PassGeom g = planes_geom(gi);
   const long long lines = (long long)g.Nx * g.Mz;
@@ -117,11 +121,11 @@ cudaError_t launch_inv_y(const InvYArgs<NF>& a, const PassGeom& gi, cudaStream_t
 #define NS3D_CASE(N)                                                                    \
   case N: {                                                                             \
     constexpr int P = p_xy(N);                                                          \
-    using S = PassSmem<N, P>;                                                           \
-    const unsigned grid = persistent_grid<KTag<1, N, P, NF>>(                           \
-        inv_y_kernel<N, P, NF>, S::BYTES, (lines + S::LPC - 1) / S::LPC);                \
+    using S = PassSmem<N, P, C, C>;                                                     \
+    const unsigned grid = persistent_grid<KTag<1, N, P, NF + prec_tag<C>()>>(           \
+        inv_y_kernel<N, P, NF, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);             \
     if (prepare_only) return cudaGetLastError();                                        \
-    inv_y_kernel<N, P, NF><<<grid, kThreads, S::BYTES, st>>>(a, g);                      \
+    inv_y_kernel<N, P, NF, C><<<grid, kThreads, S::BYTES, st>>>(a, g);                   \
     return cudaGetLastError();                                                          \
   }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
@@ -131,15 +135,15 @@ cudaError_t launch_inv_y(const InvYArgs<NF>& a, const PassGeom& gi, cudaStream_t
   }
 }
 
-template <bool UV>
-cudaError_t launch_z(const ZArgs<UV ? 6 : 3>& a, const PassGeom& gi, cudaStream_t st) {
+template <bool UV, typename C>
+cudaError_t launch_z(const ZArgs<UV ? 6 : 3, C>& a, const PassGeom& gi, cudaStream_t st) {
   const PassGeom g = planes_geom(gi);
   const long long lines = (long long)g.Nx * g.Ny;
   switch (g.Nz) {
 #define NS3D_CASE(N)                                                               \
   case N: {                                                                        \
     constexpr int P = UV ? p_zuv(N) : p_z(N);                                      \
-    z_kernel<N, P, UV><<<blocks_for(lines, lines_per_cta_z<N, P>()),              \
+    z_kernel<N, P, UV, C><<<blocks_for(lines, lines_per_cta_z<N, P>()),           \
                          kWarpsPerCta * 32, 0, st>>>(a, g);                        \
     return cudaGetLastError();                                                     \
   }
@@ -150,19 +154,20 @@ cudaError_t launch_z(const ZArgs<UV ? 6 : 3>& a, const PassGeom& gi, cudaStream_
   }
 }
 
-template <int MODE, bool COMBINE>
-cudaError_t launch_fwd_x(const FwdXArgs& a, const PassGeom& g, cudaStream_t st,
+template <int MODE, bool COMBINE, typename C>
+cudaError_t launch_fwd_x(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t st,
                          bool prepare_only = false) {
   const long long lines = (long long)g.Ny * g.Mz * nbatch(g);
   switch (g.Nx) {
 #define NS3D_CASE(N)                                                                    \
   case N: {                                                                             \
     constexpr int P = p_fx(N);                                                          \
-    using S = PassSmem<N, P>;                                                           \
-    const unsigned grid = persistent_grid<KTag<2 + 2 * MODE + (COMBINE ? 1 : 0), N, P, 0>>( \
-        fwd_x_kernel<N, P, MODE, COMBINE>, S::BYTES, (lines + S::LPC - 1) / S::LPC);     \
+    using S = PassSmem<N, P, C, C>;                                                     \
+    const unsigned grid =                                                               \
+        persistent_grid<KTag<2 + 2 * MODE + (COMBINE ? 1 : 0), N, P, prec_tag<C>()>>(   \
+            fwd_x_kernel<N, P, MODE, COMBINE, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC); \
     if (prepare_only) return cudaGetLastError();                                        \
-    fwd_x_kernel<N, P, MODE, COMBINE><<<grid, kThreads, S::BYTES, st>>>(a, g);           \
+    fwd_x_kernel<N, P, MODE, COMBINE, C><<<grid, kThreads, S::BYTES, st>>>(a, g);        \
     return cudaGetLastError();                                                          \
   }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
@@ -172,19 +177,20 @@ cudaError_t launch_fwd_x(const FwdXArgs& a, const PassGeom& g, cudaStream_t st,
   }
 }
 
-inline cudaError_t launch_fwd_y(const FwdYArgs& a, const PassGeom& gi, cudaStream_t st,
-                                bool prepare_only = false) {
+template <typename C>
+cudaError_t launch_fwd_y(const FwdYArgs<C>& a, const PassGeom& gi, cudaStream_t st,
+                         bool prepare_only = false) {
   const PassGeom g = planes_geom(gi);
   const long long lines = (long long)g.Nx * g.Mz;
   switch (g.Ny) {
 #define NS3D_CASE(N)                                                                    \
   case N: {                                                                             \
     constexpr int P = p_xy(N);                                                          \
-    using S = PassSmem<N, P>;                                                           \
-    const unsigned grid = persistent_grid<KTag<20, N, P, 0>>(                           \
-        fwd_y_kernel<N, P>, S::BYTES, (lines + S::LPC - 1) / S::LPC);                    \
+    using S = PassSmem<N, P, C, C>;                                                     \
+    const unsigned grid = persistent_grid<KTag<20, N, P, prec_tag<C>()>>(               \
+        fwd_y_kernel<N, P, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);                 \
     if (prepare_only) return cudaGetLastError();                                        \
-    fwd_y_kernel<N, P><<<grid, kThreads, S::BYTES, st>>>(a, g);                          \
+    fwd_y_kernel<N, P, C><<<grid, kThreads, S::BYTES, st>>>(a, g);                       \
     return cudaGetLastError();                                                          \
   }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)

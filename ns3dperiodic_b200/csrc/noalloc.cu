@@ -136,8 +136,8 @@ extern "C" ns3d_status ns3d_convolution_noalloc(int Nx, int Ny, int Nz, double L
   ns3d::InvXArgs<3> ax{};
   ns3d::InvYArgs<3> ay{};
   ns3d::ZArgs<3> az{};
-  ns3d::FwdYArgs fy{};
-  ns3d::FwdXArgs fx{};
+  ns3d::FwdYArgs<> fy{};
+  ns3d::FwdXArgs<> fx{};
   for (int i = 0; i < 3; ++i) {
     ax.in[i] = u[i]; ax.A[i] = A[i]; ax.B[i] = B[i];
     ay.A[i] = A[i]; ay.B[i] = B[i]; ay.C[i] = C[i]; ay.D[i] = D[i]; ay.E[i] = E[i];

@@ -100,6 +100,22 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pr
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n)
                : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred = true) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n)
+               : "memory");
+}
+// one complex element: 16 bytes (FP64) or 8 bytes (FP32)
+template <typename E>
+__device__ __forceinline__ void cp_async_elem(E* smem, const E* gmem, bool pred) {
+  static_assert(sizeof(E) == 16 || sizeof(E) == 8, "complex element");
+  if constexpr (sizeof(E) == 16) {
+    cp_async16(smem, gmem, pred);
+  } else {
+    cp_async8(smem, gmem, pred);
+  }
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
@@ -111,13 +127,14 @@ __device__ __forceinline__ void cp_async_wait() {
 // Copies the P samples t + T*s (s < P) of one line into a private slot:
 // slot[s*kThreads] <- src[base + (t + T*s) * stride], skipping (zero-filling)
 // the samples whose bit in `keep` is clear.
-template <int P, int T>
-__device__ __forceinline__ void issue_line(double2* slot, const double2* __restrict__ src,
+template <int P, int T, typename E>
+__device__ __forceinline__ void issue_line(E* slot, const E* __restrict__ src,
                                            size_t base, size_t stride, int t,
                                            uint32_t keep = 0xffffffffu) {
 #pragma unroll
   for (int s = 0; s < P; ++s)
-    cp_async16(slot + s * kThreads, src + base + (size_t)(t + T * s) * stride, (keep >> s) & 1u);
+    cp_async_elem(slot + s * kThreads, src + base + (size_t)(t + T * s) * stride,
+                  (keep >> s) & 1u);
 }
 
 // Smallest line-buffer stride >= len whose residue mod 8 (16-byte slots; one
@@ -154,19 +171,28 @@ __device__ __forceinline__ GroupRange group_range(int groups) {
   return {(int)blockIdx.x, groups, (int)gridDim.x};
 }
 
-// Dynamic shared memory of a pipelined pass, in double2 words.
-template <int N, int P>
+constexpr size_t align16(size_t b) { return (b + 15) / 16 * 16; }
+
+// Dynamic shared memory of a pipelined pass: the stage twiddles and the line
+// buffers in the line precision C, then each thread's double buffer of
+// prefetched elements of type E (the pass's input, FP64 state or scratch).
+template <int N, int P, typename C = double2, typename E = C>
 struct PassSmem {
   using F = LineFFT<N, P>;
   using LM = LaneMap<F::T>;
   static constexpr int LPC = LM::LPC;
   static constexpr int STRIDE = line_stride(F::BUF, xy_stride_target<F::T>());
-  static constexpr int TW = 0;
-  static constexpr int SBUF = F::TWLEN;
-  static constexpr int PF = SBUF + LPC * STRIDE;
-  static constexpr int WORDS = PF + 2 * P * kThreads;
-  static constexpr size_t BYTES = (size_t)WORDS * sizeof(double2);
+  static constexpr size_t SBUF_OFF = align16((size_t)F::TWLEN * sizeof(C));
+  static constexpr size_t PF_OFF = align16(SBUF_OFF + (size_t)LPC * STRIDE * sizeof(C));
+  static constexpr size_t BYTES = PF_OFF + (size_t)2 * P * kThreads * sizeof(E);
   static_assert(BYTES <= 227 * 1024, "shared memory per CTA");
+  __device__ __forceinline__ static C* tw(unsigned char* base) { return (C*)base; }
+  __device__ __forceinline__ static C* sbuf(unsigned char* base, int li) {
+    return (C*)(base + SBUF_OFF) + li * STRIDE;
+  }
+  __device__ __forceinline__ static E* pf(unsigned char* base) {
+    return (E*)(base + PF_OFF) + threadIdx.x;
+  }
 };
 
 template <int NX>
@@ -184,28 +210,29 @@ __device__ __forceinline__ uint32_t mask_bits(const uint16_t* __restrict__ qcut,
 // ---------------------------------------------------------------------------
 // inv_x: lines along x, batch L = y*Mz + z (contiguous), NF = 3 or 6 fields
 // ---------------------------------------------------------------------------
-template <int NF>
+template <int NF, typename C = double2>
 struct InvXArgs {
-  const double2* in[NF];
-  double2* A[NF];
-  double2* B[NF];
+  const double2* in[NF];  // the FP64 state
+  C* A[NF];
+  C* B[NF];
   const uint16_t* qcut;  // [Nx][Ny]: mask(j,k,l) = l < qcut[j*Ny+k], minus (0,0,0)
   const double2* tw;
 };
 
-template <int NX, int P, int NF>
-__global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF> a, PassGeom g) {
-  using S = PassSmem<NX, P>;
+template <int NX, int P, int NF, typename C>
+__global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF, C> a, PassGeom g) {
+  using S = PassSmem<NX, P, C, double2>;
   using F = typename S::F;
   using LM = typename S::LM;
+  using Rt = RealOf<C>;
   constexpr int T = F::T;
-  extern __shared__ double2 dsm[];
-  F::load_tw(dsm + S::TW, a.tw);
-  const double2* tw_s = dsm + S::TW;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  F::load_tw(S::tw(dsm), a.tw);
+  const C* tw_s = S::tw(dsm);
   int li, t;
   LM::get(li, t);
-  double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
-  double2* pf = dsm + S::PF + threadIdx.x;
+  C* sbuf = S::sbuf(dsm, li);
+  double2* pf = S::pf(dsm);
   const int nlines = g.Ny * g.Mz;               // lines of one instance
   const int tlines = nlines * nbatch(g);        // lines of all instances
   const int groups = (tlines + LM::LPC - 1) / LM::LPC;
@@ -259,9 +286,9 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF
       cp_async_commit();
       cp_async_wait<1>();
       // X (masked) then i kx X, both from the prefetched samples
-      double2 v[P];
+      C v[P];
 #pragma unroll
-      for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
+      for (int s = 0; s < P; ++s) v[s] = cvt<C>(cur[s * kThreads]);
       F::template run<+1>(v, t, sbuf, tw_s);
       if (valid) {
 #pragma unroll
@@ -269,9 +296,9 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF
       }
 #pragma unroll
       for (int s = 0; s < P; ++s) {
-        const double2 u = cur[s * kThreads];
-        const double kx = g.kfx * (double)signed_idx(t + T * s, NX);
-        v[s] = make_double2(-u.y * kx, u.x * kx);  // i kx u (build_ders_device)
+        const C u = cvt<C>(cur[s * kThreads]);
+        const Rt kx = (Rt)(g.kfx * (double)signed_idx(t + T * s, NX));
+        v[s] = mkc<C>(-u.y * kx, u.x * kx);  // i kx u (build_ders_device)
       }
       F::template run<+1>(v, t, sbuf, tw_s);
       if (valid) {
@@ -288,29 +315,30 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF
 // ---------------------------------------------------------------------------
 // inv_y: lines along y, batch b = x*Mz + z, base = x*Ny*Mz + z, stride Mz
 // ---------------------------------------------------------------------------
-template <int NF>
+template <int NF, typename Cx = double2>
 struct InvYArgs {
-  const double2* A[NF];
-  const double2* B[NF];
-  double2* C[NF];
-  double2* D[NF];
-  double2* E[NF];
+  const Cx* A[NF];
+  const Cx* B[NF];
+  Cx* C[NF];
+  Cx* D[NF];
+  Cx* E[NF];
   const double2* tw;
 };
 
-template <int NY, int P, int NF>
-__global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF> a, PassGeom g) {
-  using S = PassSmem<NY, P>;
+template <int NY, int P, int NF, typename C>
+__global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF, C> a, PassGeom g) {
+  using S = PassSmem<NY, P, C, C>;
   using F = typename S::F;
   using LM = typename S::LM;
+  using Rt = RealOf<C>;
   constexpr int T = F::T;
-  extern __shared__ double2 dsm[];
-  F::load_tw(dsm + S::TW, a.tw);
-  const double2* tw_s = dsm + S::TW;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  F::load_tw(S::tw(dsm), a.tw);
+  const C* tw_s = S::tw(dsm);
   int li, t;
   LM::get(li, t);
-  double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
-  double2* pf = dsm + S::PF + threadIdx.x;
+  C* sbuf = S::sbuf(dsm, li);
+  C* pf = S::pf(dsm);
   const int nb = g.Nx * g.Mz;
   const int groups = (nb + LM::LPC - 1) / LM::LPC;
   const size_t stride = (size_t)g.Mz;
@@ -336,12 +364,12 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF
     for (int f = 0; f < NF; ++f) {
       // unit A[f] -> C[f] = IFFT_y A, D[f] = IFFT_y(i ky A)
       {
-        const double2* cur = pf + ub * (P * kThreads);
-        double2* nxt = pf + (ub ^ 1) * (P * kThreads);
+        const C* cur = pf + ub * (P * kThreads);
+        C* nxt = pf + (ub ^ 1) * (P * kThreads);
         issue_line<P, T>(nxt, a.B[f], base, stride, t);
         cp_async_commit();
         cp_async_wait<1>();
-        double2 v[P];
+        C v[P];
 #pragma unroll
         for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
         F::template run<+1>(v, t, sbuf, tw_s);
@@ -351,9 +379,9 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF
         }
 #pragma unroll
         for (int s = 0; s < P; ++s) {
-          const double2 u = cur[s * kThreads];
-          const double ky = g.kfy * (double)signed_idx(t + T * s, NY);
-          v[s] = make_double2(-u.y * ky, u.x * ky);
+          const C u = cur[s * kThreads];
+          const Rt ky = (Rt)(g.kfy * (double)signed_idx(t + T * s, NY));
+          v[s] = mkc<C>(-u.y * ky, u.x * ky);
         }
         F::template run<+1>(v, t, sbuf, tw_s);
         if (valid) {
@@ -364,8 +392,8 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF
       }
       // unit B[f] -> E[f] = IFFT_y B
       {
-        const double2* cur = pf + ub * (P * kThreads);
-        double2* nxt = pf + (ub ^ 1) * (P * kThreads);
+        const C* cur = pf + ub * (P * kThreads);
+        C* nxt = pf + (ub ^ 1) * (P * kThreads);
         if (f + 1 < NF) {
           issue_line<P, T>(nxt, a.A[f + 1], base, stride, t);
         } else if (gn < g_end) {
@@ -373,7 +401,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF
         }
         cp_async_commit();
         cp_async_wait<1>();
-        double2 v[P];
+        C v[P];
 #pragma unroll
         for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
         F::template run<+1>(v, t, sbuf, tw_s);
@@ -391,54 +419,56 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF
 // ---------------------------------------------------------------------------
 // z pass: lines along z (contiguous), batch b = x*Ny + y, base = b*Mz
 // ---------------------------------------------------------------------------
-template <int NF>
+template <int NF, typename Cx = double2>
 struct ZArgs {
   // per velocity field (u, then v for the tangent form) and component:
-  const double2* C[NF];  // IFFT_xy(M u_i)
-  const double2* D[NF];  // IFFT_xy(i ky M u_i)
-  const double2* E[NF];  // IFFT_xy(i kx M u_i)
-  double2* Qh[3];        // R2C_z of the products (x, y still physical)
+  const Cx* C[NF];  // IFFT_xy(M u_i)
+  const Cx* D[NF];  // IFFT_xy(i ky M u_i)
+  const Cx* E[NF];  // IFFT_xy(i kx M u_i)
+  Cx* Qh[3];        // R2C_z of the products (x, y still physical)
   const double2* tw;
 };
 
 // Load W[k] = H(X1)[k] + i H(X2)[k] for positions k = t + T s, where H is the
 // Hermitian extension of a z half-line (H[0], H[N/2] keep only real parts),
 // X = line (optionally times i kz).
-template <int NZ, int P, bool IK1, bool IK2>
-__device__ __forceinline__ void load_pair(double2 (&w)[P], const double2* __restrict__ f1,
-                                          const double2* __restrict__ f2, size_t base, int t,
-                                          double kfz) {
+template <int NZ, int P, bool IK1, bool IK2, typename C>
+__device__ __forceinline__ void load_pair(C (&w)[P], const C* __restrict__ f1,
+                                          const C* __restrict__ f2, size_t base, int t,
+                                          RealOf<C> kfz) {
+  using Rt = RealOf<C>;
   constexpr int T = NZ / P;
 #pragma unroll
   for (int s = 0; s < P; ++s) {
     const int k = t + T * s;
     const bool upper = k > NZ / 2;
     const int q = upper ? NZ - k : k;
-    double2 c1 = __ldg(f1 + base + q);
-    double2 c2 = __ldg(f2 + base + q);
-    const double kz = kfz * (double)q;
-    if constexpr (IK1) c1 = make_double2(-c1.y * kz, c1.x * kz);
-    if constexpr (IK2) c2 = make_double2(-c2.y * kz, c2.x * kz);
+    C c1 = __ldg(f1 + base + q);
+    C c2 = __ldg(f2 + base + q);
+    const Rt kz = kfz * (Rt)q;
+    if constexpr (IK1) c1 = mkc<C>(-c1.y * kz, c1.x * kz);
+    if constexpr (IK2) c2 = mkc<C>(-c2.y * kz, c2.x * kz);
     if (k == 0 || k == NZ / 2) {
-      c1.y = 0.0;
-      c2.y = 0.0;
+      c1.y = (Rt)0;
+      c2.y = (Rt)0;
     }
     if (upper) {
       c1.y = -c1.y;
       c2.y = -c2.y;
     }
-    w[s] = make_double2(c1.x - c2.y, c1.y + c2.x);
+    w[s] = mkc<C>(c1.x - c2.y, c1.y + c2.x);
   }
 }
 
 // w holds FFT_z(Q1 + i Q2) at k = t + T s.  Split it with the mirror bin
 // W[N-k] (exchanged through shared memory) and store the half spectra
 // Q1h[k], Q2h[k] for k = 0..N/2.
-template <int NZ, int P>
-__device__ __forceinline__ void store_pair_spectrum(const double2 (&w)[P], double2* sbuf, int t,
-                                                    double2* __restrict__ o1,
-                                                    double2* __restrict__ o2, size_t base,
+template <int NZ, int P, typename C>
+__device__ __forceinline__ void store_pair_spectrum(const C (&w)[P], C* sbuf, int t,
+                                                    C* __restrict__ o1,
+                                                    C* __restrict__ o2, size_t base,
                                                     bool valid) {
+  using Rt = RealOf<C>;
   using F = LineFFT<NZ, P>;
   constexpr int T = F::T;
   line_sync<T>();
@@ -449,10 +479,10 @@ __device__ __forceinline__ void store_pair_spectrum(const double2 (&w)[P], doubl
   for (int s = 0; s < P; ++s) {
     const int k = t + T * s;
     if (k <= NZ / 2 && valid) {
-      const double2 a = w[s];
-      const double2 m = sbuf[spad<F::PADW>(k == 0 ? 0 : NZ - k)];
-      o1[base + k] = make_double2(0.5 * (a.x + m.x), 0.5 * (a.y - m.y));
-      o2[base + k] = make_double2(0.5 * (a.y + m.y), -0.5 * (a.x - m.x));
+      const C a = w[s];
+      const C m = sbuf[spad<F::PADW>(k == 0 ? 0 : NZ - k)];
+      o1[base + k] = mkc<C>((Rt)0.5 * (a.x + m.x), (Rt)0.5 * (a.y - m.y));
+      o2[base + k] = mkc<C>((Rt)0.5 * (a.y + m.y), (Rt)-0.5 * (a.x - m.x));
     }
   }
 }
@@ -475,15 +505,15 @@ struct ZLaneMap {  // lanes of one line are adjacent: the line is contiguous in 
 
 // One component of B(u,v)_i = (v.grad) u_i + (u.grad) v_i in the z pass
 // (convolute_2p3_UV, Source/advection_2_3.cu:414-466); 3 paired C2R lines.
-template <int NZ, int P>
-__device__ __forceinline__ void uv_component(double (&q)[P], int i, const ZArgs<6>& a, size_t base,
-                                             int t, double kfz, double sc, double2* sbuf,
-                                             const double2* tw_s, const double (&ux)[P],
-                                             const double (&uy)[P], const double (&uz)[P],
-                                             const double (&vx)[P], const double (&vy)[P],
-                                             const double (&vz)[P]) {
+template <int NZ, int P, typename C, typename Rt = RealOf<C>>
+__device__ __forceinline__ void uv_component(Rt (&q)[P], int i, const ZArgs<6, C>& a, size_t base,
+                                             int t, Rt kfz, Rt sc, C* sbuf,
+                                             const C* tw_s, const Rt (&ux)[P],
+                                             const Rt (&uy)[P], const Rt (&uz)[P],
+                                             const Rt (&vx)[P], const Rt (&vy)[P],
+                                             const Rt (&vz)[P]) {
   using F = LineFFT<NZ, P>;
-  double2 w[P];
+  C w[P];
   // (d_x u_i, d_y u_i)
   load_pair<NZ, P, false, false>(w, a.E[i], a.D[i], base, t, kfz);
   F::template run<+1>(w, t, sbuf, tw_s);
@@ -504,13 +534,14 @@ __device__ __forceinline__ void uv_component(double (&q)[P], int i, const ZArgs<
   for (int s = 0; s < P; ++s) q[s] = q[s] + (uy[s] * (w[s].x * sc) + uz[s] * (w[s].y * sc));
 }
 
-template <int NZ, int P, bool UV>
-__global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<UV ? 6 : 3> a, PassGeom g) {
+template <int NZ, int P, bool UV, typename C>
+__global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<UV ? 6 : 3, C> a, PassGeom g) {
   using F = LineFFT<NZ, P>;
+  using Rt = RealOf<C>;
   constexpr int T = F::T;
   using LM = ZLaneMap<T>;
-  __shared__ double2 tw_s[F::TWLEN];
-  __shared__ double2 sbuf_all[LM::LPC][F::BUF];
+  __shared__ C tw_s[F::TWLEN];
+  __shared__ C sbuf_all[LM::LPC][F::BUF];
   F::load_tw(tw_s, a.tw);
   int li, t;
   LM::get(li, t);
@@ -518,11 +549,11 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
   const int b = blockIdx.x * LM::LPC + li;
   const bool valid = b < nb;
   const size_t base = (size_t)(valid ? b : 0) * g.Mz;
-  double2* sbuf = sbuf_all[li];
-  const double sc = g.inv_vol;
-  const double kfz = g.kfz;
-  double2 w[P];
-  double ux[P], uy[P], uz[P], q0[P], q1[P], q2[P];
+  C* sbuf = sbuf_all[li];
+  const Rt sc = (Rt)g.inv_vol;
+  const Rt kfz = (Rt)g.kfz;
+  C w[P];
+  Rt ux[P], uy[P], uz[P], q0[P], q1[P], q2[P];
   if constexpr (!UV) {
     // Q_z first, so at most five real lines (u_x, u_y, u_z and two products)
     // are live at any time.
@@ -544,7 +575,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
       q2[s] = ux[s] * (w[s].x * sc) + uy[s] * (w[s].y * sc) + uz[s] * q2[s];
     // R2C of Q_z alone
 #pragma unroll
-    for (int s = 0; s < P; ++s) w[s] = make_double2(q2[s], 0.0);
+    for (int s = 0; s < P; ++s) w[s] = mkc<C>(q2[s], (Rt)0);
     F::template run<-1>(w, t, sbuf, tw_s);
     if (valid) {
 #pragma unroll
@@ -570,13 +601,13 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
       q1[s] = ux[s] * (w[s].x * sc) + uy[s] * (w[s].y * sc) + uz[s] * q1[s];
     // R2C of (Q_x, Q_y) packed
 #pragma unroll
-    for (int s = 0; s < P; ++s) w[s] = make_double2(q0[s], q1[s]);
+    for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], q1[s]);
     F::template run<-1>(w, t, sbuf, tw_s);
     store_pair_spectrum<NZ, P>(w, sbuf, t, a.Qh[0], a.Qh[1], base, valid);
     return;
   } else {
     // B(u,v)_i = (v.grad) u_i + (u.grad) v_i; fields 0..2 are u, 3..5 are v
-    double vx[P], vy[P], vz[P];
+    Rt vx[P], vy[P], vz[P];
     load_pair<NZ, P, false, false>(w, a.C[0], a.C[1], base, t, kfz);
     F::template run<+1>(w, t, sbuf, tw_s);
 #pragma unroll
@@ -595,11 +626,11 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
   }
   // forward R2C along z: (Q0, Q1) packed, then Q2 alone
 #pragma unroll
-  for (int s = 0; s < P; ++s) w[s] = make_double2(q0[s], q1[s]);
+  for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], q1[s]);
   F::template run<-1>(w, t, sbuf, tw_s);
   store_pair_spectrum<NZ, P>(w, sbuf, t, a.Qh[0], a.Qh[1], base, valid);
 #pragma unroll
-  for (int s = 0; s < P; ++s) w[s] = make_double2(q2[s], 0.0);
+  for (int s = 0; s < P; ++s) w[s] = mkc<C>(q2[s], (Rt)0);
   F::template run<-1>(w, t, sbuf, tw_s);
   if (valid) {
 #pragma unroll
@@ -613,24 +644,25 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
 // ---------------------------------------------------------------------------
 // fwd_y: in-place forward transform along y of the 3 product spectra
 // ---------------------------------------------------------------------------
+template <typename Cx = double2>
 struct FwdYArgs {
-  double2* Q[3];
+  Cx* Q[3];
   const double2* tw;
 };
 
-template <int NY, int P>
-__global__ void __launch_bounds__(kThreads, kMinCtasXY) fwd_y_kernel(FwdYArgs a, PassGeom g) {
-  using S = PassSmem<NY, P>;
+template <int NY, int P, typename C>
+__global__ void __launch_bounds__(kThreads, kMinCtasXY) fwd_y_kernel(FwdYArgs<C> a, PassGeom g) {
+  using S = PassSmem<NY, P, C, C>;
   using F = typename S::F;
   using LM = typename S::LM;
   constexpr int T = F::T;
-  extern __shared__ double2 dsm[];
-  F::load_tw(dsm + S::TW, a.tw);
-  const double2* tw_s = dsm + S::TW;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  F::load_tw(S::tw(dsm), a.tw);
+  const C* tw_s = S::tw(dsm);
   int li, t;
   LM::get(li, t);
-  double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
-  double2* pf = dsm + S::PF + threadIdx.x;
+  C* sbuf = S::sbuf(dsm, li);
+  C* pf = S::pf(dsm);
   const int nb = g.Nx * g.Mz;
   const int groups = (nb + LM::LPC - 1) / LM::LPC;
   const size_t stride = (size_t)g.Mz;
@@ -654,8 +686,8 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) fwd_y_kernel(FwdYArgs a,
     const size_t basen = line_base(gn < g_end ? gn : grp);
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
-      const double2* cur = pf + ub * (P * kThreads);
-      double2* nxt = pf + (ub ^ 1) * (P * kThreads);
+      const C* cur = pf + ub * (P * kThreads);
+      C* nxt = pf + (ub ^ 1) * (P * kThreads);
       if (f + 1 < 3) {
         issue_line<P, T>(nxt, a.Q[f + 1], base, stride, t);
       } else if (gn < g_end) {
@@ -663,7 +695,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) fwd_y_kernel(FwdYArgs a,
       }
       cp_async_commit();
       cp_async_wait<1>();
-      double2 v[P];
+      C v[P];
 #pragma unroll
       for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
       F::template run<-1>(v, t, sbuf, tw_s);
@@ -698,13 +730,13 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) line_kernel(LineArgs a, 
   using F = typename S::F;
   using LM = typename S::LM;
   constexpr int T = F::T;
-  extern __shared__ double2 dsm[];
-  F::load_tw(dsm + S::TW, a.tw);
-  const double2* tw_s = dsm + S::TW;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  F::load_tw(S::tw(dsm), a.tw);
+  const double2* tw_s = S::tw(dsm);
   int li, t;
   LM::get(li, t);
-  double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
-  double2* pf = dsm + S::PF + threadIdx.x;
+  double2* sbuf = S::sbuf(dsm, li);
+  double2* pf = S::pf(dsm);
   const int nb = AXIS == 0 ? g.Ny * g.Mz : g.Nx * g.Mz;
   const size_t stride = AXIS == 0 ? (size_t)g.Ny * g.Mz : (size_t)g.Mz;
   const int groups = (nb + LM::LPC - 1) / LM::LPC;
@@ -842,8 +874,9 @@ enum UpdateMode : int {
   kConvOut = 3,   // out = Qhat with Re(Qhat) = 0, Qhat(0) = 0 (calculate_convolution_2p3)
 };
 
+template <typename Cx = double2>
 struct FwdXArgs {
-  const double2* Qh[3];
+  const Cx* Qh[3];
   const double2* us[3];
   const double2* un[3];     // combination partner (COMBINE only)
   double2* out[3];
@@ -858,10 +891,10 @@ struct FwdXArgs {
 
 // One line of the forward x pass: FFT_x of the 3 product spectra (from the
 // prefetch slots), then the pointwise update of Source/diffusion.cu.
-template <int NX, int P, int MODE, bool COMBINE>
-__device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g, int t, int L,
-                                           size_t off, int inst, bool valid, double2* sbuf,
-                                           const double2* tw_s, double2* pf, int& ub,
+template <int NX, int P, int MODE, bool COMBINE, typename C>
+__device__ __forceinline__ void fwd_x_line(const FwdXArgs<C>& a, const PassGeom& g, int t, int L,
+                                           size_t off, int inst, bool valid, C* sbuf,
+                                           const C* tw_s, C* pf, int& ub,
                                            bool more, size_t offn) {
   constexpr int T = NX / P;
   using F = LineFFT<NX, P>;
@@ -872,8 +905,8 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g,
   double qi[3][P];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const double2* cur = pf + ub * (P * kThreads);
-    double2* nxt = pf + (ub ^ 1) * (P * kThreads);
+    const C* cur = pf + ub * (P * kThreads);
+    C* nxt = pf + (ub ^ 1) * (P * kThreads);
     if (c + 1 < 3) {
       issue_line<P, T>(nxt, a.Qh[c + 1], off, (size_t)nlines, t);
     } else if (more) {
@@ -881,12 +914,12 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g,
     }
     cp_async_commit();
     cp_async_wait<1>();
-    double2 v[P];
+    C v[P];
 #pragma unroll
     for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
     F::template run<-1>(v, t, sbuf, tw_s);
 #pragma unroll
-    for (int s = 0; s < P; ++s) qi[c][s] = v[s].y;
+    for (int s = 0; s < P; ++s) qi[c][s] = (double)v[s].y;
     ub ^= 1;
   }
   if (!valid) return;
@@ -958,19 +991,19 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs& a, const PassGeom& g,
   }
 }
 
-template <int NX, int P, int MODE, bool COMBINE>
-__global__ void __launch_bounds__(kThreads, kMinCtasFwdX) fwd_x_kernel(FwdXArgs a, PassGeom g) {
-  using S = PassSmem<NX, P>;
+template <int NX, int P, int MODE, bool COMBINE, typename C>
+__global__ void __launch_bounds__(kThreads, kMinCtasFwdX) fwd_x_kernel(FwdXArgs<C> a, PassGeom g) {
+  using S = PassSmem<NX, P, C, C>;
   using F = typename S::F;
   using LM = typename S::LM;
   constexpr int T = F::T;
-  extern __shared__ double2 dsm[];
-  F::load_tw(dsm + S::TW, a.tw);
-  const double2* tw_s = dsm + S::TW;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  F::load_tw(S::tw(dsm), a.tw);
+  const C* tw_s = S::tw(dsm);
   int li, t;
   LM::get(li, t);
-  double2* sbuf = dsm + S::SBUF + li * S::STRIDE;
-  double2* pf = dsm + S::PF + threadIdx.x;
+  C* sbuf = S::sbuf(dsm, li);
+  C* pf = S::pf(dsm);
   const int nlines = g.Ny * g.Mz;
   const int tlines = nlines * nbatch(g);
   const int groups = (tlines + LM::LPC - 1) / LM::LPC;
@@ -995,7 +1028,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasFwdX) fwd_x_kernel(FwdXArgs 
     const int inst = Gc / nlines;
     const int gn = grp + gr.step;
     const int Gn = gn * LM::LPC + li;
-    fwd_x_line<NX, P, MODE, COMBINE>(a, g, t, Gc - inst * nlines, line_off(Gc), inst, valid,
+    fwd_x_line<NX, P, MODE, COMBINE, C>(a, g, t, Gc - inst * nlines, line_off(Gc), inst, valid,
                                      sbuf, tw_s, pf, ub, gn < g_end,
                                      line_off(Gn < tlines ? Gn : 0));
   }

@@ -455,6 +455,16 @@ ns3d_status ns3d_server_capacity(const ns3d_server* s, int N, int* slots) {
   return NS3D_ERR_BAD_ARG;
 }
 
+ns3d_status ns3d_server_set_precision(ns3d_server* s, int precision) {
+  if (!s) return NS3D_ERR_BAD_ARG;
+  for (auto& g : s->groups) {
+    if (g.busy) return sfail(s, NS3D_ERR_BAD_ARG, "set the precision between runs");
+    const ns3d_status st = ns3d_set_precision(g.h, precision);
+    if (st != NS3D_OK) return sfail(s, st, ns3d_last_error(g.h));
+  }
+  return NS3D_OK;
+}
+
 ns3d_status ns3d_server_stats(const ns3d_server* s, int N, long long* instance_steps) {
   if (!s || !instance_steps) return NS3D_ERR_BAD_ARG;
   for (const auto& g : s->groups)

@@ -116,20 +116,24 @@ ns3d_status ensure_uv_pool(ns3d_solver* h) {
   return NS3D_OK;
 }
 
-// inv_x -> inv_y -> z -> fwd_y: leaves the y,z-transformed products in A[0..2].
-ns3d_status conv_front(ns3d_solver* h, const double2* const u[3], const double2* const v[3]) {
+// inv_x -> inv_y -> z -> fwd_y: leaves the y,z-transformed products in A[0..2]
+// (FP64 scratch, or FP32 scratch in the precision mode).
+template <typename C>
+ns3d_status conv_front_t(ns3d_solver* h, const double2* const u[3],
+                         const double2* const v[3]) {
+  auto sc = [](double2* p) { return reinterpret_cast<C*>(p); };
   const PassGeom& g = h->geom;
   cudaStream_t st = h->stream;
   if (!v) {
-    InvXArgs<3> ax{};
-    InvYArgs<3> ay{};
-    ZArgs<3> az{};
+    InvXArgs<3, C> ax{};
+    InvYArgs<3, C> ay{};
+    ZArgs<3, C> az{};
     for (int i = 0; i < 3; ++i) {
-      ax.in[i] = u[i]; ax.A[i] = h->A[i]; ax.B[i] = h->B[i];
-      ay.A[i] = h->A[i]; ay.B[i] = h->B[i];
-      ay.C[i] = h->C[i]; ay.D[i] = h->D[i]; ay.E[i] = h->E[i];
-      az.C[i] = h->C[i]; az.D[i] = h->D[i]; az.E[i] = h->E[i];
-      az.Qh[i] = h->A[i];
+      ax.in[i] = u[i]; ax.A[i] = sc(h->A[i]); ax.B[i] = sc(h->B[i]);
+      ay.A[i] = sc(h->A[i]); ay.B[i] = sc(h->B[i]);
+      ay.C[i] = sc(h->C[i]); ay.D[i] = sc(h->D[i]); ay.E[i] = sc(h->E[i]);
+      az.C[i] = sc(h->C[i]); az.D[i] = sc(h->D[i]); az.E[i] = sc(h->E[i]);
+      az.Qh[i] = sc(h->A[i]);
     }
     ax.qcut = h->qcut; ax.tw = h->tw[0];
     ay.tw = h->tw[1];
@@ -140,17 +144,17 @@ ns3d_status conv_front(ns3d_solver* h, const double2* const u[3], const double2*
   } else {
     ns3d_status s = ensure_uv_pool(h);
     if (s != NS3D_OK) return s;
-    InvXArgs<6> ax{};
-    InvYArgs<6> ay{};
-    ZArgs<6> az{};
+    InvXArgs<6, C> ax{};
+    InvYArgs<6, C> ay{};
+    ZArgs<6, C> az{};
     for (int i = 0; i < 6; ++i) {
       ax.in[i] = i < 3 ? u[i] : v[i - 3];
-      ax.A[i] = h->A[i]; ax.B[i] = h->B[i];
-      ay.A[i] = h->A[i]; ay.B[i] = h->B[i];
-      ay.C[i] = h->C[i]; ay.D[i] = h->D[i]; ay.E[i] = h->E[i];
-      az.C[i] = h->C[i]; az.D[i] = h->D[i]; az.E[i] = h->E[i];
+      ax.A[i] = sc(h->A[i]); ax.B[i] = sc(h->B[i]);
+      ay.A[i] = sc(h->A[i]); ay.B[i] = sc(h->B[i]);
+      ay.C[i] = sc(h->C[i]); ay.D[i] = sc(h->D[i]); ay.E[i] = sc(h->E[i]);
+      az.C[i] = sc(h->C[i]); az.D[i] = sc(h->D[i]); az.E[i] = sc(h->E[i]);
     }
-    for (int i = 0; i < 3; ++i) az.Qh[i] = h->A[i];
+    for (int i = 0; i < 3; ++i) az.Qh[i] = sc(h->A[i]);
     ax.qcut = h->qcut; ax.tw = h->tw[0];
     ay.tw = h->tw[1];
     az.tw = h->tw[2];
@@ -158,20 +162,26 @@ ns3d_status conv_front(ns3d_solver* h, const double2* const u[3], const double2*
     NS3D_CHECK(h, ns3d::run_inv_y(ay, g, st), "inv_y(uv)");
     NS3D_CHECK(h, ns3d::run_z(az, g, st), "z(uv)");
   }
-  FwdYArgs fy{};
-  for (int i = 0; i < 3; ++i) fy.Q[i] = h->A[i];
+  FwdYArgs<C> fy{};
+  for (int i = 0; i < 3; ++i) fy.Q[i] = sc(h->A[i]);
   fy.tw = h->tw[1];
   NS3D_CHECK(h, ns3d::run_fwd_y(fy, g, st), "fwd_y");
   return NS3D_OK;
 }
 
+ns3d_status conv_front(ns3d_solver* h, const double2* const u[3], const double2* const v[3]) {
+  return h->precision == NS3D_PRECISION_FP32 ? conv_front_t<float2>(h, u, v)
+                                             : conv_front_t<double2>(h, u, v);
+}
+
 // fwd_x + pointwise update on the products left by conv_front.
-ns3d_status finish(ns3d_solver* h, int mode, bool forcing, const double2* const us[3],
-                   double2* const out[3], const double2* const un[3], double ca, double cb,
-                   double dt, double Re) {
-  FwdXArgs a{};
+template <typename C>
+ns3d_status finish_t(ns3d_solver* h, int mode, bool forcing, const double2* const us[3],
+                     double2* const out[3], const double2* const un[3], double ca, double cb,
+                     double dt, double Re) {
+  FwdXArgs<C> a{};
   for (int i = 0; i < 3; ++i) {
-    a.Qh[i] = h->A[i];
+    a.Qh[i] = reinterpret_cast<const C*>(h->A[i]);
     a.us[i] = us ? us[i] : nullptr;
     a.un[i] = un ? un[i] : nullptr;
     a.out[i] = out[i];
@@ -188,6 +198,14 @@ ns3d_status finish(ns3d_solver* h, int mode, bool forcing, const double2* const 
   a.tw = h->tw[0];
   NS3D_CHECK(h, ns3d::run_fwd_x(mode, un != nullptr, a, h->geom, h->stream), "fwd_x");
   return NS3D_OK;
+}
+
+ns3d_status finish(ns3d_solver* h, int mode, bool forcing, const double2* const us[3],
+                   double2* const out[3], const double2* const un[3], double ca, double cb,
+                   double dt, double Re) {
+  return h->precision == NS3D_PRECISION_FP32
+             ? finish_t<float2>(h, mode, forcing, us, out, un, ca, cb, dt, Re)
+             : finish_t<double2>(h, mode, forcing, us, out, un, ca, cb, dt, Re);
 }
 
 
@@ -1075,28 +1093,29 @@ ns3d_status ns3d_shapiro_error(ns3d_solver* h, const ns3d_complex* ux, const ns3
   return NS3D_OK;
 }
 
-ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
-                                const ns3d_complex* uz, double dt, double Re, int reps,
-                                double* ms) {
-  NS3D_TRY(check_handle(h));
-  NS3D_TRY(check_step(h, dt, Re));
-  if (!args_ok3(ux, uy, uz) || !ms || reps <= 0) return fail(h, NS3D_ERR_BAD_ARG, "bad args");
+extern "C++" {
+namespace ns3d_detail {
+template <typename C>
+ns3d_status profile_passes_t(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                             const ns3d_complex* uz, double dt, double Re, int reps,
+                             double* ms) {
+  auto sc = [](double2* p) { return reinterpret_cast<C*>(p); };
   const PassGeom& g = h->geom;
   cudaStream_t st = h->stream;
   const double2* u[3] = {(const double2*)ux, (const double2*)uy, (const double2*)uz};
-  InvXArgs<3> ax{};
-  InvYArgs<3> ay{};
-  ZArgs<3> az{};
-  FwdYArgs fy{};
-  FwdXArgs fx{};
+  InvXArgs<3, C> ax{};
+  InvYArgs<3, C> ay{};
+  ZArgs<3, C> az{};
+  FwdYArgs<C> fy{};
+  FwdXArgs<C> fx{};
   for (int i = 0; i < 3; ++i) {
-    ax.in[i] = u[i]; ax.A[i] = h->A[i]; ax.B[i] = h->B[i];
-    ay.A[i] = h->A[i]; ay.B[i] = h->B[i];
-    ay.C[i] = h->C[i]; ay.D[i] = h->D[i]; ay.E[i] = h->E[i];
-    az.C[i] = h->C[i]; az.D[i] = h->D[i]; az.E[i] = h->E[i];
-    az.Qh[i] = h->A[i];
-    fy.Q[i] = h->A[i];
-    fx.Qh[i] = h->A[i]; fx.us[i] = u[i]; fx.out[i] = h->u1[i];
+    ax.in[i] = u[i]; ax.A[i] = sc(h->A[i]); ax.B[i] = sc(h->B[i]);
+    ay.A[i] = sc(h->A[i]); ay.B[i] = sc(h->B[i]);
+    ay.C[i] = sc(h->C[i]); ay.D[i] = sc(h->D[i]); ay.E[i] = sc(h->E[i]);
+    az.C[i] = sc(h->C[i]); az.D[i] = sc(h->D[i]); az.E[i] = sc(h->E[i]);
+    az.Qh[i] = sc(h->A[i]);
+    fy.Q[i] = sc(h->A[i]);
+    fx.Qh[i] = sc(h->A[i]); fx.us[i] = u[i]; fx.out[i] = h->u1[i];
     fx.fd[i] = h->f_dense[0] ? h->f_dense[i] : nullptr;
   }
   ax.qcut = h->qcut; ax.tw = h->tw[0];
@@ -1132,6 +1151,19 @@ ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns
   for (int k = 0; k < 5; ++k) ms[k] = acc[k] / reps;
   return NS3D_OK;
 }
+}  // namespace ns3d_detail
+}  // extern "C++"
+
+ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
+                                const ns3d_complex* uz, double dt, double Re, int reps,
+                                double* ms) {
+  NS3D_TRY(check_handle(h));
+  NS3D_TRY(check_step(h, dt, Re));
+  if (!args_ok3(ux, uy, uz) || !ms || reps <= 0) return fail(h, NS3D_ERR_BAD_ARG, "bad args");
+  return h->precision == NS3D_PRECISION_FP32
+             ? profile_passes_t<float2>(h, ux, uy, uz, dt, Re, reps, ms)
+             : profile_passes_t<double2>(h, ux, uy, uz, dt, Re, reps, ms);
+}
 
 }  // extern "C"
 
@@ -1141,6 +1173,24 @@ ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns
 struct ns3d_ensemble {
   ns3d_solver* h = nullptr;
 };
+
+ns3d_status ns3d_set_precision(ns3d_solver* h, int precision) {
+  NS3D_TRY(check_handle(h));
+  if (precision != NS3D_PRECISION_FP64 && precision != NS3D_PRECISION_FP32)
+    return fail(h, NS3D_ERR_BAD_ARG, "precision must be NS3D_PRECISION_FP64 or _FP32");
+  if (precision != h->precision) {
+    NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "precision sync");
+    drop_graph(h);  // the captured step launches the other kernels
+    h->precision = precision;
+  }
+  return NS3D_OK;
+}
+
+int ns3d_get_precision(const ns3d_solver* h) { return h ? h->precision : -1; }
+
+ns3d_status ns3d_ensemble_set_precision(ns3d_ensemble* e, int precision) {
+  return e ? ns3d_set_precision(e->h, precision) : NS3D_ERR_BAD_ARG;
+}
 
 ns3d_status ns3d_ensemble_create(int batch, int Nx, int Ny, int Nz, double Lx, double Ly,
                                  double Lz, ns3d_ensemble** out) {

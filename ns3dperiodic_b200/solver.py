@@ -17,6 +17,9 @@ from ._lib import Ns3dError, Request, Result, lib
 _PI2 = 2.0 * math.pi
 
 
+_PRECISIONS = {"fp64": 0, "fp32": 1}
+
+
 def _ptr(t) -> int:
     return int(t.data_ptr())
 
@@ -373,6 +376,16 @@ class Solver:
                                                float(Re), ctypes.byref(e)), "ns3d_shapiro_error")
         return e.value
 
+    @property
+    def precision(self) -> str:
+        """"fp64" (the reference's arithmetic) or "fp32" (transforms and
+        products in FP32, state and update in FP64)."""
+        return "fp32" if self._L.ns3d_get_precision(self._h) == 1 else "fp64"
+
+    @precision.setter
+    def precision(self, value: str):
+        self._check(self._L.ns3d_set_precision(self._h, _PRECISIONS[value]), "ns3d_set_precision")
+
     def request_fields(self, Re: float, seed: int):
         """The initial (u, v) of a server request on this (cubic) grid."""
         U, V = self.zeros(), self.zeros()
@@ -575,6 +588,11 @@ class Ensemble:
         self._check(self._L.ns3d_ensemble_set_forcing(self._h, *p), "ns3d_ensemble_set_forcing")
         self._forcing = Fd
 
+    def set_precision(self, value: str):
+        """"fp64" or "fp32" for every instance (see Solver.precision)."""
+        self._check(self._L.ns3d_ensemble_set_precision(self._h, _PRECISIONS[value]),
+                    "ns3d_ensemble_set_precision")
+
     def set_params(self, dt, Re):
         import numpy as np
 
@@ -665,6 +683,11 @@ class Server:
         self._check(self._L.ns3d_server_capacity(self._h, int(N), ctypes.byref(c)),
                     "ns3d_server_capacity")
         return c.value
+
+    def set_precision(self, value: str):
+        """"fp64" or "fp32" for every grid (between runs)."""
+        self._check(self._L.ns3d_server_set_precision(self._h, _PRECISIONS[value]),
+                    "ns3d_server_set_precision")
 
     def instance_steps(self, N: int) -> int:
         """JVP steps grid N has run so far, summed over its slots."""
