@@ -655,11 +655,12 @@ def ensemble_instances(count, seed0=0):
     return out
 
 
-def ensemble_bytes(instances, steps):
+def ensemble_bytes(instances, steps, fp32=False):
+    """P3L bytes of every instance (FP32 mode: scratch fields halved, state FP64)."""
     tot = 0
     for _, N, _ in instances:
         _, Sc, Sr = sizes(N)
-        tot += steps * (159 * Sc + 18 * Sr)
+        tot += steps * ((96 * Sc + 9 * Sr) if fp32 else (159 * Sc + 18 * Sr))
     return tot
 
 
@@ -784,7 +785,7 @@ def run_ours_ensemble(args, world, rank, local, pg):
         E.close()
 
     peak, peak_src = peaks()
-    B = ensemble_bytes(inst, steps)
+    B = ensemble_bytes(inst, steps, args.precision == "fp32")
     value = world * len(inst) / (ms / 1e3)
     serial = len(inst) / (t_serial / 1e3)
     return {
