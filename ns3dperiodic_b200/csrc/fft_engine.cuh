@@ -219,10 +219,17 @@ __device__ __forceinline__ void line_sync() {
   }
 }
 
-// shared-memory line buffer index with one pad slot every PADW entries
+// shared-memory line buffer index with one pad slot every PADW entries;
+// PADW = 0: no padding, the position inside each row of 16 elements XORed
+// with bits 3..6 of the index (the 8-byte lines of the FP32 z pass, whose
+// Stockham exchanges the padding leaves 2-way bank conflicted)
 template <int PADW>
 __device__ __forceinline__ int spad(int p) {
-  return p + p / PADW;
+  if constexpr (PADW == 0) {
+    return (p & ~15) | ((p & 15) ^ ((p >> 3) & 15));
+  } else {
+    return p + p / PADW;
+  }
 }
 template <int N, int PADW>
 constexpr int line_buf_len() {
@@ -394,10 +401,11 @@ struct LineFFT {
     StageTw<N, 1, L>::fill(tws, tw_g);
     __syncthreads();
   }
-  template <int DIR, typename C>
+  // PW: the line-buffer index scheme (PADW, or 0 for the XOR swizzle)
+  template <int DIR, int PW = PADW, typename C>
   __device__ __forceinline__ static void run(C (&x)[P], int t, C* sbuf,
                                              const C* __restrict__ tw) {
-    RunPlan<N, T, DIR, PADW, L>::run(x, t, sbuf, tw);
+    RunPlan<N, T, DIR, PW, L>::run(x, t, sbuf, tw);
   }
 };
 

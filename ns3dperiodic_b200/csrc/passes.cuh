@@ -463,6 +463,13 @@ __device__ __forceinline__ void load_pair(C (&w)[P], const C* __restrict__ f1,
 // w holds FFT_z(Q1 + i Q2) at k = t + T s.  Split it with the mirror bin
 // W[N-k] (exchanged through shared memory) and store the half spectra
 // Q1h[k], Q2h[k] for k = 0..N/2.
+// Line-buffer index scheme of the z pass: the XOR swizzle for FP32 lines of
+// 128 points and more (fewer shared-memory wavefronts), the padding else.
+template <int NZ, int P, typename C>
+__host__ __device__ constexpr int z_pw() {
+  return (sizeof(C) == 8 && (NZ & (NZ - 1)) == 0 && NZ >= 128) ? 0 : LineFFT<NZ, P>::PADW;
+}
+
 template <int NZ, int P, typename C>
 __device__ __forceinline__ void store_pair_spectrum(const C (&w)[P], C* sbuf, int t,
                                                     C* __restrict__ o1,
@@ -473,14 +480,14 @@ __device__ __forceinline__ void store_pair_spectrum(const C (&w)[P], C* sbuf, in
   constexpr int T = F::T;
   line_sync<T>();
 #pragma unroll
-  for (int s = 0; s < P; ++s) sbuf[spad<F::PADW>(t + T * s)] = w[s];
+  for (int s = 0; s < P; ++s) sbuf[spad<z_pw<NZ, P, C>()>(t + T * s)] = w[s];
   line_sync<T>();
 #pragma unroll
   for (int s = 0; s < P; ++s) {
     const int k = t + T * s;
     if (k <= NZ / 2 && valid) {
       const C a = w[s];
-      const C m = sbuf[spad<F::PADW>(k == 0 ? 0 : NZ - k)];
+      const C m = sbuf[spad<z_pw<NZ, P, C>()>(k == 0 ? 0 : NZ - k)];
       o1[base + k] = mkc<C>((Rt)0.5 * (a.x + m.x), (Rt)0.5 * (a.y - m.y));
       o2[base + k] = mkc<C>((Rt)0.5 * (a.y + m.y), (Rt)-0.5 * (a.x - m.x));
     }
@@ -516,12 +523,12 @@ __device__ __forceinline__ void uv_component(Rt (&q)[P], int i, const ZArgs<6, C
   C w[P];
   // (d_x u_i, d_y u_i)
   load_pair<NZ, P, false, false>(w, a.E[i], a.D[i], base, t, kfz);
-  F::template run<+1>(w, t, sbuf, tw_s);
+  F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
   for (int s = 0; s < P; ++s) q[s] = vx[s] * (w[s].x * sc) + vy[s] * (w[s].y * sc);
   // (d_z u_i, d_x v_i)
   load_pair<NZ, P, true, false>(w, a.C[i], a.E[3 + i], base, t, kfz);
-  F::template run<+1>(w, t, sbuf, tw_s);
+  F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
   for (int s = 0; s < P; ++s) {
     q[s] = q[s] + vz[s] * (w[s].x * sc);
@@ -529,7 +536,7 @@ __device__ __forceinline__ void uv_component(Rt (&q)[P], int i, const ZArgs<6, C
   }
   // (d_y v_i, d_z v_i)
   load_pair<NZ, P, false, true>(w, a.D[3 + i], a.C[3 + i], base, t, kfz);
-  F::template run<+1>(w, t, sbuf, tw_s);
+  F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
   for (int s = 0; s < P; ++s) q[s] = q[s] + (uy[s] * (w[s].x * sc) + uz[s] * (w[s].y * sc));
 }
@@ -559,24 +566,24 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
     // are live at any time.
     // (u_x, u_y)
     load_pair<NZ, P, false, false>(w, a.C[0], a.C[1], base, t, kfz);
-    F::template run<+1>(w, t, sbuf, tw_s);
+    F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { ux[s] = w[s].x * sc; uy[s] = w[s].y * sc; }
     // (u_z, d_z u_z) from one field
     load_pair<NZ, P, false, true>(w, a.C[2], a.C[2], base, t, kfz);
-    F::template run<+1>(w, t, sbuf, tw_s);
+    F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { uz[s] = w[s].x * sc; q2[s] = w[s].y * sc; }
     // Q_z = u_x d_x u_z + u_y d_y u_z + u_z d_z u_z  (calc_vels_nabla_vels)
     load_pair<NZ, P, false, false>(w, a.E[2], a.D[2], base, t, kfz);
-    F::template run<+1>(w, t, sbuf, tw_s);
+    F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s)
       q2[s] = ux[s] * (w[s].x * sc) + uy[s] * (w[s].y * sc) + uz[s] * q2[s];
     // R2C of Q_z alone
 #pragma unroll
     for (int s = 0; s < P; ++s) w[s] = mkc<C>(q2[s], (Rt)0);
-    F::template run<-1>(w, t, sbuf, tw_s);
+    F::template run<-1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
     if (valid) {
 #pragma unroll
       for (int s = 0; s < P; ++s) {
@@ -586,38 +593,38 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
     }
     // (d_z u_x, d_z u_y)
     load_pair<NZ, P, true, true>(w, a.C[0], a.C[1], base, t, kfz);
-    F::template run<+1>(w, t, sbuf, tw_s);
+    F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { q0[s] = w[s].x * sc; q1[s] = w[s].y * sc; }
     load_pair<NZ, P, false, false>(w, a.E[0], a.D[0], base, t, kfz);
-    F::template run<+1>(w, t, sbuf, tw_s);
+    F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s)
       q0[s] = ux[s] * (w[s].x * sc) + uy[s] * (w[s].y * sc) + uz[s] * q0[s];
     load_pair<NZ, P, false, false>(w, a.E[1], a.D[1], base, t, kfz);
-    F::template run<+1>(w, t, sbuf, tw_s);
+    F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s)
       q1[s] = ux[s] * (w[s].x * sc) + uy[s] * (w[s].y * sc) + uz[s] * q1[s];
     // R2C of (Q_x, Q_y) packed
 #pragma unroll
     for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], q1[s]);
-    F::template run<-1>(w, t, sbuf, tw_s);
+    F::template run<-1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
     store_pair_spectrum<NZ, P>(w, sbuf, t, a.Qh[0], a.Qh[1], base, valid);
     return;
   } else {
     // B(u,v)_i = (v.grad) u_i + (u.grad) v_i; fields 0..2 are u, 3..5 are v
     Rt vx[P], vy[P], vz[P];
     load_pair<NZ, P, false, false>(w, a.C[0], a.C[1], base, t, kfz);
-    F::template run<+1>(w, t, sbuf, tw_s);
+    F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { ux[s] = w[s].x * sc; uy[s] = w[s].y * sc; }
     load_pair<NZ, P, false, false>(w, a.C[2], a.C[3], base, t, kfz);
-    F::template run<+1>(w, t, sbuf, tw_s);
+    F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { uz[s] = w[s].x * sc; vx[s] = w[s].y * sc; }
     load_pair<NZ, P, false, false>(w, a.C[4], a.C[5], base, t, kfz);
-    F::template run<+1>(w, t, sbuf, tw_s);
+    F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { vy[s] = w[s].x * sc; vz[s] = w[s].y * sc; }
     uv_component<NZ, P>(q0, 0, a, base, t, kfz, sc, sbuf, tw_s, ux, uy, uz, vx, vy, vz);
@@ -627,11 +634,11 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
   // forward R2C along z: (Q0, Q1) packed, then Q2 alone
 #pragma unroll
   for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], q1[s]);
-  F::template run<-1>(w, t, sbuf, tw_s);
+  F::template run<-1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
   store_pair_spectrum<NZ, P>(w, sbuf, t, a.Qh[0], a.Qh[1], base, valid);
 #pragma unroll
   for (int s = 0; s < P; ++s) w[s] = mkc<C>(q2[s], (Rt)0);
-  F::template run<-1>(w, t, sbuf, tw_s);
+  F::template run<-1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
   if (valid) {
 #pragma unroll
     for (int s = 0; s < P; ++s) {
