@@ -44,7 +44,8 @@ typedef enum ns3d_status {
   NS3D_ERR_OOM = 3,         /* device allocation failed */
   NS3D_ERR_CUDA = 4,        /* a CUDA launch or API call failed (see ns3d_last_error) */
   NS3D_ERR_NONFINITE = 5,   /* a diagnostic reduction met NaN/Inf */
-  NS3D_ERR_TIMEOUT = 6      /* a bounded device wait gave up */
+  NS3D_ERR_TIMEOUT = 6,     /* a bounded device wait gave up */
+  NS3D_ERR_NOT_CONVERGED = 7 /* an inner linear solve stopped without converging */
 } ns3d_status;
 
 /* ----------------------------------------------------------------------- */
@@ -186,6 +187,17 @@ int64_t ns3d_krylov_length(const ns3d_solver* h);
  * (Source/NS3D_periodic.cu:271-284).  vec is a device array of doubles. */
 ns3d_status ns3d_pack_reduced(ns3d_solver* h, const ns3d_complex* vx, const ns3d_complex* vy,
                               const ns3d_complex* vz, double* vec);
+
+/* vec = Im v(1..) - a*vec_a (+ b*vec_b when vec_b is not NULL), in that
+ * order, on reduced vectors: A_vector_from_velocities_reduced_shifted_kernel
+ * (a = shift_real, vec_b = NULL) and the
+ * A_vector_from_velocities_reduced_shifted_rotated_kernel_Real / _Imag pair
+ * (Source/NS3D_periodic.cu:253-300; with the halves of a rotated vector as
+ * vec_a and vec_b).  vec_a is required. */
+ns3d_status ns3d_pack_reduced_shifted(ns3d_solver* h, const ns3d_complex* vx,
+                                      const ns3d_complex* vy, const ns3d_complex* vz,
+                                      const double* vec_a, double a, const double* vec_b,
+                                      double b, double* vec);
 
 /* v = i*vec, Re := 0, mode 0 := 0: velocities_from_A_vector_reduced_kernel
  * (Source/NS3D_periodic.cu:173-200). */
@@ -634,6 +646,57 @@ void ns3d_map_rhs(void* user, void* in, void* out);
  * 3*Nc-3 (Source/NS3D_periodic.cu:1717); this map uses the reduced packing
  * consistently. */
 void ns3d_map_exponential(void* user, void* in, void* out);
+
+/* Shift-invert maps of the matrix-exponent IRA
+ * (Implicit_restart_Arnoldi_GPU_data_Matrix_Exponent,
+ * Source/Arnoldi/Implicit_restart_Arnoldi.cu:456-742, driven by
+ * Source/NS3D_periodic.cu:1650-1711).  E below is `map.steps` implicit
+ * tangent steps (ns3d_implicit_tangent_step with map.dt and map.Re) of a
+ * reduced vector about the base flow map.u*, which stays fixed; map.v* are
+ * their scratch.  A reduced vector has n = ns3d_krylov_length(map.solver)
+ * entries; a rotated vector has 2n, its real half first. */
+typedef struct ns3d_shift_invert_context {
+  ns3d_map_context map; /* solver, base flow, tangent scratch, dt, Re, steps; status */
+  double shift_real;    /* sigma (shift_real) */
+  double rotate_angle;  /* theta: the rotated maps shift by sigma e^{i theta} */
+  int L;                /* BiCGStab(L) order of the inverse maps (BiCG_L) */
+  double tol;           /* their relative residual to reach (BiCG_tol) */
+  int max_iter;         /* their iteration cap (BiCG_Iter) */
+  int warm_start;       /* 0: every solve starts from x = 0; 1: from the contents
+                           of `out`, as the reference's solve does */
+  ns3d_krylov* inner;   /* workspace of the solves, length n (2n rotated); not the
+                           workspace of the driver that calls the map */
+  int last_flag;        /* out: BiCGStabL flag of the last solve */
+  int last_iter;        /* out: its iteration index */
+  double last_tol;      /* out: its relative residual */
+  long long solves;     /* out: solves so far */
+  long long inner_iter; /* out: their iterations, summed */
+} ns3d_shift_invert_context;
+
+/* user = ns3d_shift_invert_context*: out = E in - sigma*in on reduced
+ * vectors: NSCallMatrixVector_exponential_reduced
+ * (Source/NS3D_periodic.cu:473-500). */
+void ns3d_map_exponential_shifted(void* user, void* in, void* out);
+
+/* user = ns3d_shift_invert_context*, vectors of length 2n: with
+ * (sr, si) = sigma (cos theta, sin theta),
+ *   out_r = E in_r - sr*in_r + si*in_i,  out_i = E in_i - sr*in_i - si*in_r,
+ * the real form of (E - sigma e^{i theta}) (in_r + i in_i):
+ * NSCallMatrixVector_exponential_rotated_reduced
+ * (Source/NS3D_periodic.cu:552-586). */
+void ns3d_map_exponential_rotated(void* user, void* in, void* out);
+
+/* user = ns3d_shift_invert_context*: out = (E - sigma)^{-1} in, solved with
+ * ns3d_bicgstabl(inner, L, ns3d_map_exponential_shifted, ...) to `tol`:
+ * Axb_exponent_invert (Source/NS3D_periodic.cu:506-548).  The reference
+ * exits when the solve does not converge; here the map records
+ * NS3D_ERR_NOT_CONVERGED in map.status (NS3D_ERR_NONFINITE for flag -3) and
+ * fills out with NaN, so the calling driver stops. */
+void ns3d_map_exponent_invert(void* user, void* in, void* out);
+
+/* The same on rotated vectors with ns3d_map_exponential_rotated:
+ * Axb_rotated_exponent_invert (Source/NS3D_periodic.cu:590-630). */
+void ns3d_map_rotated_exponent_invert(void* user, void* in, void* out);
 
 /* The reference's Krylov self-test operator (user_Ax_function,
  * Source/Arnoldi/Matrix_Vector_emulator.cu:10-36): out_i = in_{i+1} - 2 in_i

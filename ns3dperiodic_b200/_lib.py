@@ -20,6 +20,7 @@ STATUS = {
     4: "CUDA error",
     5: "non-finite value",
     6: "device wait timed out",
+    7: "inner linear solve did not converge",
 }
 
 # every symbol include/ns3d.h declares
@@ -29,7 +30,8 @@ EXPORTS = (
     "ns3d_set_forcing", "ns3d_forcing_modes", "ns3d_rk3_step", "ns3d_rk3_steps",
     "ns3d_euler_step", "ns3d_rhs", "ns3d_convolution", "ns3d_convolution_uv",
     "ns3d_jvp_step", "ns3d_jvp_steps", "ns3d_linearised_rhs", "ns3d_implicit_tangent_step",
-    "ns3d_krylov_length", "ns3d_pack_reduced", "ns3d_unpack_reduced", "ns3d_matvec_reduced",
+    "ns3d_krylov_length", "ns3d_pack_reduced", "ns3d_pack_reduced_shifted",
+    "ns3d_unpack_reduced", "ns3d_matvec_reduced",
     "ns3d_diagnostics", "ns3d_profile_passes", "ns3d_mask_cutoff", "ns3d_twiddles",
     "ns3d_save_control_fourier", "ns3d_load_control_fourier", "ns3d_save_control_file",
     "ns3d_load_control_file", "ns3d_write_control_fourier_host", "ns3d_read_control_fourier_host",
@@ -40,6 +42,8 @@ EXPORTS = (
     "ns3d_krylov_last_error", "ns3d_arnoldi", "ns3d_krylov_stats", "ns3d_qr_shifts",
     "ns3d_ira_restart", "ns3d_krylov_profile", "ns3d_krylov_combine", "ns3d_bicgstabl", "ns3d_newton",
     "ns3d_map_rhs", "ns3d_map_linearised", "ns3d_map_exponential", "ns3d_map_laplace1d",
+    "ns3d_map_exponential_shifted", "ns3d_map_exponential_rotated", "ns3d_map_exponent_invert",
+    "ns3d_map_rotated_exponent_invert",
     "ns3d_helmholtz_filter", "ns3d_cutoff_filter", "ns3d_curl", "ns3d_record",
     "ns3d_energy_spectrum", "ns3d_shapiro_state", "ns3d_shapiro_error_physical",
     "ns3d_shapiro_error", "ns3d_series_open", "ns3d_series_write", "ns3d_series_close",
@@ -79,6 +83,16 @@ class MapContext(ctypes.Structure):
                 ("vx", ctypes.c_void_p), ("vy", ctypes.c_void_p), ("vz", ctypes.c_void_p),
                 ("dt", ctypes.c_double), ("Re", ctypes.c_double), ("tau", ctypes.c_double),
                 ("steps", ctypes.c_int), ("status", ctypes.c_int)]
+
+
+class ShiftInvertContext(ctypes.Structure):
+    """ns3d_shift_invert_context of include/ns3d.h."""
+    _fields_ = [("map", MapContext), ("shift_real", ctypes.c_double),
+                ("rotate_angle", ctypes.c_double), ("L", ctypes.c_int), ("tol", ctypes.c_double),
+                ("max_iter", ctypes.c_int), ("warm_start", ctypes.c_int),
+                ("inner", ctypes.c_void_p), ("last_flag", ctypes.c_int),
+                ("last_iter", ctypes.c_int), ("last_tol", ctypes.c_double),
+                ("solves", ctypes.c_longlong), ("inner_iter", ctypes.c_longlong)]
 
 
 class LaplaceContext(ctypes.Structure):
@@ -131,6 +145,7 @@ def _sig(lib):
         "ns3d_implicit_tangent_step": ([_P] + [_P] * 6 + [c_double, c_double], c_int),
         "ns3d_krylov_length": ([_P], c_int64),
         "ns3d_pack_reduced": ([_P] + [_P] * 3 + [_P], c_int),
+        "ns3d_pack_reduced_shifted": ([_P] + [_P] * 3 + [_P, c_double, _P, c_double, _P], c_int),
         "ns3d_unpack_reduced": ([_P, _P] + [_P] * 3, c_int),
         "ns3d_matvec_reduced": ([_P] + [_P] * 3 + [_P, _P, c_double, c_double], c_int),
         "ns3d_diagnostics": ([_P] + [_P] * 3 + [_P, _P, _P], c_int),
@@ -171,6 +186,10 @@ def _sig(lib):
         "ns3d_map_linearised": ([_P, _P, _P], None),
         "ns3d_map_exponential": ([_P, _P, _P], None),
         "ns3d_map_laplace1d": ([_P, _P, _P], None),
+        "ns3d_map_exponential_shifted": ([_P, _P, _P], None),
+        "ns3d_map_exponential_rotated": ([_P, _P, _P], None),
+        "ns3d_map_exponent_invert": ([_P, _P, _P], None),
+        "ns3d_map_rotated_exponent_invert": ([_P, _P, _P], None),
         "ns3d_helmholtz_filter": ([_P, _P, _P, _P, c_double, _P, _P, _P], c_int),
         "ns3d_cutoff_filter": ([_P, _P, _P, _P, c_double, _P, _P, _P], c_int),
         "ns3d_curl": ([_P] + [_P] * 6, c_int),

@@ -24,15 +24,21 @@ __global__ void forcing_scan_kernel(const double2* __restrict__ fx, const double
 __global__ void pack_reduced_kernel(const double2* __restrict__ vx, const double2* __restrict__ vy,
                                     const double2* __restrict__ vz, long long n,
                                     double* __restrict__ vec, const double* __restrict__ vec_shift,
-                                    double inv_tau) {
+                                    double coef, const double* __restrict__ vec_shift2,
+                                    double coef2) {
   const long long m = n - 1;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
        i += (long long)gridDim.x * blockDim.x) {
     double a = vx[i + 1].y, b = vy[i + 1].y, c = vz[i + 1].y;
     if (vec_shift) {
-      a -= vec_shift[i] * inv_tau;
-      b -= vec_shift[i + m] * inv_tau;
-      c -= vec_shift[i + 2 * m] * inv_tau;
+      a -= coef * vec_shift[i];
+      b -= coef * vec_shift[i + m];
+      c -= coef * vec_shift[i + 2 * m];
+    }
+    if (vec_shift2) {
+      a += coef2 * vec_shift2[i];
+      b += coef2 * vec_shift2[i + m];
+      c += coef2 * vec_shift2[i + 2 * m];
     }
     vec[i] = a;
     vec[i + m] = b;

@@ -17,11 +17,14 @@ __global__ void forcing_scan_kernel(const double2* __restrict__ fx, const double
                                     double2* __restrict__ val);
 
 // vec[i + c*(n-1)] = Im v_c[i+1]  (A_vector_from_velocities_reduced_kernel),
-// then vec -= vec_shift / tau when vec_shift != null.
+// then vec -= coef * vec_shift when vec_shift != null and vec += coef2 *
+// vec_shift2 when vec_shift2 != null, in that order (the shifted and
+// rotated packings, Source/NS3D_periodic.cu:253-300).
 __global__ void pack_reduced_kernel(const double2* __restrict__ vx, const double2* __restrict__ vy,
                                     const double2* __restrict__ vz, long long n,
                                     double* __restrict__ vec, const double* __restrict__ vec_shift,
-                                    double inv_tau);
+                                    double coef, const double* __restrict__ vec_shift2,
+                                    double coef2);
 
 // v_c[i+1] = (0, vec[i + c*(n-1)]), v_c[0] = 0 (velocities_from_A_vector_reduced_kernel).
 __global__ void unpack_reduced_kernel(const double* __restrict__ vec, long long n,

@@ -600,13 +600,17 @@ ns3d_status ns3d_krylov_create(int64_t n, int m_max, ns3d_krylov** out) {
   if (e == cudaSuccess) e = cudaMemset(kr->v, 0, sizeof(double) * n);
   if (e == cudaSuccess) e = cudaMemset(kr->w, 0, sizeof(double) * n);
   if (e == cudaSuccess) e = cudaMemset(kr->small, 0, sizeof(double) * small);
+  // The dynamic shared-memory caps are attributes of the kernels, shared by
+  // every workspace on the device: set them for the largest basis any
+  // workspace may have (kMaxColumns), so a workspace created later with a
+  // smaller m_max cannot lower the cap below what an earlier one launches.
   if (e == cudaSuccess) {
-    const size_t smem = sizeof(double) * (size_t)m_max * kRestartThreads;
+    const size_t smem = sizeof(double) * (size_t)kMaxColumns * kRestartThreads;
     e = cudaFuncSetAttribute(restart_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
   }
   if (e == cudaSuccess) {
-    const int sq = (int)(sizeof(double) * ((size_t)m_max * 64 + 8 + m_max + 8));
+    const int sq = (int)(sizeof(double) * ((size_t)kMaxColumns * 64 + 8 + kMaxColumns + 8));
     e = cudaFuncSetAttribute(restart_rows_reg<8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              sq);
     if (e == cudaSuccess)
@@ -947,6 +951,99 @@ void ns3d_map_exponential(void* user, void* in, void* out) {
     if (c->status == NS3D_OK) c->status = s;
     map_poison(c, static_cast<double*>(out));
   }
+}
+
+// Shift-invert maps.  E = `steps` implicit tangent steps of v = unpack(in)
+// about the fixed base flow; the result stays in the context's v fields.
+static ns3d_status implicit_tangent_steps(ns3d_map_context* c, const double* in) {
+  ns3d_status s = ns3d_unpack_reduced(c->solver, in, c->vx, c->vy, c->vz);
+  for (int t = 0; t < c->steps && s == NS3D_OK; ++t)
+    s = ns3d_implicit_tangent_step(c->solver, c->ux, c->uy, c->uz, c->vx, c->vy, c->vz, c->dt,
+                                   c->Re);
+  return s;
+}
+
+static void shift_map_fail(ns3d_shift_invert_context* c, ns3d_status s, double* out,
+                           int64_t count) {
+  if (c->map.status == NS3D_OK) c->map.status = s;
+  if (count > 0 && out) cudaMemset(out, 0xff, sizeof(double) * count);
+}
+
+void ns3d_map_exponential_shifted(void* user, void* in, void* out) {
+  ns3d_shift_invert_context* c = static_cast<ns3d_shift_invert_context*>(user);
+  if (!c) return;
+  ns3d_map_context* m = &c->map;
+  const double* x = static_cast<const double*>(in);
+  ns3d_status s = implicit_tangent_steps(m, x);
+  if (s == NS3D_OK)
+    s = ns3d_pack_reduced_shifted(m->solver, m->vx, m->vy, m->vz, x, c->shift_real, nullptr,
+                                  0.0, static_cast<double*>(out));
+  if (s == NS3D_OK) s = ns3d_synchronize(m->solver);
+  if (s != NS3D_OK)
+    shift_map_fail(c, s, static_cast<double*>(out), ns3d_krylov_length(m->solver));
+}
+
+void ns3d_map_exponential_rotated(void* user, void* in, void* out) {
+  ns3d_shift_invert_context* c = static_cast<ns3d_shift_invert_context*>(user);
+  if (!c) return;
+  ns3d_map_context* m = &c->map;
+  const int64_t n = ns3d_krylov_length(m->solver);
+  const double sr = c->shift_real * std::cos(c->rotate_angle);
+  const double si = c->shift_real * std::sin(c->rotate_angle);
+  const double* xr = static_cast<const double*>(in);
+  const double* xi = xr + n;
+  double* yr = static_cast<double*>(out);
+  double* yi = yr + n;
+  ns3d_status s = implicit_tangent_steps(m, xr);
+  if (s == NS3D_OK)
+    s = ns3d_pack_reduced_shifted(m->solver, m->vx, m->vy, m->vz, xr, sr, xi, si, yr);
+  if (s == NS3D_OK) s = implicit_tangent_steps(m, xi);
+  if (s == NS3D_OK)
+    s = ns3d_pack_reduced_shifted(m->solver, m->vx, m->vy, m->vz, xi, sr, xr, -si, yi);
+  if (s == NS3D_OK) s = ns3d_synchronize(m->solver);
+  if (s != NS3D_OK) shift_map_fail(c, s, yr, 2 * n);
+}
+
+static void exponent_invert(ns3d_shift_invert_context* c, ns3d_user_map_vector A, int64_t n,
+                            const double* rhs, double* x) {
+  ns3d_krylov* kr = c->inner;
+  if (!kr || kr->n != n || !rhs || !x || c->L < 1 || c->L > 16 || c->max_iter < 0) {
+    shift_map_fail(c, NS3D_ERR_BAD_ARG, x, n);
+    return;
+  }
+  if (!c->warm_start) {
+    cudaError_t e = cudaMemsetAsync(x, 0, sizeof(double) * n, kr->stream);
+    if (e != cudaSuccess) {
+      shift_map_fail(c, NS3D_ERR_CUDA, x, n);
+      return;
+    }
+  }
+  double tol = c->tol;
+  int iter = c->max_iter, flag = 1;
+  ns3d_status s = ns3d_bicgstabl(kr, c->L, A, c, x, rhs, &tol, &iter, &flag);
+  c->last_flag = flag;
+  c->last_iter = iter;
+  c->last_tol = tol;
+  c->solves += 1;
+  c->inner_iter += iter;
+  if (s == NS3D_OK && c->map.status != NS3D_OK) s = (ns3d_status)c->map.status;
+  if (s == NS3D_OK && flag != 0)
+    s = flag == -3 ? NS3D_ERR_NONFINITE : NS3D_ERR_NOT_CONVERGED;
+  if (s != NS3D_OK) shift_map_fail(c, s, x, n);
+}
+
+void ns3d_map_exponent_invert(void* user, void* in, void* out) {
+  ns3d_shift_invert_context* c = static_cast<ns3d_shift_invert_context*>(user);
+  if (!c) return;
+  exponent_invert(c, ns3d_map_exponential_shifted, ns3d_krylov_length(c->map.solver),
+                  static_cast<const double*>(in), static_cast<double*>(out));
+}
+
+void ns3d_map_rotated_exponent_invert(void* user, void* in, void* out) {
+  ns3d_shift_invert_context* c = static_cast<ns3d_shift_invert_context*>(user);
+  if (!c) return;
+  exponent_invert(c, ns3d_map_exponential_rotated, 2 * ns3d_krylov_length(c->map.solver),
+                  static_cast<const double*>(in), static_cast<double*>(out));
 }
 
 void ns3d_map_laplace1d(void* user, void* in, void* out) {

@@ -775,8 +775,21 @@ ns3d_status ns3d_pack_reduced(ns3d_solver* h, const ns3d_complex* vx, const ns3d
   if (!args_ok3(vx, vy, vz) || !vec) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
   ns3d::pack_reduced_kernel<<<592, 256, 0, h->stream>>>(
       (const double2*)vx, (const double2*)vy, (const double2*)vz, (long long)h->nc, vec, nullptr,
-      0.0);
+      0.0, nullptr, 0.0);
   NS3D_CHECK(h, cudaGetLastError(), "pack_reduced");
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_pack_reduced_shifted(ns3d_solver* h, const ns3d_complex* vx,
+                                      const ns3d_complex* vy, const ns3d_complex* vz,
+                                      const double* vec_a, double a, const double* vec_b,
+                                      double b, double* vec) {
+  NS3D_TRY(check_handle(h));
+  if (!args_ok3(vx, vy, vz) || !vec || !vec_a) return fail(h, NS3D_ERR_BAD_ARG, "null pointer");
+  ns3d::pack_reduced_kernel<<<592, 256, 0, h->stream>>>(
+      (const double2*)vx, (const double2*)vy, (const double2*)vz, (long long)h->nc, vec, vec_a, a,
+      vec_b, b);
+  NS3D_CHECK(h, cudaGetLastError(), "pack_reduced_shifted");
   return NS3D_OK;
 }
 
@@ -808,7 +821,8 @@ ns3d_status ns3d_matvec_reduced(ns3d_solver* h, const ns3d_complex* ux, const ns
   NS3D_TRY(finish(h, ns3d::kRhs, false, vc, v, nullptr, 0.0, 1.0, 0.0, Re));
   ns3d::pack_reduced_kernel<<<592, 256, 0, h->stream>>>(v[0], v[1], v[2], (long long)h->nc,
                                                         vec_out, tau > 0.0 ? vec_in : nullptr,
-                                                        tau > 0.0 ? 1.0 / tau : 0.0);
+                                                        tau > 0.0 ? 1.0 / tau : 0.0, nullptr,
+                                                        0.0);
   NS3D_CHECK(h, cudaGetLastError(), "pack_reduced");
   return NS3D_OK;
 }

@@ -18,7 +18,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import LaplaceContext, MAP_FN, MapContext, Ns3dError, lib
+from ._lib import LaplaceContext, MAP_FN, MapContext, Ns3dError, ShiftInvertContext, lib
 
 IM_EIG_TOL = 1.0e-15  # Source/Arnoldi/Macros.h:10
 
@@ -47,6 +47,20 @@ class Map:
 
     def ctx_ptr(self) -> int:
         return ctypes.addressof(self.ctx)
+
+
+class ShiftInvertMap(Map):
+    """A shift-invert map (ns3d_shift_invert_context): the status lives in
+    the embedded map context; the inner solves' counters are readable."""
+
+    @property
+    def status(self) -> int:
+        return int(self.ctx.map.status)
+
+    def stats(self) -> dict:
+        c = self.ctx
+        return {"last_flag": c.last_flag, "last_iter": c.last_iter, "last_tol": c.last_tol,
+                "solves": c.solves, "inner_iter": c.inner_iter}
 
 
 def select_shifts(H: np.ndarray, which: str = "LR"):
@@ -191,6 +205,61 @@ class Krylov:
         return Map(ctypes.cast(self._L.ns3d_map_rhs, ctypes.c_void_p).value, ctx,
                    keep=(U, Vscratch))
 
+    def _shift_context(self, solver, U, Vscratch, dt, Re, steps, shift, angle, rotated,
+                       L=6, tol=1e-9, max_iter=None, warm_start=False, inner=None):
+        n = int(self._L.ns3d_krylov_length(solver._h))
+        want = 2 * n if rotated else n
+        p = solver._fields(U, "U")
+        q = solver._fields(Vscratch, "V")
+        m = MapContext(solver._h.value, p[0], p[1], p[2], q[0], q[1], q[2], float(dt), float(Re),
+                       0.0, int(steps), 0)
+        return want, ShiftInvertContext(
+            m, float(shift), float(angle), int(L), float(tol),
+            int(max_iter if max_iter is not None else n + 3), int(bool(warm_start)),
+            inner._h.value if inner is not None else None, 0, 0, 0.0, 0, 0)
+
+    def exponential_shifted_map(self, solver, U, Vscratch, dt: float, Re: float, steps: int,
+                                shift: float, angle: float | None = None) -> ShiftInvertMap:
+        """E - sigma (ns3d_map_exponential_shifted, NSCallMatrixVector_exponential_reduced)
+        or, with ``angle``, its rotated real form on vectors of twice the
+        length (ns3d_map_exponential_rotated); E = ``steps`` implicit tangent
+        steps about the fixed base flow U.  This workspace's length must be
+        the map's."""
+        rotated = angle is not None
+        want, ctx = self._shift_context(solver, U, Vscratch, dt, Re, steps, shift,
+                                        angle or 0.0, rotated)
+        if want != self.n:
+            raise ValueError(f"the map acts on vectors of length {want}, this workspace on {self.n}")
+        fn = self._L.ns3d_map_exponential_rotated if rotated else self._L.ns3d_map_exponential_shifted
+        return ShiftInvertMap(ctypes.cast(fn, ctypes.c_void_p).value, ctx, keep=(U, Vscratch))
+
+    def exponent_invert_map(self, solver, U, Vscratch, dt: float, Re: float, steps: int,
+                            shift: float, angle: float | None = None, L: int = 6,
+                            tol: float = 1.0e-9, max_iter: int | None = None,
+                            warm_start: bool = False) -> ShiftInvertMap:
+        """(E - sigma)^{-1} by BiCGStab(L) (ns3d_map_exponent_invert,
+        Axb_exponent_invert) or, with ``angle``, (E - sigma e^{i angle})^{-1}
+        in real form (ns3d_map_rotated_exponent_invert,
+        Axb_rotated_exponent_invert).  The solves run in a workspace of their
+        own; max_iter defaults to 3*Nx*Ny*Mz as in the reference
+        (BiCG_Iter = N_Arnoldi, Source/NS3D_periodic.cu:1656)."""
+        rotated = angle is not None
+        n = int(self._L.ns3d_krylov_length(solver._h))
+        want = 2 * n if rotated else n
+        if want != self.n:
+            raise ValueError(f"the map acts on vectors of length {want}, this workspace on {self.n}")
+        inner = Krylov(want, 2, device=self.device)
+        if self._stream is not None:
+            inner.set_stream(self._stream)
+        if max_iter is None:
+            max_iter = n + 3
+        _, ctx = self._shift_context(solver, U, Vscratch, dt, Re, steps, shift, angle or 0.0,
+                                     rotated, L, tol, max_iter, warm_start, inner)
+        fn = (self._L.ns3d_map_rotated_exponent_invert if rotated
+              else self._L.ns3d_map_exponent_invert)
+        return ShiftInvertMap(ctypes.cast(fn, ctypes.c_void_p).value, ctx,
+                              keep=(U, Vscratch, inner))
+
     @staticmethod
     def _fnptr(A: Map) -> int:
         return A.fn if isinstance(A.fn, int) else ctypes.cast(A.fn, ctypes.c_void_p).value
@@ -312,6 +381,36 @@ class Krylov:
             ritz_norm = float(np.max(np.abs(ritz[:k0]).astype(np.float32)))
         return eig, ritz_norm, it, V, H
 
+    def implicit_restart_arnoldi_matrix_exponent(self, A_invert: Map, A: Map, which: str = "LR",
+                                                 which_exponent: str = "LM", k: int = 6,
+                                                 m: int = 30, tol: float = 5.0e-8,
+                                                 max_iter: int = 3000, rotated: bool = False,
+                                                 seed: int = 0, f0=None) -> dict:
+        """Implicit_restart_Arnoldi_GPU_data_Matrix_Exponent
+        (Implicit_restart_Arnoldi.cu:456-742): the restart loop on the
+        shift-invert map ``A_invert`` with ``which_exponent`` ordering, on
+        vectors of this workspace's length (twice the original length when
+        ``rotated``), then the eigenpairs of the original map ``A`` from the
+        converged Schur basis: :meth:`eigenpairs` (no rotation) or
+        :meth:`eigenpairs_rotated`.  Returns a dict with the eigenvalues and
+        eigenvectors of ``A`` sorted by ``which``, the residuals (real and
+        imaginary parts for the rotated form), the Ritz norm, the
+        iterations and the eigenvalues of the shift-invert map's H."""
+        if rotated and self.n % 2:
+            raise ValueError("a rotated workspace has even length")
+        eig_h, ritz_norm, it, V, H = self.implicit_restart_arnoldi(
+            A_invert, which_exponent, k, m, tol, max_iter, seed, f0)
+        if A_invert.status != 0:
+            raise Ns3dError(A_invert.status, "shift-invert map")
+        if rotated:
+            w, X, res_r, res_i = self.eigenpairs_rotated(A, V, H, k, which)
+        else:
+            w, X, res_r = self.eigenpairs(A, V, H, k, which)
+            res_i = np.zeros_like(res_r)
+        return {"eigenvalues": w, "eigenvectors": X, "residual_real": res_r,
+                "residual_imag": res_i, "ritz_norm": ritz_norm, "iterations": it,
+                "eigenvalues_invert": eig_h}
+
     # -- final stage of the implicit restart ----------------------------------
     def combine(self, V, C: np.ndarray, out=None):
         """W = V C on the device (ns3d_krylov_combine): V holds m basis
@@ -366,3 +465,44 @@ class Krylov:
         w, Y = w[order], Y[:, order]
         X = torch.complex(self.combine(V1, Y.real), self.combine(V1, Y.imag))
         return w, X, res
+
+    def eigenpairs_rotated(self, A: Map, V, H: np.ndarray, k: int, which: str = "LR"):
+        """The rotated final stage, compute_eigensystem_of_original_mapping_rotation
+        (Implicit_restart_Arnoldi.cu:335-434): the Schur basis V1 = V_k Z of
+        the leading k x k block of H on this workspace's doubled vectors, its
+        halves VR (real) and VI (imaginary), the Galerkin matrix
+        R = VR^T A VR + VI^T A VI of the original map ``A`` (length n/2), the
+        residuals ||A vr_i - VR R e_i|| and ||A vi_i - VI R e_i||, the
+        eigenpairs of R sorted by ``which`` and the eigenvectors
+        x = (VR + VI) y.  Returns (eigenvalues, eigenvectors as a complex
+        (k, n/2) tensor, real residuals, imaginary residuals); eigenvector i
+        belongs to eigenvalue i (the reference permutes the columns a second
+        time after sorting)."""
+        from scipy.linalg import schur
+
+        torch = self._torch
+        if self.n % 2:
+            raise ValueError("a rotated workspace has even length")
+        n2 = self.n // 2
+        _, Z = schur(np.asarray(H[:k, :k], dtype=np.float64), output="real")
+        V1 = self.combine(V, Z)
+        VR, VI = V1[:, :n2].contiguous(), V1[:, n2:].contiguous()
+        AVR, AVI = torch.empty_like(VR), torch.empty_like(VI)
+        for i in range(k):
+            self.apply(A, VR[i], AVR[i])
+            self.apply(A, VI[i], AVI[i])
+        R = (VR @ AVR.T + VI @ AVI.T).cpu().numpy()   # R[i, j] = vr_i . A vr_j + vi_i . A vi_j
+        Rt = torch.as_tensor(R, device=self.device).T
+        res_r = torch.linalg.vector_norm(AVR - Rt @ VR, dim=1).cpu().numpy()
+        res_i = torch.linalg.vector_norm(AVI - Rt @ VI, dim=1).cpu().numpy()
+        w, Y = np.linalg.eig(R)
+        key = -w.real if which == "LR" else -np.abs(w)
+        order = np.argsort(key, kind="stable")
+        w, Y = w[order], Y[:, order]
+        half = Krylov(n2, max(k, 2), device=self.device)
+        try:
+            VS = VR + VI
+            X = torch.complex(half.combine(VS, Y.real), half.combine(VS, Y.imag))
+        finally:
+            half.close()
+        return w, X, res_r, res_i

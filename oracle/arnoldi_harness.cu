@@ -2,7 +2,8 @@
 //
 // oracle/Makefile compiles the reference's Source/Arnoldi/{Arnoldi_Driver.cu,
 // BiCGStabL.cu, Newton.cu, cuda_supp.cu, memory_operations.cu, Matrix_Vector_emulator.cu,
-// Products.cpp, QR_Shifts.cpp, Select_Shifts.cpp, LAPACK_routines.cpp}
+// Implicit_restart_Arnoldi.cu, Products.cpp, QR_Shifts.cpp, Select_Shifts.cpp,
+// LAPACK_routines.cpp, timer.cpp, file_operations.cpp}
 // unmodified (with oracle/c99_complex_prelude.h force-included) together with
 // this file into oracle/_ref/libarnoldi_ref.so.  This file adds only:
 //   * flat C entry points for ctypes (host arrays in, host arrays out);
@@ -11,11 +12,13 @@
 //     Source/Arnoldi/Matrix_Vector_emulator.cu:27-36) and a dense matrix
 //     applied with cublasDgemv;
 //   * forwarding of the Fortran LAPACK names the reference calls (dgeqrf_,
-//     dormqr_, zgeev_, dhseqr_) to the LP64 OpenBLAS that scipy ships
-//     (exported there with a "scipy_" prefix); the image has no other LAPACK.
+//     dormqr_, zgeev_, dhseqr_) and of openblas_set_num_threads to the LP64
+//     OpenBLAS that scipy ships (exported there with a "scipy_" prefix); the
+//     image has no other LAPACK.
 // Arnoldi_driver needs a GPU; the QR-shift and shift-selection entry points
 // are host code and run anywhere the library loads.
 #include "Arnoldi_Driver.h"
+#include "Implicit_restart_Arnoldi.h"
 #include "BiCGStabL.h"
 #include "Newton.h"
 #include "QR_Shifts.h"
@@ -52,6 +55,9 @@ void zgeev_(char* jobvl, char* jobvr, int* n, double _Complex* a, int* lda, doub
 {
     scipy_zgeev_(jobvl, jobvr, n, a, lda, w, vl, ldvl, vr, ldvr, work, lwork, rwork, info);
 }
+void scipy_openblas_set_num_threads(int);
+void openblas_set_num_threads(int n) { scipy_openblas_set_num_threads(n); }
+
 void dhseqr_(char* JOB, char* COMPZ, int* N, int* ILO, int* IHI, double* H, int* LDH, double* WR,
              double* WI, double* Z, int* LDZ, double* WORK, int* LWORK, int* INFO)
 {
@@ -345,6 +351,51 @@ void ref_qr_shifts(int k, int m, double* Q, double* H, const double* eig_re,
         __imag__ eig[i] = eig_im[i];
     }
     QR_shifts(k, m, Q, H, eig.data(), ko);
+}
+
+// Implicit_restart_Arnoldi_GPU_data_Matrix_Exponent
+// (Source/Arnoldi/Implicit_restart_Arnoldi.cu:456-742) with dense operators:
+// the shift-invert map is the column-major n_rot x n_rot matrix Minv
+// (n_rot = 2n when rotated, else n) and the original map the column-major
+// n x n matrix A, both applied with cublasDgemv; which = "LR",
+// which_exponent = "LM" as main passes them (Source/NS3D_periodic.cu:1710).
+// The reference prints its progress and eigenvalues, writes H_pre.dat,
+// H_Schur.dat and Q_Schur.dat into the working directory and seeds its start
+// vector from the clock; it never fills its eigenvalue argument, so this
+// entry returns the k eigenvectors (rows of the k x n arrays vec_re, vec_im,
+// in the reference's column order) and the final Ritz norm in *ritz.
+int ref_ira_matrix_exponent_dense(int n, int rotated, const double* Minv, const double* A, int k,
+                                  int m, double tol, int max_iter, double* vec_re,
+                                  double* vec_im, double* ritz)
+{
+    const int n_rot = rotated ? 2 * n : n;
+    cublasHandle_t handle;
+    if (cublasCreate(&handle) != CUBLAS_STATUS_SUCCESS) return 1;
+    double *Minv_d = nullptr, *A_d = nullptr, *er_d = nullptr, *ei_d = nullptr;
+    cudaMalloc(&Minv_d, sizeof(double) * static_cast<size_t>(n_rot) * n_rot);
+    cudaMalloc(&A_d, sizeof(double) * static_cast<size_t>(n) * n);
+    cudaMalloc(&er_d, sizeof(double) * static_cast<size_t>(n) * k);
+    cudaMalloc(&ei_d, sizeof(double) * static_cast<size_t>(n) * k);
+    cudaMemcpy(Minv_d, Minv, sizeof(double) * static_cast<size_t>(n_rot) * n_rot,
+               cudaMemcpyHostToDevice);
+    cudaMemcpy(A_d, A, sizeof(double) * static_cast<size_t>(n) * n, cudaMemcpyHostToDevice);
+    DenseMap inv{handle, n_rot, Minv_d};
+    DenseMap orig{handle, n, A_d};
+    std::vector<double _Complex> eigenvalues(static_cast<size_t>(m));
+    char which[2] = {'L', 'R'};
+    char which_exponent[2] = {'L', 'M'};
+    *ritz = Implicit_restart_Arnoldi_GPU_data_Matrix_Exponent(
+        handle, false, n, dense_map, &inv, dense_map, &orig, which, which_exponent, k, m,
+        eigenvalues.data(), tol, max_iter, rotated != 0, er_d, ei_d, 1);
+    cudaMemcpy(vec_re, er_d, sizeof(double) * static_cast<size_t>(n) * k, cudaMemcpyDeviceToHost);
+    cudaMemcpy(vec_im, ei_d, sizeof(double) * static_cast<size_t>(n) * k, cudaMemcpyDeviceToHost);
+    const cudaError_t err = cudaDeviceSynchronize();
+    cudaFree(Minv_d);
+    cudaFree(A_d);
+    cudaFree(er_d);
+    cudaFree(ei_d);
+    cublasDestroy(handle);
+    return err == cudaSuccess ? 0 : 2;
 }
 
 // select_shifts (Source/Arnoldi/Select_Shifts.cpp:86-133); host only.

@@ -376,6 +376,38 @@ def linearised_matvec_reduced(g: Grid, U, vec, dt, Re):
     return pack_reduced(rk3_ssp_uv_rhs(g, U, V, dt, Re))
 
 
+def exponential_shifted_reduced(g: Grid, U, vec, dt, Re, steps: int, shift: float):
+    """NSCallMatrixVector_exponential_reduced (NS3D_periodic.cu:473-500):
+    ``steps`` single_time_step_iUV_RHS of v = unpack(vec) about the fixed U,
+    then A_vector_from_velocities_reduced_shifted_kernel (NS3D_periodic.cu:
+    253-270): Im v(1..) - shift * vec."""
+    V = unpack_reduced(g, vec)
+    for _ in range(steps):
+        V = single_time_step_iuv_rhs(g, U, V, dt, Re)
+    return pack_reduced(V) - shift * vec
+
+
+def exponential_rotated_reduced(g: Grid, U, vec, dt, Re, steps: int, shift: float,
+                                angle: float):
+    """NSCallMatrixVector_exponential_rotated_reduced (NS3D_periodic.cu:
+    552-586) on a doubled vector [real half; imaginary half]:
+    out_r = E in_r - sr in_r + si in_i and out_i = E in_i - sr in_i - si in_r
+    with (sr, si) = shift (cos angle, sin angle)
+    (A_vector_from_velocities_reduced_shifted_rotated_kernel_Real/_Imag,
+    NS3D_periodic.cu:273-300)."""
+    n = vec.size // 2
+    sr, si = shift * math.cos(angle), shift * math.sin(angle)
+    xr, xi = vec[:n], vec[n:]
+
+    def e(x):
+        V = unpack_reduced(g, x)
+        for _ in range(steps):
+            V = single_time_step_iuv_rhs(g, U, V, dt, Re)
+        return pack_reduced(V)
+
+    return np.concatenate([e(xr) - sr * xr + si * xi, e(xi) - sr * xi - si * xr])
+
+
 # ---------------------------------------------------------------------------
 # Diagnostics (Source/math_support.cu:720-806, divergence.cu:8-31)
 # ---------------------------------------------------------------------------

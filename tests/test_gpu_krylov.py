@@ -405,3 +405,28 @@ def test_eigenpairs_of_the_implicit_restart(torch):
         r = A @ x - w[i] * x
         assert np.linalg.norm(r) < 1e-8 * np.linalg.norm(x)
     kr.close()
+
+
+def test_restart_after_a_smaller_workspace_is_created(torch):
+    """Kernel shared-memory caps are per kernel, not per workspace: a
+    workspace created later with a small m_max (the inner solves of the
+    shift-invert maps use m_max = 2) must not break the restart of an
+    earlier, larger one."""
+    n, m, k0 = 3000, 30, 12
+    kr = _kr(n, m)
+    small = _kr(n, 2)
+    A = _dense(n, 5)
+    Am = _torch_dense_map(torch, kr, A)
+    V = torch.zeros((m, n), dtype=torch.float64, device="cuda")
+    H = np.zeros((m, m))
+    f = torch.as_tensor(np.random.default_rng(6).standard_normal(n), device="cuda")
+    kr.arnoldi(Am, V, H, f, 0, m)
+    Q = np.linalg.qr(np.random.default_rng(7).standard_normal((m, m)))[0]
+    Vo, fo = V.cpu().numpy().copy(), f.cpu().numpy().copy()
+    Qo, Ho = Q.copy(), H.copy()
+    kr.ira_restart(V, f, Q, H, k0)
+    K.ira_restart(Vo, fo, Qo, Ho, k0)
+    assert np.abs(V.cpu().numpy() - Vo).max() < 1e-12
+    assert np.abs(f.cpu().numpy() - fo).max() < 1e-12
+    small.close()
+    kr.close()
