@@ -23,6 +23,17 @@ Source/Arnoldi/Matrix_Vector_emulator.cu at its test size n = 2,300,000,
 m = 30 (Source/Arnoldi/cuda_test.cu:63-70); the reference arm runs the
 reference's own Arnoldi_driver (cuBLAS) on the same operator and start
 vector.
+
+--workload ira: one "step" is one implicitly restarted Arnoldi run of the
+linearised Navier-Stokes operator J(u0) (NSCallMatrixVector_reduced) about
+the laminar Kolmogorov flow u0 = Re/16 sin(4y) x at 64^3, Re = 200, k = 20,
+m = 40, "LR": a fresh N(0, 2) start vector, --ira-cycles restart cycles
+(tolerance 0, so every run does the same number) and the final Schur /
+Galerkin eigenvector stage.  The reference arm runs the reference's own
+Implicit_restart_Arnoldi_GPU_data (cuBLAS + host LAPACK) with its
+RK3_SSP_UV_RHS-based map on the same base flow.
+
+  python bench.py --workload ira --steps 5 --warmup 3
 """
 from __future__ import annotations
 
@@ -54,7 +65,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
-    ap.add_argument("--workload", choices=["rk3", "arnoldi", "ensemble", "serving"],
+    ap.add_argument("--workload", choices=["rk3", "arnoldi", "ira", "ensemble", "serving"],
                     default="rk3",
                     help="rk3: the RK3 step (default); arnoldi: the Krylov factorisation; "
                          "ensemble: mixed-N Kolmogorov instances stepped as batches")
@@ -64,6 +75,10 @@ def parse():
     ap.add_argument("--rate", type=float, default=200.0, help="serving: mean arrivals per s")
     ap.add_argument("--window", type=float, default=45.0, help="serving: seconds of arrivals")
     ap.add_argument("--slots", default="16,8,4", help="serving: slots for N = 64,96,128")
+    ap.add_argument("--ira-N", type=int, default=64, help="ira: grid size")
+    ap.add_argument("--ira-k", type=int, default=20, help="ira: wanted eigenvalues")
+    ap.add_argument("--ira-m", type=int, default=40, help="ira: Krylov basis size")
+    ap.add_argument("--ira-cycles", type=int, default=20, help="ira: restart cycles per run")
     ap.add_argument("--n-arnoldi", type=int, default=2300000)
     ap.add_argument("--m-arnoldi", type=int, default=30)
     return ap.parse_args()
@@ -637,6 +652,258 @@ def run_reference_arnoldi(args, world, rank, local, pg):
 
 
 # ---------------------------------------------------------------------------
+# implicit restart of the linearised operator about the laminar Kolmogorov
+# flow (64^3, Re = 200, k = 20, m = 40)
+# ---------------------------------------------------------------------------
+def ira_state(N, Re):
+    from ns3dperiodic_b200 import workload as W
+
+    U, _ = W.kolmogorov_state(N, Re, 0, rel_amp=0.0)
+    return U
+
+
+def ira_start(n, seed):
+    import numpy as np
+
+    return np.random.default_rng(seed).normal(0.0, 2.0, n)
+
+
+def run_ours_ira(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+
+    from ns3dperiodic_b200 import Krylov, Solver
+
+    N, Re, k, m, R = args.ira_N, args.Re, args.ira_k, args.ira_m, args.ira_cycles
+    U = ira_state(N, Re)
+    S = Solver(N, N, N)
+    Ud = S.to_device(U)
+    n = S.krylov_length
+    kr = Krylov(n, m)
+    A = kr.linearised_map(S, Ud, Re)
+
+    launches = [0]
+
+    def one_run(f0d):
+        _, rn, it, V, H = kr.implicit_restart_arnoldi(A, "LR", k, m, 0.0, R, f0=f0d)
+        w, X, res = kr.eigenpairs(A, V, H, k, "LR")
+        cols = list(kr.last_restart_columns)
+        # driver + restart kernels, 7 per map call (unpack, 5 passes, pack),
+        # 3 combines of the eigenvector stage
+        launches[0] += kr.last_restart_launches + 7 * (sum(cols) + k) + 3
+        return w, X, res, rn, cols
+
+    f0d = torch.as_tensor(ira_start(n, args.seed + rank), device="cuda")
+    for _ in range(args.warmup):
+        one_run(f0d)
+    barrier(pg)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    s0 = torch.cuda.default_stream()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(s0)
+    out = None
+    launches[0] = 0
+    for _ in range(args.steps):
+        out = one_run(f0d)
+    ev1.record(s0)
+    timed_launches = launches[0]
+    ev1.synchronize()
+    ms_local = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    barrier(pg)
+    ms = max_over_ranks(ms_local, pg)
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+    w, X, res, rn, cols = out
+    peak, peak_src = peaks()
+    # bytes of one run: map calls (P3L) + Gram-Schmidt (one reorthogonalisation)
+    _, Sc, Sr = sizes(N)
+    mv_bytes = 84 * Sc + 6 * Sr
+    calls = sum(cols) + k
+    gs = 0
+    for c in cols:
+        for j in range(m - c, m):
+            gs += 4 * (j + 1) * 8 * n
+    B = mv_bytes * calls + gs
+    # the map alone, timed on the device: the dominant kernel sequence
+    x = torch.as_tensor(ira_start(n, 99), device="cuda")
+    y = torch.empty_like(x)
+    for _ in range(3):
+        kr.apply(A, x, y)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 50
+    e0.record(s0)
+    for _ in range(reps):
+        kr.apply(A, x, y)
+    e1.record(s0)
+    e1.synchronize()
+    mv_ms = e0.elapsed_time(e1) / reps
+    achieved = mv_bytes / (mv_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "linearised map (unpack, 5-pass B(u,v) + update, pack)",
+                "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_src,
+                "alg_bytes_per_launch": mv_bytes, "ms_per_launch": round(mv_ms, 5),
+                "note": "per map call (host-synchronised, as the Krylov drivers call it); "
+                        "pack/unpack bytes not counted"}
+    # e2e: base flow from pinned host memory, eigenvalues and eigenvectors back
+    K = args.e2e_steps or args.steps
+    hU = [torch.from_numpy(np.ascontiguousarray(u)).pin_memory() for u in U]
+    hX = torch.empty((k, n), dtype=torch.complex128).pin_memory()
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(K):
+        for d, h in zip(Ud, hU):
+            d.copy_(h, non_blocking=True)
+        w2, X2, _, _, _ = one_run(f0d)
+        hX.copy_(X2)
+    torch.cuda.synchronize()
+    el = max_over_ranks(time.perf_counter() - t0, pg)
+    kr.close()
+    S.close()
+    nc = N * N * (N // 2 + 1)
+    return {
+        "metric": f"IRA runs/s (linearised NS about laminar Kolmogorov, {N}^3, Re={Re:g}, "
+                  f"k={k}, m={m}, {R} restart cycles + eigenvector stage, FP64)",
+        "value": round(value, 4),
+        "unit": "runs/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"ira_kolmogorov_laminar_{N}_Re{Re:g}_k{k}_m{m}_c{R}",
+                   "N": N, "Re": Re, "k": k, "m": m, "cycles": R, "n": n, "which": "LR",
+                   "map": "ns3d_map_linearised (NSCallMatrixVector_reduced)",
+                   "parallelism": f"replicas x{world}",
+                   "l2": f"basis {m * n * 8 / 1e6:.0f} MB + fields > 126 MB L2",
+                   "map_calls_per_run": calls, "alg_bytes_per_run": B,
+                   "achieved_gbs_per_run": round(B / (ms_step * 1e-3) / 1e9, 1),
+                   "ritz_norm": float(rn),
+                   "leading_eigenvalues": [[round(float(z.real), 8), round(float(z.imag), 8)]
+                                           for z in w[:4]],
+                   "max_schur_residual": float(np.max(res))},
+        "roofline": roofline,
+        "e2e": {"value": round(world * K / el, 4), "unit": "runs/s",
+                "h2d_bytes_per_step": 3 * 16 * nc, "d2h_bytes_per_step": 16 * k * n,
+                "steps": K,
+                "protocol": "base flow from pinned host memory -> device, the run, the k "
+                            "complex eigenvectors back to pinned host memory; wall clock"},
+        "gpu_launches": timed_launches,
+        "clocks": clocks,
+    }
+
+
+def cpu_baseline_ira(N, Re, m, calls, seed):
+    """The oracle's Arnoldi factorisation (numpy) over the oracle's
+    linearised map on a bounded sample: one factorisation from k = 0 with
+    min(m, 8) columns, scaled to a run's map calls."""
+    import numpy as np
+
+    from oracle import krylov_oracle as K
+    from oracle import ns3d_oracle as O
+
+    g = O.Grid(N, N, N)
+    U = ira_state(N, Re)
+    n = 3 * (N * N * (N // 2 + 1) - 1)
+    mm = min(m, 8)
+    f = ira_start(n, seed)
+    V, H = np.zeros((mm, n)), np.zeros((mm, mm))
+    t0 = time.perf_counter()
+    K.arnoldi_driver(lambda v: O.linearised_matvec_reduced(g, U, v, 0.0, Re), V, H, f.copy(), 0,
+                     mm)
+    el = time.perf_counter() - t0
+    per_col = el / mm
+    return {"value": 1.0 / (per_col * calls), "unit": "runs/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": f"one {mm}-column Arnoldi factorisation of the oracle's linearised map "
+                      f"(numpy + scipy.fft) in {el:.1f} s, scaled to the {calls} map calls "
+                      f"(and their Gram-Schmidt) of one run"}
+
+
+def run_reference_ira(args, world, rank, local, pg):
+    import ctypes
+    import tempfile
+
+    if rank != 0:
+        return None
+    path = os.path.join(ROOT, "oracle", "_ref", "libarnoldi_ref.so")
+    if not os.path.exists(path):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libarnoldi_ref.so not built "
+                                                    "(needs the reference tree to compile)"}
+    from oracle.ref_lib import RefSolver
+
+    N, Re, k, m, R = args.ira_N, args.Re, args.ira_k, args.ira_m, args.ira_cycles
+    ns = RefSolver(N, N, N)
+    ns.set_u(ira_state(N, Re))
+    arn = ctypes.CDLL(path)
+    arn.ref_ira_map.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_double)]
+    arn.ref_ira_map.restype = ctypes.c_double
+    fn = ctypes.cast(ns.lib.ref_map_linearised_reduced, ctypes.c_void_p).value
+    ctx = (ctypes.c_double * 2)(Re, 0.0)
+    n = 3 * (N * N * (N // 2 + 1) - 1)
+    libc = ctypes.CDLL(None)
+    sampler = ClockSampler(local)
+    total, rn = 0.0, 0.0
+    # the reference prints to stdout and writes H_pre.dat, H_Schur.dat and
+    # Q_Schur.dat into the working directory: send both elsewhere
+    sys.stdout.flush()
+    saved = os.dup(1)
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.dup2(2, 1)
+        os.chdir(tmp)
+        try:
+            t = ctypes.c_double(0.0)
+            for _ in range(args.warmup):
+                arn.ref_ira_map(n, fn, ctypes.cast(ctx, ctypes.c_void_p), k, m, 0.0, R, 0,
+                                ctypes.byref(t))
+            sampler.start()
+            time.sleep(0.3)
+            for _ in range(args.steps):
+                rn = arn.ref_ira_map(n, fn, ctypes.cast(ctx, ctypes.c_void_p), k, m, 0.0, R, 0,
+                                     ctypes.byref(t))
+                total += t.value
+            clocks = sampler.stop()
+        finally:
+            libc.fflush(None)
+            os.chdir(cwd)
+            os.dup2(saved, 1)
+            os.close(saved)
+    ns.close()
+    if rn < 0:
+        return {"impl": "reference", "unavailable": "reference Implicit_restart_Arnoldi_GPU_data "
+                                                    "run failed"}
+    value = args.steps / (total / 1e3)
+    return {"impl": "reference",
+            "metric": f"IRA runs/s (linearised NS about laminar Kolmogorov, {N}^3, Re={Re:g}, "
+                      f"k={k}, m={m}, {R} restart cycles + eigenvector stage, FP64)",
+            "value": round(value, 4), "unit": "runs/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"ira_kolmogorov_laminar_{N}_Re{Re:g}_k{k}_m{m}_c{R}",
+                       "N": N, "Re": Re, "k": k, "m": m, "cycles": R, "n": n,
+                       "reference": "unmodified Implicit_restart_Arnoldi_GPU_data (cuBLAS, "
+                                    "LAPACK from scipy's OpenBLAS) with RK3_SSP_UV_RHS as "
+                                    "NSCallMatrixVector_reduced, verbose off, sm_100a",
+                       "ritz_norm": rn},
+            "cpu_baseline": None,
+            "e2e": {"value": round(value, 4), "unit": "runs/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "clocks": clocks}
+
+
+# ---------------------------------------------------------------------------
 # mixed-N ensemble: 64 Kolmogorov instances, N in {32,48,64,96,128},
 # Re ~ U[50, 500], seeds 0..63, 200 RK3 steps each
 # ---------------------------------------------------------------------------
@@ -1039,6 +1306,15 @@ def main():
                 line = run_reference_ensemble(args, world, rank, local, pg)
             else:
                 line = run_ours_ensemble(args, world, rank, local, pg)
+        elif args.workload == "ira":
+            if args.impl == "reference":
+                line = run_reference_ira(args, world, rank, local, pg)
+            else:
+                line = run_ours_ira(args, world, rank, local, pg)
+                if rank == 0 and world == 1 and not args.no_cpu_baseline:
+                    line["cpu_baseline"] = cpu_baseline_ira(
+                        args.ira_N, args.Re, args.ira_m, line["config"]["map_calls_per_run"],
+                        args.seed)
         elif args.workload == "arnoldi":
             if args.impl == "reference":
                 line = run_reference_arnoldi(args, world, rank, local, pg)

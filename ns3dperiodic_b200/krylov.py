@@ -368,9 +368,13 @@ class Krylov:
         H = np.zeros((m, m))
         k0, it, ritz_norm = 1, 0, 1.0
         eig = np.zeros(m, dtype=np.complex128)
+        self.last_restart_columns = []  # Arnoldi columns built per cycle (map calls)
+        self.last_restart_launches = 0  # kernels of the driver and the restarts (maps excluded)
         while it < max_iter and ritz_norm > tol:
             it += 1
-            self.arnoldi(A, V, H, f, k0 - 1, m)
+            st = self.arnoldi(A, V, H, f, k0 - 1, m)
+            self.last_restart_columns.append(m - k0 + 1)
+            self.last_restart_launches += st["launches"] + 3  # + norm (2) and restart (1)
             eig, ritz = select_shifts(H, which)
             Q, H, k0 = qr_shifts(k, H, eig)
             if k0 < 1:

@@ -398,6 +398,47 @@ int ref_ira_matrix_exponent_dense(int n, int rotated, const double* Minv, const 
     return err == cudaSuccess ? 0 : 2;
 }
 
+// Implicit_restart_Arnoldi_GPU_data (Source/Arnoldi/Implicit_restart_Arnoldi.cu:
+// 444-453) with a caller's map (a user_map_vector, e.g. the NS harness's
+// ref_map_linearised_reduced) on vectors of length n, verbose off, the
+// eigenvector arrays allocated here beforehand as main does; which = "LR"
+// (which_lm = 0) or "LM".  The reference prints its timer and eigenvalues to
+// stdout and writes H_pre.dat, H_Schur.dat and Q_Schur.dat into the working
+// directory.  Returns the Ritz norm; *ms the device time of the call (CUDA
+// events on the legacy stream, synchronised).  With tol = 0 the loop runs
+// exactly max_iter restart cycles before the final stage.
+double ref_ira_map(int n, void* Axb, void* ctx, int k, int m, double tol, int max_iter,
+                   int which_lm, double* ms)
+{
+    cublasHandle_t handle;
+    if (cublasCreate(&handle) != CUBLAS_STATUS_SUCCESS) return -1.0;
+    double *er_d = nullptr, *ei_d = nullptr;
+    cudaMalloc(&er_d, sizeof(double) * static_cast<size_t>(n) * k);
+    cudaMalloc(&ei_d, sizeof(double) * static_cast<size_t>(n) * k);
+    std::vector<double _Complex> eigenvalues(static_cast<size_t>(m));
+    char which[2] = {'L', which_lm ? 'M' : 'R'};
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaDeviceSynchronize();
+    cudaEventRecord(a, 0);
+    const double ritz = Implicit_restart_Arnoldi_GPU_data(
+        handle, false, n, reinterpret_cast<user_map_vector>(Axb), ctx, which, k, m,
+        eigenvalues.data(), tol, max_iter, er_d, ei_d, 1);
+    cudaEventRecord(b, 0);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    *ms = t;
+    const cudaError_t err = cudaDeviceSynchronize();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(er_d);
+    cudaFree(ei_d);
+    cublasDestroy(handle);
+    return err == cudaSuccess ? ritz : -1.0;
+}
+
 // select_shifts (Source/Arnoldi/Select_Shifts.cpp:86-133); host only.
 void ref_select_shifts(int m, double* H, const char* which, double* eig_re, double* eig_im,
                        double* ritz)

@@ -107,9 +107,63 @@ void rk3(double dt, double Re) {
           S.AM[5]);
 }
 
+// The reference's reduced Krylov packing (velocities_from_A_vector_reduced_kernel
+// and A_vector_from_velocities_reduced_kernel, Source/NS3D_periodic.cu:173-200,
+// 239-250; those kernels live in the reference's main file, which this
+// harness does not compile): v(0) = 0, v(i) = i vec(i-1); vec(i-1) = Im v(i).
+__global__ void harness_unpack_reduced(long long n, const double* vec, cudaComplex* vx,
+                                       cudaComplex* vy, cudaComplex* vz) {
+  const long long m = n - 1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (i == 0) {
+      vx[0].x = vx[0].y = vy[0].x = vy[0].y = vz[0].x = vz[0].y = 0.0;
+    } else {
+      vx[i].x = 0.0;
+      vx[i].y = vec[i - 1];
+      vy[i].x = 0.0;
+      vy[i].y = vec[i - 1 + m];
+      vz[i].x = 0.0;
+      vz[i].y = vec[i - 1 + 2 * m];
+    }
+  }
+}
+
+__global__ void harness_pack_reduced(long long n, const cudaComplex* vx, const cudaComplex* vy,
+                                     const cudaComplex* vz, double* vec) {
+  const long long m = n - 1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
+       i += (long long)gridDim.x * blockDim.x) {
+    vec[i] = vx[i + 1].y;
+    vec[i + m] = vy[i + 1].y;
+    vec[i + 2 * m] = vz[i + 1].y;
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+// NSCallMatrixVector_reduced (Source/NS3D_periodic.cu:340-361) on the
+// harness state, as a user_map_vector for the reference's Krylov code:
+// ctx = double[2] {Re, dt}; vec_in -> S.v (reduced unpacking),
+// RK3_SSP_UV_RHS about S.u (set with ref_set_u), S.v -> vec_out.  No
+// synchronisation, as in the reference (its cuBLAS calls follow on the
+// legacy stream).
+void ref_map_linearised_reduced(void* ctx, void* in, void* out) {
+  const double* c = static_cast<const double*>(ctx);
+  const long long n = (long long)nc();
+  harness_unpack_reduced<<<592, 256>>>(n, static_cast<const double*>(in), S.v[0], S.v[1],
+                                       S.v[2]);
+  RK3_SSP_UV_RHS(S.dimGrid, S.dimBlock, S.dimGrid_C, S.dimBlock_C, S.dx, S.dy, S.dz, c[1], c[0],
+                 S.Nx, S.Ny, S.Nz, S.Mz, S.u[0], S.u[1], S.u[2], S.v[0], S.v[1], S.v[2],
+                 S.u1[0], S.u1[1], S.u1[2], S.u2[0], S.u2[1], S.u2[2], S.u3[0], S.u3[1],
+                 S.u3[2], S.f[0], S.f[1], S.f[2], S.Q[0], S.Q[1], S.Q[2], S.div_hat, S.kx, S.ky,
+                 S.kz, S.din_diffusion, S.din_poisson, S.AM[0], S.AM[1], S.AM[2], S.AM[3],
+                 S.AM[4], S.AM[5]);
+  harness_pack_reduced<<<592, 256>>>(n, S.v[0], S.v[1], S.v[2], static_cast<double*>(out));
+}
+
 
 int ref_create(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz) {
   if (S.live) return -2;

@@ -430,3 +430,46 @@ def test_restart_after_a_smaller_workspace_is_created(torch):
     assert np.abs(f.cpu().numpy() - fo).max() < 1e-12
     small.close()
     kr.close()
+
+
+def test_linearised_map_matches_the_reference_map(torch):
+    """ns3d_map_linearised against the reference's own RK3_SSP_UV_RHS behind
+    the reduced packing of NSCallMatrixVector_reduced (oracle/ref_harness.cu,
+    the map the IRA benchmark's reference arm uses), on the same device
+    vectors."""
+    import ctypes
+
+    from ns3dperiodic_b200 import Solver
+
+    lib = os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref", "libns3d_ref.so")
+    if not os.path.exists(lib):
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    from oracle.ref_lib import RefSolver
+
+    g = O.Grid(16, 16, 16)
+    Re = 40.0
+    U = _kolmogorov(g, Re, 9)
+    S = Solver(16, 16, 16)
+    Ud = S.to_device(U)
+    n = S.krylov_length
+    kr = _kr(n, 2)
+    A = kr.linearised_map(S, Ud, Re)
+    ref = RefSolver(16, 16, 16)
+    try:
+        ref.set_u(U)
+        fn = ref.lib.ref_map_linearised_reduced
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        fn.restype = None
+        ctx = (ctypes.c_double * 2)(Re, 0.0)
+        for seed in (1, 2):
+            x = torch.as_tensor(np.random.default_rng(seed).standard_normal(n), device="cuda")
+            y = torch.empty_like(x)
+            yr = torch.empty_like(x)
+            kr.apply(A, x, y)
+            fn(ctypes.cast(ctx, ctypes.c_void_p), x.data_ptr(), yr.data_ptr())
+            torch.cuda.synchronize()
+            assert O.rel_l2(y.cpu().numpy(), yr.cpu().numpy()) < 1e-12
+    finally:
+        ref.close()
+        kr.close()
+        S.close()
