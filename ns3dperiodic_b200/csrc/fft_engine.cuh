@@ -208,11 +208,13 @@ template <int DIR>
 struct DFT<16, DIR> : DFT_CT<4, 4, DIR> {};
 
 // ---------------------------------------------------------------------------
-// synchronisation of the threads that own a line
+// synchronisation of the threads that own a line: SW is the width of the
+// group that shares the line buffers (the T threads of the line when they
+// sit in one warp, the whole CTA when lines are spread over warps)
 // ---------------------------------------------------------------------------
-template <int T>
+template <int SW>
 __device__ __forceinline__ void line_sync() {
-  if constexpr (T <= 32) {
+  if constexpr (SW <= 32) {
     __syncwarp();
   } else {
     __syncthreads();
@@ -245,7 +247,7 @@ constexpr int line_buf_len() {
 #define NS3D_TW_COMPOSE 1
 #endif
 constexpr bool kComposeTwiddles = NS3D_TW_COMPOSE != 0;
-template <int N, int T, int DIR, int PADW, int NS, int R, int... Rest>
+template <int N, int T, int DIR, int PADW, int SW, int NS, int R, int... Rest>
 struct Stages {
   static constexpr int P = N / T;
   static constexpr int U = P / R;
@@ -256,7 +258,7 @@ struct Stages {
                                              const C* __restrict__ tw) {
     constexpr bool last = sizeof...(Rest) == 0;
     static_assert(!last || NS * R == N, "radices must multiply to N");
-    if constexpr (!last) line_sync<T>();  // previous readers of sbuf are done
+    if constexpr (!last) line_sync<SW>();  // previous readers of sbuf are done
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int b = t + T * u;
@@ -293,10 +295,10 @@ struct Stages {
       }
     }
     if constexpr (!last) {
-      line_sync<T>();
+      line_sync<SW>();
 #pragma unroll
       for (int s = 0; s < P; ++s) x[s] = sbuf[spad<PADW>(t + T * s)];
-      Stages<N, T, DIR, PADW, NS * R, Rest...>::run(x, t, sbuf,
+      Stages<N, T, DIR, PADW, SW, NS * R, Rest...>::run(x, t, sbuf,
                                                     NS > 1 ? tw + (R - 1) * NS : tw);
     }
   }
@@ -339,14 +341,14 @@ template <> struct Plan<384, 12> { using L = RadixList<6, 4, 4, 4>; };
 template <> struct Plan<512, 8> { using L = RadixList<8, 8, 8>; };
 template <> struct Plan<512, 16> { using L = RadixList<16, 16, 2>; };
 
-template <int N, int T, int DIR, int PADW, typename L>
+template <int N, int T, int DIR, int PADW, int SW, typename L>
 struct RunPlan;
-template <int N, int T, int DIR, int PADW, int... Rs>
-struct RunPlan<N, T, DIR, PADW, RadixList<Rs...>> {
+template <int N, int T, int DIR, int PADW, int SW, int... Rs>
+struct RunPlan<N, T, DIR, PADW, SW, RadixList<Rs...>> {
   template <typename C>
   __device__ __forceinline__ static void run(C (&x)[N / T], int t, C* sbuf,
                                              const C* __restrict__ tw) {
-    Stages<N, T, DIR, PADW, 1, Rs...>::run(x, t, sbuf, tw);
+    Stages<N, T, DIR, PADW, SW, 1, Rs...>::run(x, t, sbuf, tw);
   }
 };
 
@@ -401,11 +403,12 @@ struct LineFFT {
     StageTw<N, 1, L>::fill(tws, tw_g);
     __syncthreads();
   }
-  // PW: the line-buffer index scheme (PADW, or 0 for the XOR swizzle)
-  template <int DIR, int PW = PADW, typename C>
+  // PW: the line-buffer index scheme (PADW, or 0 for the XOR swizzle);
+  // SW: the synchronisation width (T: the line's threads share a warp)
+  template <int DIR, int PW = PADW, int SW = T, typename C>
   __device__ __forceinline__ static void run(C (&x)[P], int t, C* sbuf,
                                              const C* __restrict__ tw) {
-    RunPlan<N, T, DIR, PW, L>::run(x, t, sbuf, tw);
+    RunPlan<N, T, DIR, PW, SW, L>::run(x, t, sbuf, tw);
   }
 };
 

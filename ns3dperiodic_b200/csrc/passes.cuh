@@ -66,19 +66,27 @@ __device__ __forceinline__ int signed_idx(int j, int n) { return j < (n >> 1) ? 
 
 // Thread -> (line slot, t) for passes whose batch index is contiguous in
 // memory: lanes with the same t and consecutive lines are adjacent, so a warp
-// reads LPW consecutive elements of each row.
+// reads runs of consecutive elements of each row.  Lines of fewer than 32
+// threads stay inside a warp (LPW lines per warp, synchronised per warp).
+// Lines of 32 threads or more are interleaved over the whole CTA (line
+// threadIdx % LPC, t = threadIdx / LPC, synchronised per CTA): with one line
+// per warp every 16-byte load would sit alone in its 32-byte sector.
 template <int T>
 struct LaneMap {
-  static constexpr int LPW = T <= 32 ? 32 / T : 1;
-  static constexpr int LPC = T <= 32 ? kWarpsPerCta * LPW : (kWarpsPerCta * 32) / T;
+  static constexpr bool kSpread = T >= 32;
+  static constexpr int LPW = T < 32 ? 32 / T : 1;
+  static constexpr int LPC = T < 32 ? kWarpsPerCta * LPW : (kWarpsPerCta * 32) / T;
+  static constexpr int SW = kSpread ? kWarpsPerCta * 32 : T;  // line_sync width
+  // lines side by side in the lanes of one load
+  static constexpr int ADJ = kSpread ? LPC : LPW;
   __device__ __forceinline__ static void get(int& li, int& t) {
-    if constexpr (T <= 32) {
+    if constexpr (!kSpread) {
       const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
       t = lane / LPW;
       li = warp * LPW + lane % LPW;
     } else {
-      t = threadIdx.x % T;
-      li = threadIdx.x / T;
+      li = threadIdx.x % LPC;
+      t = threadIdx.x / LPC;
     }
   }
 };
@@ -142,12 +150,12 @@ __device__ __forceinline__ void issue_line(E* slot, const E* __restrict__ src,
 constexpr int line_stride(int len, int target) {
   return target == 0 ? len : (len % 8 == target % 8 ? len : line_stride(len + 1, target));
 }
-// LaneMap puts LPW lines side by side in a quarter warp: give each its own
+// LaneMap puts ADJ lines side by side in a quarter warp: give each its own
 // 16-byte slots.
 template <int T>
 constexpr int xy_stride_target() {
-  constexpr int lpw = T <= 32 ? 32 / T : 1;
-  constexpr int per_phase = lpw < 8 ? lpw : 8;
+  constexpr int adj = LaneMap<T>::ADJ;
+  constexpr int per_phase = adj < 8 ? adj : 8;
   return per_phase <= 1 ? 0 : 8 / per_phase;
 }
 
@@ -289,7 +297,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF
       C v[P];
 #pragma unroll
       for (int s = 0; s < P; ++s) v[s] = cvt<C>(cur[s * kThreads]);
-      F::template run<+1>(v, t, sbuf, tw_s);
+      F::template run<+1, F::PADW, LM::SW>(v, t, sbuf, tw_s);
       if (valid) {
 #pragma unroll
         for (int s = 0; s < P; ++s) a.A[f][off + (size_t)(t + T * s) * nlines] = v[s];
@@ -300,7 +308,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF
         const Rt kx = (Rt)(g.kfx * (double)signed_idx(t + T * s, NX));
         v[s] = mkc<C>(-u.y * kx, u.x * kx);  // i kx u (build_ders_device)
       }
-      F::template run<+1>(v, t, sbuf, tw_s);
+      F::template run<+1, F::PADW, LM::SW>(v, t, sbuf, tw_s);
       if (valid) {
 #pragma unroll
         for (int s = 0; s < P; ++s) a.B[f][off + (size_t)(t + T * s) * nlines] = v[s];
@@ -372,7 +380,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF
         C v[P];
 #pragma unroll
         for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
-        F::template run<+1>(v, t, sbuf, tw_s);
+        F::template run<+1, F::PADW, LM::SW>(v, t, sbuf, tw_s);
         if (valid) {
 #pragma unroll
           for (int s = 0; s < P; ++s) a.C[f][base + (size_t)(t + T * s) * stride] = v[s];
@@ -383,7 +391,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF
           const Rt ky = (Rt)(g.kfy * (double)signed_idx(t + T * s, NY));
           v[s] = mkc<C>(-u.y * ky, u.x * ky);
         }
-        F::template run<+1>(v, t, sbuf, tw_s);
+        F::template run<+1, F::PADW, LM::SW>(v, t, sbuf, tw_s);
         if (valid) {
 #pragma unroll
           for (int s = 0; s < P; ++s) a.D[f][base + (size_t)(t + T * s) * stride] = v[s];
@@ -404,7 +412,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF
         C v[P];
 #pragma unroll
         for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
-        F::template run<+1>(v, t, sbuf, tw_s);
+        F::template run<+1, F::PADW, LM::SW>(v, t, sbuf, tw_s);
         if (valid) {
 #pragma unroll
           for (int s = 0; s < P; ++s) a.E[f][base + (size_t)(t + T * s) * stride] = v[s];
@@ -705,7 +713,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) fwd_y_kernel(FwdYArgs<C>
       C v[P];
 #pragma unroll
       for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
-      F::template run<-1>(v, t, sbuf, tw_s);
+      F::template run<-1, F::PADW, LaneMap<T>::SW>(v, t, sbuf, tw_s);
       if (valid) {
 #pragma unroll
         for (int s = 0; s < P; ++s) a.Q[f][base + (size_t)(t + T * s) * stride] = v[s];
@@ -772,7 +780,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) line_kernel(LineArgs a, 
     double2 v[P];
 #pragma unroll
     for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
-    F::template run<DIR>(v, t, sbuf, tw_s);
+    F::template run<DIR, F::PADW, LM::SW>(v, t, sbuf, tw_s);
     if (valid) {
 #pragma unroll
       for (int s = 0; s < P; ++s) a.out[base + (size_t)(t + T * s) * stride] = v[s];
@@ -924,7 +932,7 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs<C>& a, const PassGeom&
     C v[P];
 #pragma unroll
     for (int s = 0; s < P; ++s) v[s] = cur[s * kThreads];
-    F::template run<-1>(v, t, sbuf, tw_s);
+    F::template run<-1, F::PADW, LaneMap<T>::SW>(v, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) qi[c][s] = (double)v[s].y;
     ub ^= 1;
