@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--Re", type=float, default=200.0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default pass tiles (ours; the tuner runs before the "
+                         "warm-up, outside the timed region)")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps")
     ap.add_argument("--workload", choices=["rk3", "arnoldi", "ira", "ensemble", "serving"],
                     default="rk3",
@@ -283,6 +286,7 @@ def run_ours(args, world, rank, local, pg):
     stream = torch.cuda.Stream()
     S.set_stream(stream)
     S.precision = args.precision
+    tiles = S.tiles if args.no_autotune else S.autotune()["tiles"]
     fp32 = args.precision == "fp32"
     U = S.to_device(U0)
     F = S.to_device(F0)
@@ -395,6 +399,7 @@ def run_ours(args, world, rank, local, pg):
         "config": {"workload": f"kolmogorov_{N}^3_{args.precision}", "N": N, "Re": Re, "dt": dt,
                    "forcing": "sin(4y) x", "perturbation": "seeded 1e-3, |k|^-2 on 1<=|k|<=8",
                    "parallelism": f"replicas x{world}",
+                   "tiles": dict(zip(("inv_x", "inv_y", "fwd_y", "fwd_x"), tiles)),
                    "l2": f"working set {(24 * Sc) / 1e6:.0f} MB (state + scratch) > 126 MB L2",
                    "mpts_steps_per_s": round(value * N ** 3 / 1e6, 1),
                    "p3l_bytes_per_step": p3l,
@@ -677,6 +682,7 @@ def run_ours_ira(args, world, rank, local, pg):
     N, Re, k, m, R = args.ira_N, args.Re, args.ira_k, args.ira_m, args.ira_cycles
     U = ira_state(N, Re)
     S = Solver(N, N, N)
+    tiles = S.tiles if args.no_autotune else S.autotune()["tiles"]
     Ud = S.to_device(U)
     n = S.krylov_length
     kr = Krylov(n, m)
@@ -782,6 +788,7 @@ def run_ours_ira(args, world, rank, local, pg):
         "config": {"workload": f"ira_kolmogorov_laminar_{N}_Re{Re:g}_k{k}_m{m}_c{R}",
                    "N": N, "Re": Re, "k": k, "m": m, "cycles": R, "n": n, "which": "LR",
                    "map": "ns3d_map_linearised (NSCallMatrixVector_reduced)",
+                   "tiles": dict(zip(("inv_x", "inv_y", "fwd_y", "fwd_x"), tiles)),
                    "parallelism": f"replicas x{world}",
                    "l2": f"basis {m * n * 8 / 1e6:.0f} MB + fields > 126 MB L2",
                    "map_calls_per_run": calls, "alg_bytes_per_run": B,
@@ -943,11 +950,14 @@ def run_ours_ensemble(args, world, rank, local, pg):
     groups = {}
     for seed, N, Re in inst:
         groups.setdefault(N, []).append((seed, Re))
-    ens, fields, pristine, hosts, streams = {}, {}, {}, {}, {}
+    ens, fields, pristine, hosts, streams, ens_tiles = {}, {}, {}, {}, {}, {}
     for N, members in sorted(groups.items()):
         states = [W.kolmogorov_state(N, Re, seed) for seed, Re in members]
         E = Ensemble(len(members), N, N, N)
         E.set_precision(args.precision)
+        if not args.no_autotune:
+            E.autotune()
+        ens_tiles[N] = E.tiles
         st = torch.cuda.Stream()
         E.set_stream(st)
         E.set_forcing(states[0][1])
@@ -998,6 +1008,8 @@ def run_ours_ensemble(args, world, rank, local, pg):
     solo = {N: Solver(N, N, N) for N in groups}
     for N, S in solo.items():
         S.set_stream(solo_st)
+        if not args.no_autotune:
+            S.autotune()
         S.set_forcing(S.to_device(W.kolmogorov_forcing(N, N, N)))
     one = {N: [S.zeros() for _ in range(1)] for N, S in solo.items()}
     torch.cuda.synchronize()
@@ -1022,7 +1034,16 @@ def run_ours_ensemble(args, world, rank, local, pg):
             z.record()
             z.synchronize()
             t_serial += a.elapsed_time(z)
-            # identical to the batched result, instance by instance
+            # identical to the batched result, instance by instance (with the
+            # ensemble's tiles: the solo timing above used the tiles tuned for
+            # one instance, which may differ)
+            if args.precision != "fp32" and S.tiles != ens_tiles[N]:
+                solo_tiles = S.tiles
+                S.tiles = ens_tiles[N]
+                for c in range(3):
+                    U[c].copy_(pristine[N][c][b])
+                S.rk3_ssp(U, dt, Re, nsteps=steps)
+                S.tiles = solo_tiles
             if args.precision == "fp32":  # error of the FP32 ensemble against FP64 alone
                 num = sum(float(torch.linalg.vector_norm(fields[N][c][b] - U[c])) ** 2
                           for c in range(3))
@@ -1076,6 +1097,8 @@ def run_ours_ensemble(args, world, rank, local, pg):
                                             "instances": len(rel_err), "tolerance": 1e-5}
                                            if rel_err else None),
                    "instances_per_N": {str(N): len(m) for N, m in sorted(groups.items())},
+                   "tiles_per_N (inv_x, inv_y, fwd_y, fwd_x)": {str(N): t for N, t in
+                                                                sorted(ens_tiles.items())},
                    "dt": "CFL 0.3 of the laminar peak Re/16 per instance",
                    "parallelism": f"replicas x{world}; one batched ensemble per N, each on its "
                                   "own stream",

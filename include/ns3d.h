@@ -340,6 +340,30 @@ ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns
                                 const ns3d_complex* uz, double dt, double Re, int reps,
                                 double* ms);
 
+/* Autotuner of the pass tiles (no reference counterpart).  Each of the four
+ * pipelined pass families -- 0 inv_x, 1 inv_y, 2 fwd_y, 3 fwd_x -- has a
+ * default tile (16 points per thread for powers of two, 12 for multiples of
+ * 3) and, for extents >= 32 (powers of two) or >= 48 (multiples of 3), an
+ * alternative one (8 or 6 points per thread: twice the lines per CTA, half
+ * the registers and prefetch buffers).  tiles[f] = 0 picks the default, 1
+ * the alternative.  Different tiles change the order of the floating-point
+ * operations of the transforms, so results agree to round-off, not bit for
+ * bit.  The tiles are per precision; a new handle starts with the defaults. */
+#define NS3D_TILE_FAMILIES 4
+ns3d_status ns3d_get_tiles(const ns3d_solver* h, int* tiles);
+/* NS3D_ERR_BAD_ARG for a value other than 0/1 or an alternative the extent
+ * lacks.  Synchronises the handle's stream. */
+ns3d_status ns3d_set_tiles(ns3d_solver* h, const int* tiles);
+/* Times every family with each of its tiles on the handle's own scratch
+ * (`reps` launches after one warm-up, CUDA events, as ns3d_profile_passes;
+ * the state is not touched), keeps the alternative where it is at least 2%
+ * faster, and applies the choice.  Choices are cached per process and
+ * device for (Nx, Ny, Nz, batch, precision): unless `force`, a cached
+ * choice is applied without timing.  ms (8 doubles, may be NULL) receives
+ * per family the mean ms of the default and the alternative tile (-1: not
+ * timed).  Synchronous. */
+ns3d_status ns3d_autotune(ns3d_solver* h, int reps, int force, double* ms);
+
 /* ----------------------------------------------------------------------- */
 /* precision mode                                                           */
 /* ----------------------------------------------------------------------- */
@@ -385,6 +409,10 @@ ns3d_status ns3d_ensemble_set_forcing(ns3d_ensemble* e, const ns3d_complex* fx,
                                       const ns3d_complex* fy, const ns3d_complex* fz);
 /* ns3d_set_precision for the whole ensemble. */
 ns3d_status ns3d_ensemble_set_precision(ns3d_ensemble* e, int precision);
+/* ns3d_autotune / ns3d_get_tiles / ns3d_set_tiles for the ensemble's batch. */
+ns3d_status ns3d_ensemble_autotune(ns3d_ensemble* e, int reps, int force, double* ms);
+ns3d_status ns3d_ensemble_get_tiles(const ns3d_ensemble* e, int* tiles);
+ns3d_status ns3d_ensemble_set_tiles(ns3d_ensemble* e, const int* tiles);
 /* Host arrays of `batch` entries; synchronous.  Required before stepping. */
 ns3d_status ns3d_ensemble_set_params(ns3d_ensemble* e, const double* dt, const double* Re);
 /* nsteps RK3 steps of every instance, in place.  Asynchronous. */

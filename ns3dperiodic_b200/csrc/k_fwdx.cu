@@ -45,8 +45,14 @@ cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs<float2>& a, const P
 }
 
 cudaError_t prepare_fwdx(const PassGeom& g) {
-  const cudaError_t e = prepare_fwdx_prec<double2>(g);
-  return e != cudaSuccess ? e : prepare_fwdx_prec<float2>(g);
+  for (int tile = 0; tile < 2; ++tile) {
+    PassGeom gt = g;
+    for (int& f : gt.tile) f = tile;
+    cudaError_t e = prepare_fwdx_prec<double2>(gt);
+    if (e == cudaSuccess) e = prepare_fwdx_prec<float2>(gt);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace ns3d

@@ -5,6 +5,7 @@
 namespace ns3d {
 
 bool extent_supported(int n) { return extent_supported_inline(n); }
+bool extent_has_alt_tile(int n) { return has_alt_tile(n); }
 
 cudaError_t run_inv_x(const InvXArgs<3>& a, const PassGeom& g, cudaStream_t st) {
   return launch_inv_x<3>(a, g, st);
@@ -50,8 +51,14 @@ cudaError_t prepare_xy_prec(const PassGeom& g) {
 }  // namespace
 
 cudaError_t prepare_xy(const PassGeom& g) {
-  const cudaError_t e = prepare_xy_prec<double2>(g);
-  return e != cudaSuccess ? e : prepare_xy_prec<float2>(g);
+  for (int tile = 0; tile < 2; ++tile) {  // both tiles of every pass family
+    PassGeom gt = g;
+    for (int& f : gt.tile) f = tile;
+    cudaError_t e = prepare_xy_prec<double2>(gt);
+    if (e == cudaSuccess) e = prepare_xy_prec<float2>(gt);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace ns3d

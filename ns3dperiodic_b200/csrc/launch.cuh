@@ -37,6 +37,23 @@ constexpr int p_zuv(int n) { return n % 3 == 0 ? 6 : 4; }
 #define NS3D_PLINE 16
 #endif
 constexpr int p_line(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PLINE); }
+// The autotuner's alternative tile of the pipelined x / y passes: 8 points
+// per thread for powers of two from 32, 6 for multiples of 3 from 48 (twice
+// the lines per CTA, half the registers and prefetch buffers); 0: none.
+constexpr int p_alt(int n) {
+  return n % 3 == 0 ? (n >= 48 ? 6 : 0) : (n >= 32 ? 8 : 0);
+}
+inline bool has_alt_tile(int n) {
+  switch (n) {
+#define NS3D_CASE(N) \
+  case N:            \
+    return p_alt(N) > 0;
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    default:
+      return false;
+  }
+}
 
 inline bool extent_supported_inline(int n) {
   switch (n) {
@@ -90,21 +107,29 @@ inline unsigned persistent_grid(Kern kern, size_t smem, long long groups) {
 template <typename C>
 constexpr int prec_tag() { return sizeof(C) == 16 ? 0 : 100; }
 
+template <int N, int P, int NF, typename C>
+cudaError_t launch_inv_x_p(const InvXArgs<NF, C>& a, const PassGeom& g, cudaStream_t st,
+                           bool prepare_only) {
+  const long long lines = (long long)g.Ny * g.Mz * nbatch(g);
+  using S = PassSmem<N, P, C, double2>;
+  const unsigned grid = persistent_grid<KTag<0, N, P, NF + prec_tag<C>()>>(
+      inv_x_kernel<N, P, NF, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);
+  if (prepare_only) return cudaGetLastError();
+  inv_x_kernel<N, P, NF, C><<<grid, kThreads, S::BYTES, st>>>(a, g);
+  return cudaGetLastError();
+}
+
 template <int NF, typename C>
 cudaError_t launch_inv_x(const InvXArgs<NF, C>& a, const PassGeom& g, cudaStream_t st,
                          bool prepare_only = false) {
-  const long long lines = (long long)g.Ny * g.Mz * nbatch(g);
   switch (g.Nx) {
-#define NS3D_CASE(N)                                                                    \
-  case N: {                                                                             \
-    constexpr int P = p_xy(N);                                                          \
-    using S = PassSmem<N, P, C, double2>;                                               \
-    const unsigned grid = persistent_grid<KTag<0, N, P, NF + prec_tag<C>()>>(           \
-        inv_x_kernel<N, P, NF, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);             \
-    if (prepare_only) return cudaGetLastError();                                        \
-    inv_x_kernel<N, P, NF, C><<<grid, kThreads, S::BYTES, st>>>(a, g);                   \
-    return cudaGetLastError();                                                          \
-  }
+#define NS3D_CASE(N)                                                         \
+  case N:                                                                    \
+    if constexpr (p_alt(N) > 0) {                                            \
+      if (g.tile[kTileInvX])                                                 \
+        return launch_inv_x_p<N, p_alt(N), NF, C>(a, g, st, prepare_only);   \
+    }                                                                        \
+    return launch_inv_x_p<N, p_xy(N), NF, C>(a, g, st, prepare_only);
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE
     default:
@@ -112,22 +137,30 @@ cudaError_t launch_inv_x(const InvXArgs<NF, C>& a, const PassGeom& g, cudaStream
   }
 }
 
+template <int N, int P, int NF, typename C>
+cudaError_t launch_inv_y_p(const InvYArgs<NF, C>& a, const PassGeom& g, cudaStream_t st,
+                           bool prepare_only) {
+  const long long lines = (long long)g.Nx * g.Mz;
+  using S = PassSmem<N, P, C, C>;
+  const unsigned grid = persistent_grid<KTag<1, N, P, NF + prec_tag<C>()>>(
+      inv_y_kernel<N, P, NF, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);
+  if (prepare_only) return cudaGetLastError();
+  inv_y_kernel<N, P, NF, C><<<grid, kThreads, S::BYTES, st>>>(a, g);
+  return cudaGetLastError();
+}
+
 template <int NF, typename C>
 cudaError_t launch_inv_y(const InvYArgs<NF, C>& a, const PassGeom& gi, cudaStream_t st,
                          bool prepare_only = false) {
   const PassGeom g = planes_geom(gi);
-  const long long lines = (long long)g.Nx * g.Mz;
   switch (g.Ny) {
-#define NS3D_CASE(N)                                                                    \
-  case N: {                                                                             \
-    constexpr int P = p_xy(N);                                                          \
-    using S = PassSmem<N, P, C, C>;                                                     \
-    const unsigned grid = persistent_grid<KTag<1, N, P, NF + prec_tag<C>()>>(           \
-        inv_y_kernel<N, P, NF, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);             \
-    if (prepare_only) return cudaGetLastError();                                        \
-    inv_y_kernel<N, P, NF, C><<<grid, kThreads, S::BYTES, st>>>(a, g);                   \
-    return cudaGetLastError();                                                          \
-  }
+#define NS3D_CASE(N)                                                         \
+  case N:                                                                    \
+    if constexpr (p_alt(N) > 0) {                                            \
+      if (g.tile[kTileInvY])                                                 \
+        return launch_inv_y_p<N, p_alt(N), NF, C>(a, g, st, prepare_only);   \
+    }                                                                        \
+    return launch_inv_y_p<N, p_xy(N), NF, C>(a, g, st, prepare_only);
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE
     default:
@@ -154,22 +187,30 @@ cudaError_t launch_z(const ZArgs<UV ? 6 : 3, C>& a, const PassGeom& gi, cudaStre
   }
 }
 
+template <int N, int P, int MODE, bool COMBINE, typename C>
+cudaError_t launch_fwd_x_p(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t st,
+                           bool prepare_only) {
+  const long long lines = (long long)g.Ny * g.Mz * nbatch(g);
+  using S = PassSmem<N, P, C, C>;
+  const unsigned grid =
+      persistent_grid<KTag<2 + 2 * MODE + (COMBINE ? 1 : 0), N, P, prec_tag<C>()>>(
+          fwd_x_kernel<N, P, MODE, COMBINE, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);
+  if (prepare_only) return cudaGetLastError();
+  fwd_x_kernel<N, P, MODE, COMBINE, C><<<grid, kThreads, S::BYTES, st>>>(a, g);
+  return cudaGetLastError();
+}
+
 template <int MODE, bool COMBINE, typename C>
 cudaError_t launch_fwd_x(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t st,
                          bool prepare_only = false) {
-  const long long lines = (long long)g.Ny * g.Mz * nbatch(g);
   switch (g.Nx) {
-#define NS3D_CASE(N)                                                                    \
-  case N: {                                                                             \
-    constexpr int P = p_fx(N);                                                          \
-    using S = PassSmem<N, P, C, C>;                                                     \
-    const unsigned grid =                                                               \
-        persistent_grid<KTag<2 + 2 * MODE + (COMBINE ? 1 : 0), N, P, prec_tag<C>()>>(   \
-            fwd_x_kernel<N, P, MODE, COMBINE, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC); \
-    if (prepare_only) return cudaGetLastError();                                        \
-    fwd_x_kernel<N, P, MODE, COMBINE, C><<<grid, kThreads, S::BYTES, st>>>(a, g);        \
-    return cudaGetLastError();                                                          \
-  }
+#define NS3D_CASE(N)                                                                  \
+  case N:                                                                             \
+    if constexpr (p_alt(N) > 0) {                                                     \
+      if (g.tile[kTileFwdX])                                                          \
+        return launch_fwd_x_p<N, p_alt(N), MODE, COMBINE, C>(a, g, st, prepare_only); \
+    }                                                                                 \
+    return launch_fwd_x_p<N, p_fx(N), MODE, COMBINE, C>(a, g, st, prepare_only);
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE
     default:
@@ -177,22 +218,30 @@ cudaError_t launch_fwd_x(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t s
   }
 }
 
+template <int N, int P, typename C>
+cudaError_t launch_fwd_y_p(const FwdYArgs<C>& a, const PassGeom& g, cudaStream_t st,
+                           bool prepare_only) {
+  const long long lines = (long long)g.Nx * g.Mz;
+  using S = PassSmem<N, P, C, C>;
+  const unsigned grid = persistent_grid<KTag<20, N, P, prec_tag<C>()>>(
+      fwd_y_kernel<N, P, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);
+  if (prepare_only) return cudaGetLastError();
+  fwd_y_kernel<N, P, C><<<grid, kThreads, S::BYTES, st>>>(a, g);
+  return cudaGetLastError();
+}
+
 template <typename C>
 cudaError_t launch_fwd_y(const FwdYArgs<C>& a, const PassGeom& gi, cudaStream_t st,
                          bool prepare_only = false) {
   const PassGeom g = planes_geom(gi);
-  const long long lines = (long long)g.Nx * g.Mz;
   switch (g.Ny) {
-#define NS3D_CASE(N)                                                                    \
-  case N: {                                                                             \
-    constexpr int P = p_xy(N);                                                          \
-    using S = PassSmem<N, P, C, C>;                                                     \
-    const unsigned grid = persistent_grid<KTag<20, N, P, prec_tag<C>()>>(               \
-        fwd_y_kernel<N, P, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);                 \
-    if (prepare_only) return cudaGetLastError();                                        \
-    fwd_y_kernel<N, P, C><<<grid, kThreads, S::BYTES, st>>>(a, g);                       \
-    return cudaGetLastError();                                                          \
-  }
+#define NS3D_CASE(N)                                                      \
+  case N:                                                                 \
+    if constexpr (p_alt(N) > 0) {                                         \
+      if (g.tile[kTileFwdY])                                              \
+        return launch_fwd_y_p<N, p_alt(N), C>(a, g, st, prepare_only);    \
+    }                                                                     \
+    return launch_fwd_y_p<N, p_xy(N), C>(a, g, st, prepare_only);
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE
     default:

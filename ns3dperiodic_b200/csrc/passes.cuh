@@ -48,7 +48,11 @@ struct PassGeom {
   // the x passes split their line index into (instance, y*Mz + z).  0 or 1:
   // a single instance.
   int batch;
+  // Tile choice per pipelined pass family (TileFamily): 0 the default points
+  // per thread, 1 the alternative (p_alt), set by the autotuner.
+  int tile[4];
 };
+enum TileFamily { kTileInvX = 0, kTileInvY = 1, kTileFwdY = 2, kTileFwdX = 3 };
 __host__ __device__ __forceinline__ int nbatch(const PassGeom& g) {
   return g.batch > 1 ? g.batch : 1;
 }

@@ -1,8 +1,11 @@
 // Host side of the C ABI (include/ns3d.h): handle, scratch, RHS pipelines and
 // the steppers of Source/RK_time_step.cu rebuilt on the fused pass kernels.
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1168,6 +1171,107 @@ ns3d_status profile_passes_t(ns3d_solver* h, const ns3d_complex* ux, const ns3d_
 }  // namespace ns3d_detail
 }  // extern "C++"
 
+// ---------------------------------------------------------------------------
+// Autotuner of the pipelined pass tiles
+// ---------------------------------------------------------------------------
+namespace {
+std::mutex g_tune_mu;
+std::map<std::array<int, 6>, std::array<int, 4>> g_tune_cache;
+
+// the extent each pass family transforms along (x: inv_x, fwd_x; y: inv_y, fwd_y)
+int family_extent(const ns3d_solver* h, int f) {
+  return (f == ns3d::kTileInvX || f == ns3d::kTileFwdX) ? h->Nx : h->Ny;
+}
+
+void apply_tiles(ns3d_solver* h, const int* tiles) {
+  drop_graph(h);  // a captured step holds the previous kernels
+  for (int f = 0; f < 4; ++f) {
+    h->tiles[h->precision][f] = tiles[f];
+    h->geom.tile[f] = tiles[f];
+  }
+}
+}  // namespace
+
+extern "C" {
+
+ns3d_status ns3d_get_tiles(const ns3d_solver* h, int* tiles) {
+  if (!h || !tiles) return NS3D_ERR_BAD_ARG;
+  for (int f = 0; f < 4; ++f) tiles[f] = h->geom.tile[f];
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_set_tiles(ns3d_solver* h, const int* tiles) {
+  NS3D_TRY(check_handle(h));
+  if (!tiles) return fail(h, NS3D_ERR_BAD_ARG, "null tiles");
+  for (int f = 0; f < 4; ++f) {
+    if (tiles[f] != 0 && tiles[f] != 1) return fail(h, NS3D_ERR_BAD_ARG, "a tile is 0 or 1");
+    if (tiles[f] == 1 && !ns3d::extent_has_alt_tile(family_extent(h, f)))
+      return fail(h, NS3D_ERR_BAD_ARG, "no alternative tile for this extent");
+  }
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "tiles sync");
+  apply_tiles(h, tiles);
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_autotune(ns3d_solver* h, int reps, int force, double* ms) {
+  NS3D_TRY(check_handle(h));
+  if (reps < 1) return fail(h, NS3D_ERR_BAD_ARG, "reps must be >= 1");
+  const std::array<int, 6> key = {h->device, h->Nx, h->Ny, h->Nz, h->batch, h->precision};
+  bool alt[4];
+  bool any = false;
+  for (int f = 0; f < 4; ++f) any |= (alt[f] = ns3d::extent_has_alt_tile(family_extent(h, f)));
+  if (ms)
+    for (int i = 0; i < 8; ++i) ms[i] = -1.0;
+  NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "autotune sync");
+  if (!force) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      apply_tiles(h, it->second.data());
+      return NS3D_OK;
+    }
+  }
+  // time every pass with each tile on the handle's own scratch: zeros in
+  // u2 stand for the state, fwd_x writes u1 (profile_passes_t)
+  const size_t fb = sizeof(double2) * h->nc * (size_t)h->batch;
+  for (int c = 0; c < 3; ++c)
+    NS3D_CHECK(h, cudaMemsetAsync(h->u2[c], 0, fb, h->stream), "autotune input");
+  const ns3d_complex* u[3] = {(const ns3d_complex*)h->u2[0], (const ns3d_complex*)h->u2[1],
+                              (const ns3d_complex*)h->u2[2]};
+  const int saved[4] = {h->geom.tile[0], h->geom.tile[1], h->geom.tile[2], h->geom.tile[3]};
+  double t[2][5] = {};
+  for (int tile = 0; tile < (any ? 2 : 1); ++tile) {
+    for (int f = 0; f < 4; ++f) h->geom.tile[f] = alt[f] ? tile : 0;
+    const ns3d_status s =
+        h->precision == NS3D_PRECISION_FP32
+            ? profile_passes_t<float2>(h, u[0], u[1], u[2], 1.0e-3, 100.0, reps, t[tile])
+            : profile_passes_t<double2>(h, u[0], u[1], u[2], 1.0e-3, 100.0, reps, t[tile]);
+    if (s != NS3D_OK) {
+      for (int f = 0; f < 4; ++f) h->geom.tile[f] = saved[f];
+      return s;
+    }
+  }
+  // pass index of each family in profile_passes_t: inv_x 0, inv_y 1, fwd_y 3, fwd_x 4
+  const int pass_of[4] = {0, 1, 3, 4};
+  std::array<int, 4> best{};
+  for (int f = 0; f < 4; ++f) {
+    const double t0 = t[0][pass_of[f]], t1 = t[1][pass_of[f]];
+    best[f] = (alt[f] && t1 < 0.98 * t0) ? 1 : 0;  // the default unless 2% faster
+    if (ms) {
+      ms[2 * f] = t0;
+      ms[2 * f + 1] = alt[f] ? t1 : -1.0;
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+  }
+  apply_tiles(h, best.data());
+  return NS3D_OK;
+}
+
+}  // extern "C"
+
 ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns3d_complex* uy,
                                 const ns3d_complex* uz, double dt, double Re, int reps,
                                 double* ms) {
@@ -1196,6 +1300,7 @@ ns3d_status ns3d_set_precision(ns3d_solver* h, int precision) {
     NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "precision sync");
     drop_graph(h);  // the captured step launches the other kernels
     h->precision = precision;
+    for (int f = 0; f < 4; ++f) h->geom.tile[f] = h->tiles[precision][f];
   }
   return NS3D_OK;
 }
@@ -1204,6 +1309,18 @@ int ns3d_get_precision(const ns3d_solver* h) { return h ? h->precision : -1; }
 
 ns3d_status ns3d_ensemble_set_precision(ns3d_ensemble* e, int precision) {
   return e ? ns3d_set_precision(e->h, precision) : NS3D_ERR_BAD_ARG;
+}
+
+ns3d_status ns3d_ensemble_autotune(ns3d_ensemble* e, int reps, int force, double* ms) {
+  return e ? ns3d_autotune(e->h, reps, force, ms) : NS3D_ERR_BAD_ARG;
+}
+
+ns3d_status ns3d_ensemble_get_tiles(const ns3d_ensemble* e, int* tiles) {
+  return e ? ns3d_get_tiles(e->h, tiles) : NS3D_ERR_BAD_ARG;
+}
+
+ns3d_status ns3d_ensemble_set_tiles(ns3d_ensemble* e, const int* tiles) {
+  return e ? ns3d_set_tiles(e->h, tiles) : NS3D_ERR_BAD_ARG;
 }
 
 ns3d_status ns3d_ensemble_create(int batch, int Nx, int Ny, int Nz, double Lx, double Ly,

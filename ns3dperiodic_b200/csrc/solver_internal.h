@@ -19,6 +19,7 @@ struct ns3d_solver {
   size_t nc = 0;  // complex points per field (one instance)
   int batch = 1;  // instances stepped together (ns3d_ensemble); scratch is batch x nc
   int precision = 0;  // NS3D_PRECISION_FP64, or _FP32: transforms and products in FP32
+  int tiles[2][4] = {};  // per precision: tile of each pass family (geom.tile is the current)
   double* dtRe = nullptr;  // per instance (dt, Re) of a batch, device
   double ens_dt = 0.0, ens_Re = 0.0;  // the same for an ensemble of one
   bool ens_params = false;            // ns3d_ensemble_set_params was called

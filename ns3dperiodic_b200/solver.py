@@ -401,6 +401,43 @@ class Solver:
                                                 int(reps), ms), "ns3d_profile_passes")
         return list(ms)
 
+    @property
+    def tiles(self):
+        """Tile of each pass family (inv_x, inv_y, fwd_y, fwd_x): 0 default,
+        1 alternative (see ns3d_set_tiles)."""
+        return _get_tiles(self._L.ns3d_get_tiles, self._h)
+
+    @tiles.setter
+    def tiles(self, value):
+        t = (ctypes.c_int * 4)(*[int(v) for v in value])
+        self._check(self._L.ns3d_set_tiles(self._h, t), "ns3d_set_tiles")
+
+    def autotune(self, reps: int = 20, force: bool = False) -> dict:
+        """Times each pass family with both tiles and keeps the faster
+        (ns3d_autotune).  Returns {"tiles": [...], "ms": 4 x (default,
+        alternative) ms, None when a cached choice was applied}."""
+        return _autotune(self._L.ns3d_autotune, self._h, self._check, reps, force,
+                         self._L.ns3d_get_tiles)
+
+
+TILE_FAMILIES = ("inv_x", "inv_y", "fwd_y", "fwd_x")
+
+
+def _get_tiles(fn, h):
+    t = (ctypes.c_int * 4)()
+    rc = fn(h, t)
+    if rc != 0:
+        raise Ns3dError(rc, "get_tiles")
+    return list(t)
+
+
+def _autotune(fn, h, check, reps, force, get_fn):
+    ms = (ctypes.c_double * 8)()
+    check(fn(h, int(reps), int(bool(force)), ms), "autotune")
+    times = [[ms[2 * f], ms[2 * f + 1]] for f in range(4)]
+    timed = any(x >= 0.0 for row in times for x in row)
+    return {"tiles": _get_tiles(get_fn, h), "ms": times if timed else None}
+
 
 def supported_extent(n: int) -> bool:
     return bool(lib().ns3d_supported_extent(int(n)))
@@ -592,6 +629,21 @@ class Ensemble:
         """"fp64" or "fp32" for every instance (see Solver.precision)."""
         self._check(self._L.ns3d_ensemble_set_precision(self._h, _PRECISIONS[value]),
                     "ns3d_ensemble_set_precision")
+
+    @property
+    def tiles(self):
+        """Pass tiles of the batch (see Solver.tiles)."""
+        return _get_tiles(self._L.ns3d_ensemble_get_tiles, self._h)
+
+    @tiles.setter
+    def tiles(self, value):
+        t = (ctypes.c_int * 4)(*[int(v) for v in value])
+        self._check(self._L.ns3d_ensemble_set_tiles(self._h, t), "ns3d_ensemble_set_tiles")
+
+    def autotune(self, reps: int = 20, force: bool = False) -> dict:
+        """Solver.autotune for the ensemble's batch (ns3d_ensemble_autotune)."""
+        return _autotune(self._L.ns3d_ensemble_autotune, self._h, self._check, reps, force,
+                         self._L.ns3d_ensemble_get_tiles)
 
     def set_params(self, dt, Re):
         import numpy as np

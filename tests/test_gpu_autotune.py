@@ -1,0 +1,163 @@
+"""Autotuner of the pass tiles (ns3d_autotune, ns3d_get/set_tiles): every
+tile gives the default's result to round-off (the transforms only reorder
+their floating-point operations), the tuner keeps what it measured, caches
+per geometry, and an ensemble with tuned tiles still equals its instances
+stepped alone with the same tiles, bit for bit."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ONES = [1, 1, 1, 1]
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+
+    if not t.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    return t
+
+
+def _state(shape, Re, seed):
+    from ns3dperiodic_b200 import workload as W
+
+    Nx, Ny, Nz = shape
+    if Nx == Ny == Nz:
+        return W.kolmogorov_state(Nx, Re, seed, rel_amp=0.05)
+    rng = np.random.default_rng(seed)
+    Mz = Nz // 2 + 1
+    U = [1j * rng.standard_normal((Nx, Ny, Mz)) * 1e-2 * Nx * Ny * Nz for _ in range(3)]
+    for u in U:
+        u[0, 0, 0] = 0.0
+    return U, [np.zeros_like(U[0]) for _ in range(3)]
+
+
+def _rel(a, b, torch):
+    num = sum(float(torch.linalg.vector_norm(x - y)) ** 2 for x, y in zip(a, b))
+    den = sum(float(torch.linalg.vector_norm(y)) ** 2 for y in b)
+    return (num / den) ** 0.5
+
+
+def _alt_tiles(shape):
+    Nx, Ny, _ = shape
+
+    def alt(n):
+        return n >= 48 if n % 3 == 0 else n >= 32
+
+    return [int(alt(Nx)), int(alt(Ny)), int(alt(Ny)), int(alt(Nx))]
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (48, 48, 48), (64, 64, 64), (128, 128, 128),
+                                   (512, 8, 8), (8, 512, 8), (384, 8, 16), (256, 32, 8)])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_alternative_tiles_match_the_default(torch, shape, precision):
+    from ns3dperiodic_b200 import Solver
+
+    Re, dt = 200.0, 1.0e-3
+    U0, F = _state(shape, Re, 3)
+    out = []
+    for tiles in ([0, 0, 0, 0], _alt_tiles(shape)):
+        with Solver(*shape) as S:
+            S.precision = precision
+            S.tiles = tiles
+            assert S.tiles == tiles
+            S.set_forcing(S.to_device(F))
+            U = S.rk3_ssp(S.to_device(U0), dt, Re, nsteps=3)
+            V = S.to_device([0.5 * u for u in U0])
+            Uj, Vj = S.rk3_ssp_uv(S.to_device(U0), V, dt, Re, nsteps=2)
+            out.append((U, Vj))
+    tol = 1e-12 if precision == "fp64" else 2e-6
+    assert _rel(out[1][0], out[0][0], torch) < tol
+    assert _rel(out[1][1], out[0][1], torch) < tol
+
+
+def test_autotune_keeps_what_it_measured_and_caches(torch):
+    from ns3dperiodic_b200 import Solver
+
+    with Solver(64, 64, 64) as S:
+        r = S.autotune(reps=10, force=True)
+        assert r["ms"] is not None and len(r["ms"]) == 4
+        for f, (t0, t1) in enumerate(r["ms"]):
+            assert t0 > 0.0 and t1 > 0.0
+            assert r["tiles"][f] == int(t1 < 0.98 * t0)
+        assert S.tiles == r["tiles"]
+        with Solver(64, 64, 64) as S2:
+            r2 = S2.autotune()
+            assert r2["ms"] is None and r2["tiles"] == r["tiles"]
+    with Solver(16, 16, 16) as S:  # no alternative tile below 32
+        r = S.autotune(reps=3, force=True)
+        assert r["tiles"] == [0, 0, 0, 0]
+        assert all(t1 < 0.0 for _, t1 in r["ms"])
+
+
+def test_set_tiles_rejects_what_the_extent_lacks(torch):
+    from ns3dperiodic_b200 import Solver
+    from ns3dperiodic_b200._lib import Ns3dError
+
+    with Solver(16, 64, 16) as S:
+        with pytest.raises(Ns3dError):
+            S.tiles = [1, 0, 0, 0]  # x = 16 has no alternative
+        with pytest.raises(Ns3dError):
+            S.tiles = [0, 2, 0, 0]
+        S.tiles = [0, 1, 1, 0]       # y = 64 has one
+        assert S.tiles == [0, 1, 1, 0]
+
+
+def test_tiles_follow_the_precision(torch):
+    from ns3dperiodic_b200 import Solver
+
+    with Solver(32, 32, 32) as S:
+        S.tiles = ONES
+        S.precision = "fp32"
+        assert S.tiles == [0, 0, 0, 0]
+        S.tiles = [1, 0, 1, 0]
+        S.precision = "fp64"
+        assert S.tiles == ONES
+        S.precision = "fp32"
+        assert S.tiles == [1, 0, 1, 0]
+
+
+def test_tuned_ensemble_equals_its_instances_alone(torch):
+    from ns3dperiodic_b200 import Ensemble, Solver
+    from ns3dperiodic_b200 import workload as W
+
+    N, Res = 48, [80.0, 160.0, 320.0]
+    states = [W.kolmogorov_state(N, Re, b, rel_amp=0.05) for b, Re in enumerate(Res)]
+    E = Ensemble(len(Res), N, N, N)
+    E.autotune(reps=5, force=True)
+    E.tiles = ONES
+    E.set_forcing(states[0][1])
+    E.set_params([W.kolmogorov_dt(N, Re) for Re in Res], Res)
+    U = E.to_device([np.stack([st[0][c] for st in states]) for c in range(3)])
+    E.rk3_steps(U, 5)
+    with Solver(N, N, N) as S:
+        S.tiles = ONES
+        S.set_forcing(S.to_device(states[0][1]))
+        for b, Re in enumerate(Res):
+            Ub = S.rk3_ssp(S.to_device(states[b][0]), W.kolmogorov_dt(N, Re), Re, nsteps=5)
+            for c in range(3):
+                assert torch.equal(U[c][b], Ub[c])
+    E.close()
+
+
+def test_changing_tiles_recaptures_the_step(torch):
+    """The cached RK3 step graph holds the kernels of the tiles it was
+    captured with: after set_tiles the step uses the new ones."""
+    from ns3dperiodic_b200 import Solver
+    from ns3dperiodic_b200 import workload as W
+
+    N, Re = 64, 200.0
+    U0, F = W.kolmogorov_state(N, Re, 1, rel_amp=0.05)
+    dt = W.kolmogorov_dt(N, Re)
+    with Solver(N, N, N) as S, Solver(N, N, N) as T:
+        for X in (S, T):
+            X.set_forcing(X.to_device(F))
+        T.tiles = ONES
+        S.rk3_ssp(S.to_device(U0), dt, Re, nsteps=2)  # captures the default step
+        S.tiles = ONES
+        a = S.rk3_ssp(S.to_device(U0), dt, Re, nsteps=2)
+        b = T.rk3_ssp(T.to_device(U0), dt, Re, nsteps=2)
+        for c in range(3):
+            assert torch.equal(a[c], b[c])
