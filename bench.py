@@ -1228,6 +1228,8 @@ def run_ours_serving(args, world, rank, local, pg):
     sampler = ClockSampler(local)
     sampler.start()
     with Server(SERVE_NS, capacity=slots, hbm_fraction=0.8) as srv:
+        if not args.no_autotune:
+            srv.autotune()
         caps = {N: srv.capacity(N) for N in SERVE_NS}
         srv.submit([(N, Re, T, sd, a, 0) for N, Re, T, sd, a in reqs])
         t0 = time.perf_counter()
@@ -1246,6 +1248,8 @@ def run_ours_serving(args, world, rank, local, pg):
     sub_rate = max(0.6 * len(done) / wall, 0.05)
     reqs2 = serving_requests(sub_rate, args.window, seed=1000 + rank)
     with Server(SERVE_NS, capacity=slots, hbm_fraction=0.8) as srv:
+        if not args.no_autotune:
+            srv.autotune()
         if reqs2:
             srv.submit([(N, Re, T, sd, a, 0) for N, Re, T, sd, a in reqs2])
             srv.run()

@@ -474,6 +474,10 @@ const char* ns3d_server_last_error(const ns3d_server* s);
 ns3d_status ns3d_server_capacity(const ns3d_server* s, int N, int* slots);
 /* ns3d_set_precision for every grid of the server (between runs). */
 ns3d_status ns3d_server_set_precision(ns3d_server* s, int precision);
+/* ns3d_autotune for every grid at its full slot count, between runs.  Tuned
+ * grids give results that agree with the single-grid API to round-off; with
+ * the default tiles (no call) they agree bit for bit. */
+ns3d_status ns3d_server_autotune(ns3d_server* s, int reps);
 /* JVP steps the grid N has launched so far, summed over its active slots
  * (the work done, finished requests or not). */
 ns3d_status ns3d_server_stats(const ns3d_server* s, int N, long long* instance_steps);

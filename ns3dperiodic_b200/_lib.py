@@ -53,7 +53,7 @@ EXPORTS = (
     "ns3d_ensemble_set_params", "ns3d_ensemble_rk3_steps", "ns3d_ensemble_diagnostics",
     "ns3d_set_precision", "ns3d_get_precision", "ns3d_ensemble_set_precision",
     "ns3d_get_tiles", "ns3d_set_tiles", "ns3d_autotune", "ns3d_ensemble_autotune",
-    "ns3d_ensemble_get_tiles", "ns3d_ensemble_set_tiles",
+    "ns3d_ensemble_get_tiles", "ns3d_ensemble_set_tiles", "ns3d_server_autotune",
     "ns3d_server_create", "ns3d_server_destroy", "ns3d_server_last_error",
     "ns3d_server_capacity", "ns3d_server_stats", "ns3d_server_set_precision", "ns3d_server_submit", "ns3d_server_run", "ns3d_server_results",
     "ns3d_server_result_field", "ns3d_request_fields", "ns3d_request_steps",
@@ -223,6 +223,7 @@ def _sig(lib):
         "ns3d_ensemble_autotune": ([_P, c_int, c_int, _P], c_int),
         "ns3d_ensemble_get_tiles": ([_P, _P], c_int),
         "ns3d_ensemble_set_tiles": ([_P, _P], c_int),
+        "ns3d_server_autotune": ([_P, c_int], c_int),
         "ns3d_server_create": ([_P, c_int, _P, c_double, ctypes.POINTER(c_void_p)], c_int),
         "ns3d_server_destroy": ([_P], c_int),
         "ns3d_server_last_error": ([_P], ctypes.c_char_p),

@@ -465,6 +465,17 @@ ns3d_status ns3d_server_set_precision(ns3d_server* s, int precision) {
   return NS3D_OK;
 }
 
+ns3d_status ns3d_server_autotune(ns3d_server* s, int reps) {
+  if (!s || reps < 1) return NS3D_ERR_BAD_ARG;
+  for (auto& g : s->groups) {
+    if (g.busy) return sfail(s, NS3D_ERR_BAD_ARG, "tune between runs");
+    g.h->geom.batch = g.h->batch;  // tune for the full slot count
+    const ns3d_status st = ns3d_autotune(g.h, reps, 0, nullptr);
+    if (st != NS3D_OK) return sfail(s, st, ns3d_last_error(g.h));
+  }
+  return NS3D_OK;
+}
+
 ns3d_status ns3d_server_stats(const ns3d_server* s, int N, long long* instance_steps) {
   if (!s || !instance_steps) return NS3D_ERR_BAD_ARG;
   for (const auto& g : s->groups)

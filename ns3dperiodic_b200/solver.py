@@ -741,6 +741,10 @@ class Server:
         self._check(self._L.ns3d_server_set_precision(self._h, _PRECISIONS[value]),
                     "ns3d_server_set_precision")
 
+    def autotune(self, reps: int = 10):
+        """Tile autotuner for every grid at its slot count (between runs)."""
+        self._check(self._L.ns3d_server_autotune(self._h, int(reps)), "ns3d_server_autotune")
+
     def instance_steps(self, N: int) -> int:
         """JVP steps grid N has run so far, summed over its slots."""
         c = ctypes.c_longlong()

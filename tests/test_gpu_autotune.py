@@ -161,3 +161,27 @@ def test_changing_tiles_recaptures_the_step(torch):
         b = T.rk3_ssp(T.to_device(U0), dt, Re, nsteps=2)
         for c in range(3):
             assert torch.equal(a[c], b[c])
+
+
+def test_server_autotune_runs_between_runs(torch):
+    """Tuned server grids give the single-grid result to round-off."""
+    import math
+
+    from ns3dperiodic_b200 import Server, Solver, request_steps
+    from ns3dperiodic_b200 import workload as W
+
+    N, Re, T, seed = 64, 100.0, 0.05, 7
+    with Server([N], capacity=[2]) as srv:
+        srv.autotune(reps=3)
+        first = srv.submit([(N, Re, T, seed, 0.0, 1)])
+        assert srv.run() == 1
+        v = srv.result_field(first, N)
+    with Solver(N, N, N) as S:
+        S.set_forcing(S.to_device(W.kolmogorov_forcing(N, N, N)))
+        U, V = S.request_fields(Re, seed)
+        dt = 0.3 * (2.0 * math.pi / N) / (Re / 16.0)
+        S.rk3_ssp_uv(U, V, dt, Re, nsteps=request_steps(N, Re, T))
+        ref = [x.cpu().numpy() for x in V]
+    num = sum(float(np.linalg.norm(a - b)) ** 2 for a, b in zip(v, ref))
+    den = sum(float(np.linalg.norm(b)) ** 2 for b in ref)
+    assert math.sqrt(num / den) < 1e-12
