@@ -17,12 +17,4 @@ cudaError_t run_z(const ZArgs<6, float2>& a, const PassGeom& g, cudaStream_t st)
   return launch_z<true>(a, g, st);
 }
 
-cudaError_t prepare_z(const PassGeom& g) {
-  cudaError_t e;
-  if ((e = launch_z<false>(ZArgs<3>{}, g, nullptr, true)) != cudaSuccess) return e;
-  if ((e = launch_z<true>(ZArgs<6>{}, g, nullptr, true)) != cudaSuccess) return e;
-  if ((e = launch_z<false>(ZArgs<3, float2>{}, g, nullptr, true)) != cudaSuccess) return e;
-  return launch_z<true>(ZArgs<6, float2>{}, g, nullptr, true);
-}
-
 }  // namespace ns3d

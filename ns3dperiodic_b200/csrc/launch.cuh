@@ -168,43 +168,16 @@ cudaError_t launch_inv_y(const InvYArgs<NF, C>& a, const PassGeom& gi, cudaStrea
   }
 }
 
-// Dynamic shared memory of a staged z pass (ZStage): the attribute is set
-// once per instantiation and device (at handle creation through prepare_z, or
-// on the first launch).
-template <int N, int P, bool UV, typename C>
-inline cudaError_t z_stage_attr() {
-  using S = ZStage<N, P, UV, C>;
-  if constexpr (S::ON) {
-    static int done[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    dev &= 63;
-    if (!done[dev]) {
-      const cudaError_t e = cudaFuncSetAttribute(z_kernel<N, P, UV, true, C>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)S::BYTES);
-      if (e != cudaSuccess) return e;
-      done[dev] = 1;
-    }
-  }
-  return cudaSuccess;
-}
-
 template <bool UV, typename C>
-cudaError_t launch_z(const ZArgs<UV ? 6 : 3, C>& a, const PassGeom& gi, cudaStream_t st,
-                     bool prepare_only = false) {
+cudaError_t launch_z(const ZArgs<UV ? 6 : 3, C>& a, const PassGeom& gi, cudaStream_t st) {
   const PassGeom g = planes_geom(gi);
   const long long lines = (long long)g.Nx * g.Ny;
   switch (g.Nz) {
 #define NS3D_CASE(N)                                                               \
   case N: {                                                                        \
     constexpr int P = UV ? p_zuv(N) : p_z(N);                                      \
-    using S = ZStage<N, P, UV, C>;                                                 \
-    const cudaError_t e = z_stage_attr<N, P, UV, C>();                             \
-    if (e != cudaSuccess || prepare_only) return e;                                \
-    z_kernel<N, P, UV, S::ON, C><<<blocks_for(lines, lines_per_cta_z<N, P>()),     \
-                                   kWarpsPerCta * 32, S::ON ? S::BYTES : 0, st>>>( \
-        a, g);                                                                     \
+    z_kernel<N, P, UV, C><<<blocks_for(lines, lines_per_cta_z<N, P>()),           \
+                         kWarpsPerCta * 32, 0, st>>>(a, g);                        \
     return cudaGetLastError();                                                     \
   }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)

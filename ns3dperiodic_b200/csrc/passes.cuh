@@ -136,44 +136,6 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// L2 prefetch of one contiguous run (16-byte aligned, a multiple of 16 bytes)
-// by the bulk-copy unit: no registers, no shared memory, nothing to wait for.
-__device__ __forceinline__ void prefetch_l2_bulk(const void* p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// y passes: L2 prefetch of a group's whole input when the group starts, so
-// the double-buffered cp.async pipeline reads from L2.  Lines b = x*Mz + z;
-// for every y the group's LPC lines are one contiguous run per x plane
-// (elements x*Ny*Mz + y*Mz + z), at most two planes per group here.  FP64
-// lines only (an FP32 run is not a whole number of 16-byte units).
-#ifndef NS3D_L2PF_Y
-#define NS3D_L2PF_Y 0
-#endif
-template <int NY, int LPC, int NFLD, typename C>
-__device__ __forceinline__ void prefetch_y_rows(const C* const* f, int b0, int nb, int Mz,
-                                                int Ny) {
-  if constexpr (sizeof(C) == 16) {
-    int nv = nb - b0;
-    if (nv > LPC) nv = LPC;
-    if (nv <= 0) return;
-    const int x0 = b0 / Mz, z0 = b0 - x0 * Mz;
-    const int n1 = nv < Mz - z0 ? nv : Mz - z0;  // lines in plane x0
-    const int n2 = nv - n1;                      // lines in plane x0 + 1, from z = 0
-    if (n2 > Mz) return;
-    const size_t plane = (size_t)Ny * Mz;
-    for (int r = threadIdx.x; r < NFLD * NY * 2; r += kThreads) {
-      const int seg = r & 1, fy = r >> 1;
-      const int fi = fy / NY, y = fy - fi * NY;
-      const int n = seg ? n2 : n1;
-      if (n == 0) continue;
-      const size_t e = seg ? (size_t)(x0 + 1) * plane + (size_t)y * Mz
-                           : (size_t)x0 * plane + (size_t)y * Mz + z0;
-      prefetch_l2_bulk(f[fi] + e, (unsigned)n * 16u);
-    }
-  }
-}
-
 // Copies the P samples t + T*s (s < P) of one line into a private slot:
 // slot[s*kThreads] <- src[base + (t + T*s) * stride], skipping (zero-filling)
 // the samples whose bit in `keep` is clear.
@@ -410,12 +372,6 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF
     const size_t base = line_base(grp);
     const int gn = grp + gr.step;
     const size_t basen = line_base(gn < g_end ? gn : grp);
-    if constexpr (NS3D_L2PF_Y != 0) {
-      const C* in[2 * NF];
-#pragma unroll
-      for (int f = 0; f < NF; ++f) { in[f] = a.A[f]; in[NF + f] = a.B[f]; }
-      prefetch_y_rows<NY, LM::LPC, 2 * NF>(in, grp * LM::LPC, nb, g.Mz, g.Ny);
-    }
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
       // unit A[f] -> C[f] = IFFT_y A, D[f] = IFFT_y(i ky A)
@@ -487,9 +443,8 @@ struct ZArgs {
 
 // Load W[k] = H(X1)[k] + i H(X2)[k] for positions k = t + T s, where H is the
 // Hermitian extension of a z half-line (H[0], H[N/2] keep only real parts),
-// X = line (optionally times i kz).  SM: the lines are staged in shared
-// memory (plain loads) instead of read from global memory.
-template <int NZ, int P, bool IK1, bool IK2, typename C, bool SM = false>
+// X = line (optionally times i kz).
+template <int NZ, int P, bool IK1, bool IK2, typename C>
 __device__ __forceinline__ void load_pair(C (&w)[P], const C* __restrict__ f1,
                                           const C* __restrict__ f2, size_t base, int t,
                                           RealOf<C> kfz) {
@@ -500,14 +455,8 @@ __device__ __forceinline__ void load_pair(C (&w)[P], const C* __restrict__ f1,
     const int k = t + T * s;
     const bool upper = k > NZ / 2;
     const int q = upper ? NZ - k : k;
-    C c1, c2;
-    if constexpr (SM) {
-      c1 = f1[base + q];
-      c2 = f2[base + q];
-    } else {
-      c1 = __ldg(f1 + base + q);
-      c2 = __ldg(f2 + base + q);
-    }
+    C c1 = __ldg(f1 + base + q);
+    C c2 = __ldg(f2 + base + q);
     const Rt kz = kfz * (Rt)q;
     if constexpr (IK1) c1 = mkc<C>(-c1.y * kz, c1.x * kz);
     if constexpr (IK2) c2 = mkc<C>(-c2.y * kz, c2.x * kz);
@@ -573,78 +522,10 @@ struct ZLaneMap {  // lanes of one line are adjacent: the line is contiguous in 
   }
 };
 
-// Inputs of the z pass staged in shared memory.  The LPC lines of a CTA are
-// consecutive (b = x*Ny + y), so each input field contributes one contiguous
-// run of LPC*Mz elements.  Every thread copies a share of each run with
-// cp.async (element e -> line e / Mz, position e % Mz, lines MZP apart), one
-// commit group per set of fields the transforms consume together, all issued
-// before the first transform: the CTA's whole input is in flight from its
-// first instructions and the transforms of the first fields overlap the
-// arrival of the rest (reading straight from global memory waits for every
-// field pair in turn).  MZP gives the lines that one shared-memory wavefront
-// reads (SLOTS elements) distinct banks.  ON: used when the stage and the
-// kernel's static shared memory leave room for two CTAs per SM (the register
-// limit of the FP64 pass); the 12-point extents (stage of ~110 KB) read
-// global memory directly.
-#ifndef NS3D_ZSTAGE64
-#define NS3D_ZSTAGE64 1
-#endif
-#ifndef NS3D_ZSTAGE32
-#define NS3D_ZSTAGE32 1
-#endif
-constexpr int z_stage_stride(int len, int res, int mod) {
-  return len % mod == res % mod ? len : z_stage_stride(len + 1, res, mod);
-}
-template <int NZ, int P, bool UV, typename C>
-struct ZStage {
-  static constexpr int T = NZ / P;
-  static constexpr int LPC = ZLaneMap<T>::LPC;
-  static constexpr int NF = UV ? 18 : 9;
-  static constexpr int MZ = NZ / 2 + 1;
-  static constexpr int SLOTS = 128 / (int)sizeof(C);
-  static constexpr int MZP = T >= SLOTS ? MZ : z_stage_stride(MZ, T, SLOTS);
-  static constexpr int LEN = LPC * MZP;  // elements per field
-  static constexpr int TOT = LPC * MZ;   // elements copied per field
-  static constexpr size_t BYTES = (size_t)NF * LEN * sizeof(C);
-  static constexpr size_t STATIC =
-      sizeof(C) * ((size_t)LineFFT<NZ, P>::TWLEN + (size_t)LPC * LineFFT<NZ, P>::BUF);
-  static constexpr bool ON = (sizeof(C) == 16 ? NS3D_ZSTAGE64 : NS3D_ZSTAGE32) != 0 &&
-                             BYTES + STATIC <= (size_t)112 * 1024;
-  // stage slot F <- src[off + e] for e < n (the CTA's valid lines), zeros after
-  template <int F>
-  __device__ __forceinline__ static void copy(C* stage, const C* __restrict__ src, size_t off,
-                                              int n) {
-    C* dst = stage + F * LEN;
-    constexpr int NT = kWarpsPerCta * 32;
-#pragma unroll
-    for (int r = 0; r < (TOT + NT - 1) / NT; ++r) {
-      const int e = (int)threadIdx.x + r * NT;
-      if (TOT % NT == 0 || e < TOT) {
-        const int line = e / MZ;
-        const bool ok = e < n;
-        cp_async_elem(dst + line * MZP + (e - line * MZ), src + (ok ? off + e : 0), ok);
-      }
-    }
-  }
-};
-
-// wait until at most PENDING commit groups of the stage are in flight; the
-// barrier publishes every thread's copies to the CTA
-template <bool ST, int PENDING>
-__device__ __forceinline__ void z_stage_wait() {
-  if constexpr (ST) {
-    cp_async_wait<PENDING>();
-    __syncthreads();
-  }
-}
-
 // One component of B(u,v)_i = (v.grad) u_i + (u.grad) v_i in the z pass
 // (convolute_2p3_UV, Source/advection_2_3.cu:414-466); 3 paired C2R lines.
-// Ei, Di, Ci: E, D, C of u_i; Ev, Dv, Cv: those of v_i (global memory, or the
-// shared-memory stage when SM).
-template <int NZ, int P, typename C, bool SM, typename Rt = RealOf<C>>
-__device__ __forceinline__ void uv_component(Rt (&q)[P], const C* Ei, const C* Di, const C* Ci,
-                                             const C* Ev, const C* Dv, const C* Cv, size_t base,
+template <int NZ, int P, typename C, typename Rt = RealOf<C>>
+__device__ __forceinline__ void uv_component(Rt (&q)[P], int i, const ZArgs<6, C>& a, size_t base,
                                              int t, Rt kfz, Rt sc, C* sbuf,
                                              const C* tw_s, const Rt (&ux)[P],
                                              const Rt (&uy)[P], const Rt (&uz)[P],
@@ -653,12 +534,12 @@ __device__ __forceinline__ void uv_component(Rt (&q)[P], const C* Ei, const C* D
   using F = LineFFT<NZ, P>;
   C w[P];
   // (d_x u_i, d_y u_i)
-  load_pair<NZ, P, false, false, C, SM>(w, Ei, Di, base, t, kfz);
+  load_pair<NZ, P, false, false>(w, a.E[i], a.D[i], base, t, kfz);
   F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
   for (int s = 0; s < P; ++s) q[s] = vx[s] * (w[s].x * sc) + vy[s] * (w[s].y * sc);
   // (d_z u_i, d_x v_i)
-  load_pair<NZ, P, true, false, C, SM>(w, Ci, Ev, base, t, kfz);
+  load_pair<NZ, P, true, false>(w, a.C[i], a.E[3 + i], base, t, kfz);
   F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
   for (int s = 0; s < P; ++s) {
@@ -666,117 +547,47 @@ __device__ __forceinline__ void uv_component(Rt (&q)[P], const C* Ei, const C* D
     q[s] = q[s] + ux[s] * (w[s].y * sc);
   }
   // (d_y v_i, d_z v_i)
-  load_pair<NZ, P, false, true, C, SM>(w, Dv, Cv, base, t, kfz);
+  load_pair<NZ, P, false, true>(w, a.D[3 + i], a.C[3 + i], base, t, kfz);
   F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
   for (int s = 0; s < P; ++s) q[s] = q[s] + (uy[s] * (w[s].x * sc) + uz[s] * (w[s].y * sc));
 }
 
-// ST: inputs staged in shared memory (ZStage, dynamic shared memory of
-// ZStage::BYTES); otherwise read from global memory as each pair is needed.
-template <int NZ, int P, bool UV, bool ST, typename C>
+template <int NZ, int P, bool UV, typename C>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<UV ? 6 : 3, C> a, PassGeom g) {
   using F = LineFFT<NZ, P>;
   using Rt = RealOf<C>;
   constexpr int T = F::T;
   using LM = ZLaneMap<T>;
-  using S = ZStage<NZ, P, UV, C>;
-  extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ C tw_s[F::TWLEN];
   __shared__ C sbuf_all[LM::LPC][F::BUF];
-  const int nb = g.Nx * g.Ny;
-  C* stg = reinterpret_cast<C*>(dsm);
-  if constexpr (ST) {
-    // the CTA's lines b0 .. b0+LPC-1, of which n_el / Mz exist
-    const int b0 = blockIdx.x * LM::LPC;
-    const int nl = nb - b0 < LM::LPC ? nb - b0 : LM::LPC;
-    const int n_el = nl * S::MZ;
-    const size_t off = (size_t)b0 * S::MZ;
-    if constexpr (!UV) {
-      // consumed as C0 C1 | C2 | E2 D2 | E0 D0 | E1 D1
-      S::template copy<0>(stg, a.C[0], off, n_el);
-      S::template copy<1>(stg, a.C[1], off, n_el);
-      cp_async_commit();
-      S::template copy<2>(stg, a.C[2], off, n_el);
-      cp_async_commit();
-      S::template copy<3>(stg, a.E[2], off, n_el);
-      S::template copy<4>(stg, a.D[2], off, n_el);
-      cp_async_commit();
-      S::template copy<5>(stg, a.E[0], off, n_el);
-      S::template copy<6>(stg, a.D[0], off, n_el);
-      cp_async_commit();
-      S::template copy<7>(stg, a.E[1], off, n_el);
-      S::template copy<8>(stg, a.D[1], off, n_el);
-      cp_async_commit();
-    } else {
-      // consumed as C0 C1 | C2 C3 | C4 C5 | then per component i:
-      // E_i D_i E_3+i D_3+i (slots 6+4i .. 9+4i)
-      S::template copy<0>(stg, a.C[0], off, n_el);
-      S::template copy<1>(stg, a.C[1], off, n_el);
-      cp_async_commit();
-      S::template copy<2>(stg, a.C[2], off, n_el);
-      S::template copy<3>(stg, a.C[3], off, n_el);
-      cp_async_commit();
-      S::template copy<4>(stg, a.C[4], off, n_el);
-      S::template copy<5>(stg, a.C[5], off, n_el);
-      cp_async_commit();
-      S::template copy<6>(stg, a.E[0], off, n_el);
-      S::template copy<7>(stg, a.D[0], off, n_el);
-      S::template copy<8>(stg, a.E[3], off, n_el);
-      S::template copy<9>(stg, a.D[3], off, n_el);
-      cp_async_commit();
-      S::template copy<10>(stg, a.E[1], off, n_el);
-      S::template copy<11>(stg, a.D[1], off, n_el);
-      S::template copy<12>(stg, a.E[4], off, n_el);
-      S::template copy<13>(stg, a.D[4], off, n_el);
-      cp_async_commit();
-      S::template copy<14>(stg, a.E[2], off, n_el);
-      S::template copy<15>(stg, a.D[2], off, n_el);
-      S::template copy<16>(stg, a.E[5], off, n_el);
-      S::template copy<17>(stg, a.D[5], off, n_el);
-      cp_async_commit();
-    }
-  }
   F::load_tw(tw_s, a.tw);
   int li, t;
   LM::get(li, t);
+  const int nb = g.Nx * g.Ny;
   const int b = blockIdx.x * LM::LPC + li;
   const bool valid = b < nb;
   const size_t base = (size_t)(valid ? b : 0) * g.Mz;
-  // where load_pair reads: the stage (line li) or global memory (line b)
-  const size_t sb = ST ? (size_t)li * S::MZP : base;
   C* sbuf = sbuf_all[li];
   const Rt sc = (Rt)g.inv_vol;
   const Rt kfz = (Rt)g.kfz;
   C w[P];
   Rt ux[P], uy[P], uz[P], q0[P], q1[P], q2[P];
   if constexpr (!UV) {
-    const C* pC[3] = {a.C[0], a.C[1], a.C[2]};
-    const C* pD[3] = {a.D[0], a.D[1], a.D[2]};
-    const C* pE[3] = {a.E[0], a.E[1], a.E[2]};
-    if constexpr (ST) {
-      pC[0] = stg; pC[1] = stg + S::LEN; pC[2] = stg + 2 * S::LEN;
-      pE[2] = stg + 3 * S::LEN; pD[2] = stg + 4 * S::LEN;
-      pE[0] = stg + 5 * S::LEN; pD[0] = stg + 6 * S::LEN;
-      pE[1] = stg + 7 * S::LEN; pD[1] = stg + 8 * S::LEN;
-    }
     // Q_z first, so at most five real lines (u_x, u_y, u_z and two products)
     // are live at any time.
     // (u_x, u_y)
-    z_stage_wait<ST, 4>();
-    load_pair<NZ, P, false, false, C, ST>(w, pC[0], pC[1], sb, t, kfz);
+    load_pair<NZ, P, false, false>(w, a.C[0], a.C[1], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { ux[s] = w[s].x * sc; uy[s] = w[s].y * sc; }
     // (u_z, d_z u_z) from one field
-    z_stage_wait<ST, 3>();
-    load_pair<NZ, P, false, true, C, ST>(w, pC[2], pC[2], sb, t, kfz);
+    load_pair<NZ, P, false, true>(w, a.C[2], a.C[2], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { uz[s] = w[s].x * sc; q2[s] = w[s].y * sc; }
     // Q_z = u_x d_x u_z + u_y d_y u_z + u_z d_z u_z  (calc_vels_nabla_vels)
-    z_stage_wait<ST, 2>();
-    load_pair<NZ, P, false, false, C, ST>(w, pE[2], pD[2], sb, t, kfz);
+    load_pair<NZ, P, false, false>(w, a.E[2], a.D[2], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s)
@@ -793,18 +604,16 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
       }
     }
     // (d_z u_x, d_z u_y)
-    load_pair<NZ, P, true, true, C, ST>(w, pC[0], pC[1], sb, t, kfz);
+    load_pair<NZ, P, true, true>(w, a.C[0], a.C[1], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { q0[s] = w[s].x * sc; q1[s] = w[s].y * sc; }
-    z_stage_wait<ST, 1>();
-    load_pair<NZ, P, false, false, C, ST>(w, pE[0], pD[0], sb, t, kfz);
+    load_pair<NZ, P, false, false>(w, a.E[0], a.D[0], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s)
       q0[s] = ux[s] * (w[s].x * sc) + uy[s] * (w[s].y * sc) + uz[s] * q0[s];
-    z_stage_wait<ST, 0>();
-    load_pair<NZ, P, false, false, C, ST>(w, pE[1], pD[1], sb, t, kfz);
+    load_pair<NZ, P, false, false>(w, a.E[1], a.D[1], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s)
@@ -814,57 +623,39 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
     for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], q1[s]);
     F::template run<-1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
     store_pair_spectrum<NZ, P>(w, sbuf, t, a.Qh[0], a.Qh[1], base, valid);
+    return;
   } else {
     // B(u,v)_i = (v.grad) u_i + (u.grad) v_i; fields 0..2 are u, 3..5 are v
-    const C* pC[6];
-    const C* pD[6];
-    const C* pE[6];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      pC[i] = ST ? stg + i * S::LEN : a.C[i];
-      const int j = i < 3 ? 6 + 4 * i : 8 + 4 * (i - 3);  // stage slot of E_i
-      pE[i] = ST ? stg + j * S::LEN : a.E[i];
-      pD[i] = ST ? stg + (j + 1) * S::LEN : a.D[i];
-    }
     Rt vx[P], vy[P], vz[P];
-    z_stage_wait<ST, 5>();
-    load_pair<NZ, P, false, false, C, ST>(w, pC[0], pC[1], sb, t, kfz);
+    load_pair<NZ, P, false, false>(w, a.C[0], a.C[1], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { ux[s] = w[s].x * sc; uy[s] = w[s].y * sc; }
-    z_stage_wait<ST, 4>();
-    load_pair<NZ, P, false, false, C, ST>(w, pC[2], pC[3], sb, t, kfz);
+    load_pair<NZ, P, false, false>(w, a.C[2], a.C[3], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { uz[s] = w[s].x * sc; vx[s] = w[s].y * sc; }
-    z_stage_wait<ST, 3>();
-    load_pair<NZ, P, false, false, C, ST>(w, pC[4], pC[5], sb, t, kfz);
+    load_pair<NZ, P, false, false>(w, a.C[4], a.C[5], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { vy[s] = w[s].x * sc; vz[s] = w[s].y * sc; }
-    z_stage_wait<ST, 2>();
-    uv_component<NZ, P, C, ST>(q0, pE[0], pD[0], pC[0], pE[3], pD[3], pC[3], sb, t, kfz, sc,
-                               sbuf, tw_s, ux, uy, uz, vx, vy, vz);
-    z_stage_wait<ST, 1>();
-    uv_component<NZ, P, C, ST>(q1, pE[1], pD[1], pC[1], pE[4], pD[4], pC[4], sb, t, kfz, sc,
-                               sbuf, tw_s, ux, uy, uz, vx, vy, vz);
-    z_stage_wait<ST, 0>();
-    uv_component<NZ, P, C, ST>(q2, pE[2], pD[2], pC[2], pE[5], pD[5], pC[5], sb, t, kfz, sc,
-                               sbuf, tw_s, ux, uy, uz, vx, vy, vz);
-    // forward R2C along z: (Q0, Q1) packed, then Q2 alone
+    uv_component<NZ, P>(q0, 0, a, base, t, kfz, sc, sbuf, tw_s, ux, uy, uz, vx, vy, vz);
+    uv_component<NZ, P>(q1, 1, a, base, t, kfz, sc, sbuf, tw_s, ux, uy, uz, vx, vy, vz);
+    uv_component<NZ, P>(q2, 2, a, base, t, kfz, sc, sbuf, tw_s, ux, uy, uz, vx, vy, vz);
+  }
+  // forward R2C along z: (Q0, Q1) packed, then Q2 alone
 #pragma unroll
-    for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], q1[s]);
-    F::template run<-1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
-    store_pair_spectrum<NZ, P>(w, sbuf, t, a.Qh[0], a.Qh[1], base, valid);
+  for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], q1[s]);
+  F::template run<-1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
+  store_pair_spectrum<NZ, P>(w, sbuf, t, a.Qh[0], a.Qh[1], base, valid);
 #pragma unroll
-    for (int s = 0; s < P; ++s) w[s] = mkc<C>(q2[s], (Rt)0);
-    F::template run<-1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
-    if (valid) {
+  for (int s = 0; s < P; ++s) w[s] = mkc<C>(q2[s], (Rt)0);
+  F::template run<-1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
+  if (valid) {
 #pragma unroll
-      for (int s = 0; s < P; ++s) {
-        const int k = t + T * s;
-        if (k <= NZ / 2) a.Qh[2][base + k] = w[s];
-      }
+    for (int s = 0; s < P; ++s) {
+      const int k = t + T * s;
+      if (k <= NZ / 2) a.Qh[2][base + k] = w[s];
     }
   }
 }
@@ -912,10 +703,6 @@ __global__ void __launch_bounds__(kThreads, kMinCtasXY) fwd_y_kernel(FwdYArgs<C>
     const size_t base = line_base(grp);
     const int gn = grp + gr.step;
     const size_t basen = line_base(gn < g_end ? gn : grp);
-    if constexpr (NS3D_L2PF_Y != 0) {
-      const C* in[3] = {a.Q[0], a.Q[1], a.Q[2]};
-      prefetch_y_rows<NY, LM::LPC, 3>(in, grp * LM::LPC, nb, g.Mz, g.Ny);
-    }
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
       const C* cur = pf + ub * (P * kThreads);
@@ -1221,6 +1008,12 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs<C>& a, const PassGeom&
       a.out[c][idx] = r;
     }
   }
+}
+
+// L2 prefetch of one contiguous run (16-byte aligned, a multiple of 16 bytes)
+// by the bulk-copy unit: no registers, no shared memory, nothing to wait for.
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
 }
 
 // The update at the end of a fwd_x group reads, for every x, the state (and

@@ -362,7 +362,6 @@ ns3d_status create_solver(int batch, int Nx, int Ny, int Nz, double Lx, double L
   }
   if ((e = ns3d::prepare_xy(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   if ((e = ns3d::prepare_fwdx(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
-  if ((e = ns3d::prepare_z(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   if ((e = ns3d::prepare_fft3d(h->geom)) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(NS3D_ERR_CUDA);
   *out = h;
