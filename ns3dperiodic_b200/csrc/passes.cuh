@@ -893,6 +893,21 @@ enum UpdateMode : int {
   kConvOut = 3,   // out = Qhat with Re(Qhat) = 0, Qhat(0) = 0 (calculate_convolution_2p3)
 };
 
+// points of the fwd_x update whose state samples are loaded together in the
+// plain explicit form with FP64 lines (the combining form, which also loads
+// the RK partner, the RHS / implicit forms, the FP32 lines and lines spread
+// over the CTA keep one point's loads where they are used: chunks spill there).  B200, per launch of the plain form: 2 points
+// 128^3 64.5 -> 59.4 us, 256^3 455 -> 415 us; 4 points 60.0 / 444-449 us.
+#ifndef NS3D_FX_CHUNK
+#define NS3D_FX_CHUNK 2
+#endif
+// a divisor of P near NS3D_FX_CHUNK (P is 2^k or 3 * 2^k)
+__host__ __device__ constexpr int fx_chunk(int P) {
+  return NS3D_FX_CHUNK >= P ? P
+         : P % NS3D_FX_CHUNK == 0 ? NS3D_FX_CHUNK
+         : (NS3D_FX_CHUNK >= 6 && P % 6 == 0) ? 6 : 3;
+}
+
 template <typename Cx = double2>
 struct FwdXArgs {
   const Cx* Qh[3];
@@ -958,54 +973,80 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs<C>& a, const PassGeom&
   const bool dense_f = a.fd[0] != nullptr;
   const double dt = a.dtRe ? __ldg(a.dtRe + 2 * inst) : a.dt;
   const double Re = a.dtRe ? __ldg(a.dtRe + 2 * inst + 1) : a.Re;
+  // The state samples of CH points are loaded before any of them is
+  // updated: the stores may alias the loads (an in-place update), so the
+  // compiler keeps every load behind the previous point's store, and point by
+  // point each load would wait a full memory round trip.  Each element is
+  // still read before it is written, by the same thread.
+  constexpr int CH =
+      (COMBINE || MODE != kExplicit || sizeof(C) != 16 || LaneMap<T>::kSpread) ? 1 : fx_chunk(P);
+  static_assert(P % CH == 0, "update chunk");
 #pragma unroll
-  for (int s = 0; s < P; ++s) {
-    const int x = t + T * s;
-    const size_t fi = (size_t)x * nlines + L;  // index inside the instance (forcing)
-    const size_t idx = off + (size_t)x * nlines;
-    const double kx = g.kfx * (double)signed_idx(x, NX);
-    const double kk = kx * kx + ky * ky + kz * kz;
-    // set_to_zero_real: Re(Qh) = 0 everywhere, Qh(0,0,0) = 0
-    const bool origin = (x == 0) && (L == 0);
-    const double Q0 = origin ? 0.0 : qi[0][s];
-    const double Q1 = origin ? 0.0 : qi[1][s];
-    const double Q2 = origin ? 0.0 : qi[2][s];
-    // AM.Q - Q with AM_ij = k_i k_j / |k|^2 (0 at k = 0); imaginary part only
-    const double kq = kk > 0.0 ? (kx * Q0 + ky * Q1 + kz * Q2) / kk : 0.0;
-    const double p[3] = {kx * kq - Q0, ky * kq - Q1, kz * kq - Q2};
-    double2 f[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
-    if constexpr (MODE != kImplicit) {
-      if (dense_f) {
+  for (int s0 = 0; s0 < P; s0 += CH) {
+    // CH == 1: each sample is loaded where it is used (fewest live registers)
+    double2 us[3][CH];
+    double2 un[3][COMBINE ? CH : 1];
+    if constexpr (CH > 1) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) f[c] = __ldg(a.fd[c] + fi);
-      } else {
-        for (int e = 0; e < a.fnnz; ++e) {
-          if (__ldg(a.fidx + e) == (int)fi) {
+      for (int j = 0; j < CH; ++j) {
+        const size_t idx = off + (size_t)(t + T * (s0 + j)) * nlines;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) f[c] = cadd(f[c], __ldg(a.fval + 3 * e + c));
-          }
+        for (int c = 0; c < 3; ++c) {
+          us[c][j] = __ldg(a.us[c] + idx);
+          if constexpr (COMBINE) un[c][j] = __ldg(a.un[c] + idx);
         }
       }
     }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const double2 u = __ldg(a.us[c] + idx);
-      double2 r;
-      if constexpr (MODE == kExplicit) {
-        const double G = 1.0 - kk * dt / Re;
-        r = make_double2(G * u.x + dt * f[c].x, dt * p[c] + G * u.y + dt * f[c].y);
-      } else if constexpr (MODE == kRhs) {
-        const double G = -kk / Re;
-        r = make_double2(G * u.x + f[c].x, p[c] + G * u.y + f[c].y);
-      } else {
-        const double G = 1.0 + kk * dt / Re;
-        r = make_double2(u.x / G, (dt * p[c] + u.y) / G);
+    for (int j = 0; j < CH; ++j) {
+      const int s = s0 + j;
+      const int x = t + T * s;
+      const size_t fi = (size_t)x * nlines + L;  // index inside the instance (forcing)
+      const size_t idx = off + (size_t)x * nlines;
+      const double kx = g.kfx * (double)signed_idx(x, NX);
+      const double kk = kx * kx + ky * ky + kz * kz;
+      // set_to_zero_real: Re(Qh) = 0 everywhere, Qh(0,0,0) = 0
+      const bool origin = (x == 0) && (L == 0);
+      const double Q0 = origin ? 0.0 : qi[0][s];
+      const double Q1 = origin ? 0.0 : qi[1][s];
+      const double Q2 = origin ? 0.0 : qi[2][s];
+      // AM.Q - Q with AM_ij = k_i k_j / |k|^2 (0 at k = 0); imaginary part only
+      const double kq = kk > 0.0 ? (kx * Q0 + ky * Q1 + kz * Q2) / kk : 0.0;
+      const double p[3] = {kx * kq - Q0, ky * kq - Q1, kz * kq - Q2};
+      double2 f[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+      if constexpr (MODE != kImplicit) {
+        if (dense_f) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) f[c] = __ldg(a.fd[c] + fi);
+        } else {
+          for (int e = 0; e < a.fnnz; ++e) {
+            if (__ldg(a.fidx + e) == (int)fi) {
+#pragma unroll
+              for (int c = 0; c < 3; ++c) f[c] = cadd(f[c], __ldg(a.fval + 3 * e + c));
+            }
+          }
+        }
       }
-      if constexpr (COMBINE) {
-        const double2 n = __ldg(a.un[c] + idx);
-        r = make_double2(a.ca * n.x + a.cb * r.x, a.ca * n.y + a.cb * r.y);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double2 u = CH > 1 ? us[c][j] : __ldg(a.us[c] + idx);
+        double2 r;
+        if constexpr (MODE == kExplicit) {
+          const double G = 1.0 - kk * dt / Re;
+          r = make_double2(G * u.x + dt * f[c].x, dt * p[c] + G * u.y + dt * f[c].y);
+        } else if constexpr (MODE == kRhs) {
+          const double G = -kk / Re;
+          r = make_double2(G * u.x + f[c].x, p[c] + G * u.y + f[c].y);
+        } else {
+          const double G = 1.0 + kk * dt / Re;
+          r = make_double2(u.x / G, (dt * p[c] + u.y) / G);
+        }
+        if constexpr (COMBINE) {
+          const double2 n = CH > 1 ? un[c][j] : __ldg(a.un[c] + idx);
+          r = make_double2(a.ca * n.x + a.cb * r.x, a.ca * n.y + a.cb * r.y);
+        }
+        a.out[c][idx] = r;
       }
-      a.out[c][idx] = r;
     }
   }
 }
@@ -1021,7 +1062,8 @@ __device__ __forceinline__ void prefetch_l2_bulk(const void* p, unsigned bytes) 
 // contiguous row of LPC x 16 bytes per (x, field).  Requesting those rows into
 // L2 when the group starts lets the group's three transforms cover their DRAM
 // latency, and the update's loads then hit L2.  A group whose lines straddle
-// two instances of a batch is not prefetched.
+// two instances of a batch is not prefetched, nor are the groups of lines
+// spread over the CTA (LPC <= 4: rows of 64 bytes or less).
 template <int NX, int LPC, bool COMBINE, typename C, typename Off>
 __device__ __forceinline__ void prefetch_update_rows(const FwdXArgs<C>& a, int G0, int tlines,
                                                      int nlines, Off line_off) {
@@ -1075,7 +1117,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtasFwdX) fwd_x_kernel(FwdXArgs<
     const int inst = Gc / nlines;
     const int gn = grp + gr.step;
     const int Gn = gn * LM::LPC + li;
-    if constexpr (MODE != kConvOut)
+    if constexpr (MODE != kConvOut && !LM::kSpread)
       prefetch_update_rows<NX, LM::LPC, COMBINE>(a, grp * LM::LPC, tlines, nlines, line_off);
     fwd_x_line<NX, P, MODE, COMBINE, C>(a, g, t, Gc - inst * nlines, line_off(Gc), inst, valid,
                                      sbuf, tw_s, pf, ub, gn < g_end,
