@@ -894,10 +894,11 @@ enum UpdateMode : int {
 };
 
 // points of the fwd_x update whose state samples are loaded together in the
-// plain explicit form with FP64 lines (the combining form, which also loads
-// the RK partner, the RHS / implicit forms, the FP32 lines and lines spread
-// over the CTA keep one point's loads where they are used: chunks spill there).  B200, per launch of the plain form: 2 points
-// 128^3 64.5 -> 59.4 us, 256^3 455 -> 415 us; 4 points 60.0 / 444-449 us.
+// plain explicit form (the combining form, which also loads the RK partner,
+// the RHS / implicit forms and lines spread over the CTA keep one point's
+// loads where they are used: chunks spill there).  B200, per launch of the
+// plain form: 2 points 128^3 64.5 -> 59.4 us, 256^3 455 -> 415 us (FP32
+// lines 419 -> 367 us); 4 points 60.0 / 444-449 us.
 #ifndef NS3D_FX_CHUNK
 #define NS3D_FX_CHUNK 2
 #endif
@@ -979,7 +980,7 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs<C>& a, const PassGeom&
   // point each load would wait a full memory round trip.  Each element is
   // still read before it is written, by the same thread.
   constexpr int CH =
-      (COMBINE || MODE != kExplicit || sizeof(C) != 16 || LaneMap<T>::kSpread) ? 1 : fx_chunk(P);
+      (COMBINE || MODE != kExplicit || LaneMap<T>::kSpread) ? 1 : fx_chunk(P);
   static_assert(P % CH == 0, "update chunk");
 #pragma unroll
   for (int s0 = 0; s0 < P; s0 += CH) {
