@@ -1,12 +1,12 @@
 #!/usr/bin/env python
 """Benchmark of the FP64 pseudo-spectral SSP-RK3 step (forced Kolmogorov flow).
 
-Workload (default): N^3 = 128^3 on the 2pi-periodic box, f = (sin 4y, 0, 0),
-Re = 200, laminar profile plus a seeded 1e-3 divergence-free perturbation,
+Workload (default): N^3 = 256^3 on the 2pi-periodic box, f = (sin 4y, 0, 0),
+Re = 400 (200 below 256^3), laminar profile plus a seeded 1e-3 divergence-free perturbation,
 dt from CFL 0.3 on the laminar peak velocity, FP64 throughout.  A "step" is
 one RK3_SSP step (3 right-hand sides).  The metric is RK3 steps/s.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--N 128]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--N 256]
   python bench.py --workload arnoldi [--n-arnoldi 2300000] [--m-arnoldi 30] [...]
 
 --impl ours       : the CUDA library (libns3d_b200.so) through its C ABI.
@@ -60,8 +60,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--N", type=int, default=128)
-    ap.add_argument("--Re", type=float, default=200.0)
+    ap.add_argument("--N", type=int, default=256)
+    ap.add_argument("--Re", type=float, default=None,
+                    help="default: 400 for the rk3 workload from 256^3 (the precision-mode "
+                         "configuration), else 200")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
@@ -84,7 +86,10 @@ def parse():
     ap.add_argument("--ira-cycles", type=int, default=20, help="ira: restart cycles per run")
     ap.add_argument("--n-arnoldi", type=int, default=2300000)
     ap.add_argument("--m-arnoldi", type=int, default=30)
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.Re is None:
+        a.Re = 400.0 if (a.workload == "rk3" and a.N >= 256) else 200.0
+    return a
 
 
 # ---------------------------------------------------------------------------
@@ -1077,8 +1082,9 @@ def run_ours_ensemble(args, world, rank, local, pg):
     value = world * len(inst) / (ms / 1e3)
     serial = len(inst) / (t_serial / 1e3)
     return {
-        "metric": "mixed-N ensemble solves/s (64 Kolmogorov instances, N in {32,48,64,96,128}, "
-                  f"Re in [50,500], 200 RK3 steps each, {args.precision.upper()})",
+        "metric": f"mixed-N ensemble solves/s ({len(inst)} Kolmogorov instances, N in "
+                  f"{{32,48,64,96,128}}, Re in [50,500], {steps} RK3 steps each, "
+                  f"{args.precision.upper()})",
         "value": round(value, 3),
         "unit": "solves/s",
         "n_gpus": world,
@@ -1157,8 +1163,8 @@ def run_reference_ensemble(args, world, rank, local, pg):
     clocks = sampler.stop()
     value = len(inst) / (total_ms / 1e3)
     return {"impl": "reference",
-            "metric": "mixed-N ensemble solves/s (64 Kolmogorov instances, N in {32,48,64,96,128}, "
-                      "Re in [50,500], 200 RK3 steps each, FP64)",
+            "metric": f"mixed-N ensemble solves/s ({len(inst)} Kolmogorov instances, N in "
+                      f"{{32,48,64,96,128}}, Re in [50,500], {steps} RK3 steps each, FP64)",
             "value": round(value, 3), "unit": "solves/s", "n_gpus": 1, "steps": steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / steps, 5),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",

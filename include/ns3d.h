@@ -517,12 +517,15 @@ int ns3d_request_steps(int N, double Re, double T);
  * held from the first call on a device until the process exits).  The first
  * call on each device looks up that array's device address and uploads the
  * grid's twiddle and mask tables; make that first call before capturing the
- * stream.  Later calls with the same grid reuse the tables.  All calls on a
- * device share the array, so calls that overlap on the GPU race: serialise
- * them (one stream, one host thread).  Runs on `stream` (cudaStream_t, 0 for
- * the legacy default stream) on the current device.  Returns
- * NS3D_ERR_BAD_ARG when Nx*Ny*(Nz/2+1) > NS3D_NOALLOC_MAX_POINTS (nothing is
- * launched), NS3D_ERR_UNSUPPORTED for an extent without a compiled plan. */
+ * stream.  Later calls with the same grid and box reuse the tables; a call
+ * whose grid or box differs from the previous call's on that device uploads
+ * new tables and synchronises `stream`, which is refused (NS3D_ERR_BAD_ARG,
+ * nothing launched) while `stream` is being captured.  All calls on a device
+ * share the array, so calls that overlap on the GPU race: serialise them
+ * (one stream, one host thread).  Runs on `stream` (cudaStream_t, 0 for the
+ * legacy default stream) on the current device.  Returns NS3D_ERR_BAD_ARG
+ * when Nx*Ny*(Nz/2+1) > NS3D_NOALLOC_MAX_POINTS (nothing is launched),
+ * NS3D_ERR_UNSUPPORTED for an extent without a compiled plan. */
 ns3d_status ns3d_convolution_noalloc(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
                                      const ns3d_complex* ux, const ns3d_complex* uy,
                                      const ns3d_complex* uz, ns3d_complex* Qx, ns3d_complex* Qy,

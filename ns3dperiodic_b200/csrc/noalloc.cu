@@ -25,6 +25,7 @@
 
 #include "../../include/ns3d.h"
 #include "dispatch.h"
+#include "launch.cuh"
 
 namespace {
 
@@ -35,6 +36,11 @@ constexpr long long kTwWords = 3 * kMaxExtent;               // twiddles of x, y
 constexpr long long kQcutWords = kMaxPoints / 4;             // uint16 cut-offs, 8 per word
 constexpr long long kWords = kFieldWords + kTwWords + kQcutWords;
 static_assert(kWords * 16 == NS3D_NOALLOC_SCRATCH_BYTES, "scratch size and header disagree");
+// the twiddle slots hold kMaxExtent entries per direction: every compiled
+// extent must fit (a build that adds a larger extent must raise kMaxExtent)
+#define NS3D_NOALLOC_EXTENT_FITS(N) static_assert(N <= kMaxExtent, "extent above kMaxExtent");
+NS3D_FOR_EACH_EXTENT(NS3D_NOALLOC_EXTENT_FITS)
+#undef NS3D_NOALLOC_EXTENT_FITS
 
 // The scratch itself.  Host code must not use this name as an address: on the
 // host it is only a stand-in, so it is resolved with cudaGetSymbolAddress.
@@ -66,6 +72,7 @@ extern "C" ns3d_status ns3d_convolution_noalloc(int Nx, int Ny, int Nz, double L
     return NS3D_ERR_BAD_ARG;
   if (!ns3d::extent_supported(Nx) || !ns3d::extent_supported(Ny) || !ns3d::extent_supported(Nz))
     return NS3D_ERR_UNSUPPORTED;
+  if (Nx > kMaxExtent || Ny > kMaxExtent || Nz > kMaxExtent) return NS3D_ERR_UNSUPPORTED;
   const int Mz = Nz / 2 + 1;
   const long long nc = (long long)Nx * Ny * Mz;
   if (nc > kMaxPoints) return NS3D_ERR_BAD_ARG;  // larger than the fixed scratch
@@ -92,6 +99,14 @@ extern "C" ns3d_status ns3d_convolution_noalloc(int Nx, int Ny, int Nz, double L
   // wave-number tables: refreshed only when the grid differs from the last call
   if (slot.Nx != Nx || slot.Ny != Ny || slot.Nz != Nz || slot.Lx != Lx || slot.Ly != Ly ||
       slot.Lz != Lz) {
+    // the refresh copies from pageable host memory and synchronises the
+    // stream, which a stream capture does not allow: refuse it there
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+      cudaGetLastError();
+      return NS3D_ERR_CUDA;
+    }
+    if (cap != cudaStreamCaptureStatusNone) return NS3D_ERR_BAD_ARG;
     if (ns3d_mask_cutoff(Nx, Ny, Nz, Lx, Ly, Lz, g_host_qcut) != NS3D_OK) return NS3D_ERR_BAD_ARG;
     const int ext[3] = {Nx, Ny, Nz};
     for (int d = 0; d < 3; ++d) {
