@@ -45,7 +45,8 @@ typedef enum ns3d_status {
   NS3D_ERR_CUDA = 4,        /* a CUDA launch or API call failed (see ns3d_last_error) */
   NS3D_ERR_NONFINITE = 5,   /* a diagnostic reduction met NaN/Inf */
   NS3D_ERR_TIMEOUT = 6,     /* a bounded device wait gave up */
-  NS3D_ERR_NOT_CONVERGED = 7 /* an inner linear solve stopped without converging */
+  NS3D_ERR_NOT_CONVERGED = 7, /* an inner linear solve stopped without converging */
+  NS3D_ERR_CANCELLED = 8      /* a server request was cancelled (ns3d_server_cancel) */
 } ns3d_status;
 
 /* ----------------------------------------------------------------------- */
@@ -464,8 +465,32 @@ typedef struct ns3d_result {
   int steps;
   double arrival, admitted, done; /* -1: not yet */
   double v_norm;
-  int status; /* -1 pending, NS3D_OK, NS3D_ERR_NONFINITE */
+  int status; /* -1 pending, NS3D_OK, NS3D_ERR_NONFINITE, NS3D_ERR_CANCELLED */
 } ns3d_result;
+
+/* A request that brings its own fields: the work a Newton-Krylov,
+ * BiCGStab(L) or Arnoldi caller hands out with every matrix-vector product
+ * (NSCallMatrixVector_exponential, Source/NS3D_periodic.cu:444-470, and the
+ * Jacobian maps Source/Arnoldi/Newton.cu:40-47 calls): `steps` RK3_SSP_UV
+ * steps of the base state u and tangent v with time step dt and Reynolds
+ * number Re, under the grid's forcing (ns3d_server_set_forcing; sin(4y) x
+ * unless set).  u_in and v_in are read when the request is admitted; v_out
+ * (and u_out, unless null) are written when it completes, before its status
+ * leaves -1.  The buffers hold [N][N][N/2+1] complex values each, in device
+ * memory or in host memory cudaMemcpyAsync can read and write (pinned), and
+ * must stay valid until the request is done; v_out may be v_in and u_out
+ * u_in.  arrival < 0 stands for the server clock at submission (at least the
+ * previous request's arrival).  The result's T is steps * dt. */
+typedef struct ns3d_field_request {
+  int N;
+  double Re, dt;
+  int steps;
+  const ns3d_complex* u_in[3];
+  const ns3d_complex* v_in[3];
+  ns3d_complex* u_out[3];
+  ns3d_complex* v_out[3];
+  double arrival;
+} ns3d_field_request;
 
 ns3d_status ns3d_server_create(const int* Ns, int nN, const int* capacity, double hbm_fraction,
                                ns3d_server** out);
@@ -483,6 +508,25 @@ ns3d_status ns3d_server_autotune(ns3d_server* s, int reps);
 ns3d_status ns3d_server_stats(const ns3d_server* s, int N, long long* instance_steps);
 /* Queues n requests (ids first_id .. first_id + n - 1). */
 ns3d_status ns3d_server_submit(ns3d_server* s, const ns3d_request* r, int n, long long* first_id);
+/* Queues n requests that carry their own fields (ns3d_field_request); they
+ * share the ids, the arrival order and the slots of ns3d_server_submit's. */
+ns3d_status ns3d_server_submit_fields(ns3d_server* s, const ns3d_field_request* r, int n,
+                                      long long* first_id);
+/* Forcing of grid N's base flow (device memory, [N][N][N/2+1] each), for the
+ * requests admitted from now on; between runs. */
+ns3d_status ns3d_server_set_forcing(ns3d_server* s, int N, const ns3d_complex* fx,
+                                    const ns3d_complex* fy, const ns3d_complex* fz);
+/* Cancels a request that has not finished: a queued request never starts, an
+ * admitted one leaves its slot at its grid's next step boundary, and the slot
+ * goes to the next arrival.  Its status becomes NS3D_ERR_CANCELLED (its
+ * output fields are not written).  The one call that may come from another
+ * host thread while ns3d_server_run runs.  NS3D_ERR_BAD_ARG for an unknown
+ * or finished request. */
+ns3d_status ns3d_server_cancel(ns3d_server* s, long long id);
+/* Runs the engine like ns3d_server_run but returns as soon as request `id`
+ * is done (other requests progress meanwhile and keep their slots). */
+ns3d_status ns3d_server_run_until(ns3d_server* s, long long id, double max_seconds,
+                                  int* completed);
 /* Runs the engine on the calling thread until every submitted request is
  * done or max_seconds have passed (then nothing more is admitted or launched
  * and the steps in flight are finished; unfinished requests keep their slots
@@ -681,6 +725,21 @@ void ns3d_map_rhs(void* user, void* in, void* out);
  * 3*Nc-3 (Source/NS3D_periodic.cu:1717); this map uses the reduced packing
  * consistently. */
 void ns3d_map_exponential(void* user, void* in, void* out);
+
+/* The exponential map served by a request server: what ns3d_map_exponential
+ * computes (in -> v, `steps` RK3_SSP_UV steps of (u, v), v -> out; the base
+ * flow u advances with every call), with the steps run by `server` as a
+ * field request (ns3d_server_submit_fields + ns3d_server_run_until), so the
+ * matrix-vector products of a Krylov driver share the device with the
+ * server's other requests.  `solver` (a handle of the server's grid N)
+ * packs and unpacks the reduced vectors; with the server's default tiles and
+ * the same forcing the result equals ns3d_map_exponential's bit for bit. */
+typedef struct ns3d_served_map_context {
+  ns3d_map_context map; /* solver, base flow u, tangent v, dt, Re, steps; status */
+  ns3d_server* server;
+  long long requests;   /* out: requests served so far */
+} ns3d_served_map_context;
+void ns3d_map_exponential_served(void* user, void* in, void* out);
 
 /* Shift-invert maps of the matrix-exponent IRA
  * (Implicit_restart_Arnoldi_GPU_data_Matrix_Exponent,

@@ -21,6 +21,7 @@ STATUS = {
     5: "non-finite value",
     6: "device wait timed out",
     7: "inner linear solve did not converge",
+    8: "request cancelled",
 }
 
 # every symbol include/ns3d.h declares
@@ -57,6 +58,8 @@ EXPORTS = (
     "ns3d_server_create", "ns3d_server_destroy", "ns3d_server_last_error",
     "ns3d_server_capacity", "ns3d_server_stats", "ns3d_server_set_precision", "ns3d_server_submit", "ns3d_server_run", "ns3d_server_results",
     "ns3d_server_result_field", "ns3d_request_fields", "ns3d_request_steps",
+    "ns3d_server_submit_fields", "ns3d_server_set_forcing", "ns3d_server_cancel",
+    "ns3d_server_run_until", "ns3d_map_exponential_served",
 )
 
 class Request(ctypes.Structure):
@@ -74,6 +77,14 @@ class Result(ctypes.Structure):
                 ("v_norm", ctypes.c_double), ("status", ctypes.c_int)]
 
 
+class FieldRequest(ctypes.Structure):
+    """ns3d_field_request of include/ns3d.h."""
+    _fields_ = [("N", ctypes.c_int), ("Re", ctypes.c_double), ("dt", ctypes.c_double),
+                ("steps", ctypes.c_int), ("u_in", ctypes.c_void_p * 3),
+                ("v_in", ctypes.c_void_p * 3), ("u_out", ctypes.c_void_p * 3),
+                ("v_out", ctypes.c_void_p * 3), ("arrival", ctypes.c_double)]
+
+
 # the matrix-vector callback type of ns3d_arnoldi: void (*)(void*, void*, void*)
 MAP_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
 
@@ -85,6 +96,12 @@ class MapContext(ctypes.Structure):
                 ("vx", ctypes.c_void_p), ("vy", ctypes.c_void_p), ("vz", ctypes.c_void_p),
                 ("dt", ctypes.c_double), ("Re", ctypes.c_double), ("tau", ctypes.c_double),
                 ("steps", ctypes.c_int), ("status", ctypes.c_int)]
+
+
+class ServedMapContext(ctypes.Structure):
+    """ns3d_served_map_context of include/ns3d.h."""
+    _fields_ = [("map", MapContext), ("server", ctypes.c_void_p),
+                ("requests", ctypes.c_longlong)]
 
 
 class ShiftInvertContext(ctypes.Structure):
@@ -236,6 +253,11 @@ def _sig(lib):
         "ns3d_server_result_field": ([_P, ctypes.c_longlong, _P, _P, _P], c_int),
         "ns3d_request_fields": ([_P, c_double, ctypes.c_ulonglong] + [_P] * 6, c_int),
         "ns3d_request_steps": ([c_int, c_double, c_double], c_int),
+        "ns3d_server_submit_fields": ([_P, _P, c_int, _P], c_int),
+        "ns3d_server_set_forcing": ([_P, c_int, _P, _P, _P], c_int),
+        "ns3d_server_cancel": ([_P, ctypes.c_longlong], c_int),
+        "ns3d_server_run_until": ([_P, ctypes.c_longlong, c_double, _P], c_int),
+        "ns3d_map_exponential_served": ([_P, _P, _P], None),
     }
     for name, (args, res) in S.items():
         f = getattr(lib, name)

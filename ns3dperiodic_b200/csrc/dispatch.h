@@ -32,6 +32,7 @@ cudaError_t run_z(const ZArgs<6, float2>& a, const PassGeom& g, cudaStream_t st)
 // device; called when a handle is created (outside any stream capture).
 cudaError_t prepare_xy(const PassGeom& g);
 cudaError_t prepare_fwdx(const PassGeom& g);
+cudaError_t prepare_fwdx_f32(const PassGeom& g);  // the FP32 half (k_fwdx32.cu)
 // Plain 3-D transforms (k_fft3d.cu): one complex line pass along x (axis 0)
 // or y (axis 1), dir +1 inverse / -1 forward; the paired z passes.
 cudaError_t run_line(int axis, int dir, const LineArgs& a, const PassGeom& g, cudaStream_t st);

@@ -1,58 +1,20 @@
-// Forward x pass + pointwise update instantiations.
+// Forward x pass + pointwise update instantiations, FP64 lines (the FP32
+// lines of the precision mode are in k_fwdx32.cu: the two halves compile in
+// parallel).
 #include "dispatch.h"
-#include "launch.cuh"
+#include "k_fwdx.cuh"
 
 namespace ns3d {
-
-namespace {
-template <typename C>
-cudaError_t fwd_x_mode(int mode, bool combine, const FwdXArgs<C>& a, const PassGeom& g,
-                       cudaStream_t st) {
-  switch (mode) {
-    case kExplicit:
-      return combine ? launch_fwd_x<kExplicit, true>(a, g, st)
-                     : launch_fwd_x<kExplicit, false>(a, g, st);
-    case kRhs:
-      return launch_fwd_x<kRhs, false>(a, g, st);
-    case kImplicit:
-      return launch_fwd_x<kImplicit, false>(a, g, st);
-    case kConvOut:
-      return launch_fwd_x<kConvOut, false>(a, g, st);
-    default:
-      return cudaErrorInvalidValue;
-  }
-}
-
-template <typename C>
-cudaError_t prepare_fwdx_prec(const PassGeom& g) {
-  const FwdXArgs<C> a{};
-  cudaError_t e;
-  if ((e = launch_fwd_x<kExplicit, false>(a, g, nullptr, true)) != cudaSuccess) return e;
-  if ((e = launch_fwd_x<kExplicit, true>(a, g, nullptr, true)) != cudaSuccess) return e;
-  if ((e = launch_fwd_x<kRhs, false>(a, g, nullptr, true)) != cudaSuccess) return e;
-  if ((e = launch_fwd_x<kImplicit, false>(a, g, nullptr, true)) != cudaSuccess) return e;
-  return launch_fwd_x<kConvOut, false>(a, g, nullptr, true);
-}
-}  // namespace
 
 cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs<>& a, const PassGeom& g,
                       cudaStream_t st) {
   return fwd_x_mode(mode, combine, a, g, st);
 }
-cudaError_t run_fwd_x(int mode, bool combine, const FwdXArgs<float2>& a, const PassGeom& g,
-                      cudaStream_t st) {
-  return fwd_x_mode(mode, combine, a, g, st);
-}
 
 cudaError_t prepare_fwdx(const PassGeom& g) {
-  for (int tile = 0; tile < 2; ++tile) {
-    PassGeom gt = g;
-    for (int& f : gt.tile) f = tile;
-    cudaError_t e = prepare_fwdx_prec<double2>(gt);
-    if (e == cudaSuccess) e = prepare_fwdx_prec<float2>(gt);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
+  cudaError_t e = prepare_fwdx_tiles<double2>(g);
+  if (e == cudaSuccess) e = prepare_fwdx_f32(g);
+  return e;
 }
 
 }  // namespace ns3d

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "passes.cuh"
 
 namespace ns3d {
@@ -32,6 +34,17 @@ constexpr int p_z(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PZ); }
 constexpr int p_fx(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PFX); }
 // the tangent z pass keeps u, v and the three products live: fewer points
 constexpr int p_zuv(int n) { return n % 3 == 0 ? 6 : 4; }
+// The nonlinear term's z pass with the velocities stashed in shared memory
+// (z_kernel_st): 16 points per thread for powers of two (one Stockham
+// exchange per 256-point transform instead of two), 12 for multiples of 3.
+// NS3D_Z_STASH 0 keeps z_kernel with p_z points per thread.
+#ifndef NS3D_Z_STASH
+#define NS3D_Z_STASH 1
+#endif
+#ifndef NS3D_PZST
+#define NS3D_PZST 16
+#endif
+constexpr int p_zst(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PZST); }
 // points per thread of the plain line passes (8 measured slower than 16 at 256^3 and 512^3)
 #ifndef NS3D_PLINE
 #define NS3D_PLINE 16
@@ -83,23 +96,26 @@ inline unsigned blocks_for(long long lines, int lpc) { return (unsigned)((lines 
 template <int KIND, int N, int P, int X>
 struct KTag {};
 
+// The caches are atomics: host threads that launch on the same device may
+// race to fill them, and each writes the same values.
 template <typename Tag, typename Kern>
 inline unsigned persistent_grid(Kern kern, size_t smem, long long groups) {
-  static int per_sm[64] = {};
-  static int sms[64] = {};
+  static std::atomic<int> per_sm[64] = {};
+  static std::atomic<int> sms[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   dev &= 63;
-  if (per_sm[dev] == 0) {
+  if (per_sm[dev].load(std::memory_order_acquire) == 0) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem);
     int n = 0;
     cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    sms[dev] = n > 0 ? n : 1;
-    per_sm[dev] = occ > 0 ? occ : 1;
+    sms[dev].store(n > 0 ? n : 1, std::memory_order_relaxed);
+    per_sm[dev].store(occ > 0 ? occ : 1, std::memory_order_release);
   }
-  const long long cap = NS3D_SCHED == 0 ? groups : (long long)sms[dev] * per_sm[dev];
+  const long long cap =
+      NS3D_SCHED == 0 ? groups : (long long)sms[dev].load() * per_sm[dev].load();
   return (unsigned)(groups < cap ? (groups > 0 ? groups : 1) : cap);
 }
 
@@ -168,6 +184,17 @@ cudaError_t launch_inv_y(const InvYArgs<NF, C>& a, const PassGeom& gi, cudaStrea
   }
 }
 
+template <int N, typename C>
+cudaError_t launch_z_stash(const ZArgs<3, C>& a, const PassGeom& g, cudaStream_t st) {
+  constexpr int P = p_zst(N);
+  using S = ZStashSmem<N, P, C>;
+  const long long lines = (long long)g.Nx * g.Ny;
+  const unsigned grid = persistent_grid<KTag<40, N, P, prec_tag<C>()>>(
+      z_kernel_st<N, P, C>, S::BYTES, blocks_for(lines, lines_per_cta_z<N, P>()));
+  z_kernel_st<N, P, C><<<grid, kThreads, S::BYTES, st>>>(a, g);
+  return cudaGetLastError();
+}
+
 template <bool UV, typename C>
 cudaError_t launch_z(const ZArgs<UV ? 6 : 3, C>& a, const PassGeom& gi, cudaStream_t st) {
   const PassGeom g = planes_geom(gi);
@@ -175,6 +202,9 @@ cudaError_t launch_z(const ZArgs<UV ? 6 : 3, C>& a, const PassGeom& gi, cudaStre
   switch (g.Nz) {
 #define NS3D_CASE(N)                                                               \
   case N: {                                                                        \
+    if constexpr (!UV && NS3D_Z_STASH && sizeof(C) == 16) {                        \
+      return launch_z_stash<N, C>(a, g, st);                                       \
+    }                                                                              \
     constexpr int P = UV ? p_zuv(N) : p_z(N);                                      \
     z_kernel<N, P, UV, C><<<blocks_for(lines, lines_per_cta_z<N, P>()),           \
                          kWarpsPerCta * 32, 0, st>>>(a, g);                        \
@@ -200,6 +230,39 @@ cudaError_t launch_fwd_x_p(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t
   return cudaGetLastError();
 }
 
+// fwd_x with the update operands in the prefetch ring (fwd_x_ring_kernel):
+// 8 points per thread for powers of two, 12 for multiples of 3, and as many
+// slots as two CTAs per SM leave room for; used where a line fits in a warp
+// (to 256 and 384 points).  At 512 points the ring's lines would spread over
+// the CTA two at a time (32-byte rows): measured 4.69 ms per launch
+// there against 3.42 ms for fwd_x_kernel with 16 points per thread.
+#ifndef NS3D_FX_RING
+#define NS3D_FX_RING 1
+#endif
+#ifndef NS3D_FX_RING32
+#define NS3D_FX_RING32 1
+#endif
+#ifndef NS3D_PFXR
+#define NS3D_PFXR 8
+#endif
+constexpr int p_fxr(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PFXR); }
+constexpr int nslot_fxr(int p) { return p > 8 ? 3 : NS3D_FX_SLOTS; }
+
+template <int N, int P, int MODE, bool COMBINE, typename C>
+cudaError_t launch_fwd_x_ring(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t st,
+                              bool prepare_only) {
+  constexpr int NSLOT = nslot_fxr(P);
+  const long long lines = (long long)g.Ny * g.Mz * nbatch(g);
+  using S = FxRingSmem<N, P, NSLOT, C>;
+  const unsigned grid =
+      persistent_grid<KTag<50 + 2 * MODE + (COMBINE ? 1 : 0), N, P, prec_tag<C>()>>(
+          fwd_x_ring_kernel<N, P, MODE, COMBINE, NSLOT, C>, S::BYTES,
+          (lines + S::LPC - 1) / S::LPC);
+  if (prepare_only) return cudaGetLastError();
+  fwd_x_ring_kernel<N, P, MODE, COMBINE, NSLOT, C><<<grid, kThreads, S::BYTES, st>>>(a, g);
+  return cudaGetLastError();
+}
+
 template <int MODE, bool COMBINE, typename C>
 cudaError_t launch_fwd_x(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t st,
                          bool prepare_only = false) {
@@ -210,6 +273,8 @@ cudaError_t launch_fwd_x(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t s
       if (g.tile[kTileFwdX])                                                          \
         return launch_fwd_x_p<N, p_alt(N), MODE, COMBINE, C>(a, g, st, prepare_only); \
     }                                                                                 \
+    if constexpr (NS3D_FX_RING && N / p_fxr(N) <= 32 && (NS3D_FX_RING32 || sizeof(C) == 16)) \
+      return launch_fwd_x_ring<N, p_fxr(N), MODE, COMBINE, C>(a, g, st, prepare_only); \
     return launch_fwd_x_p<N, p_fx(N), MODE, COMBINE, C>(a, g, st, prepare_only);
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE

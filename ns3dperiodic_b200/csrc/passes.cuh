@@ -137,15 +137,16 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // Copies the P samples t + T*s (s < P) of one line into a private slot:
-// slot[s*kThreads] <- src[base + (t + T*s) * stride], skipping (zero-filling)
-// the samples whose bit in `keep` is clear.
-template <int P, int T, typename E>
+// slot[s*SS] <- src[base + (t + T*s) * stride], skipping (zero-filling)
+// the samples whose bit in `keep` is clear.  SS is the slot's sample stride
+// in elements (kThreads: each thread's samples interleaved with the others').
+template <int P, int T, int SS = kThreads, typename E>
 __device__ __forceinline__ void issue_line(E* slot, const E* __restrict__ src,
                                            size_t base, size_t stride, int t,
                                            uint32_t keep = 0xffffffffu) {
 #pragma unroll
   for (int s = 0; s < P; ++s)
-    cp_async_elem(slot + s * kThreads, src + base + (size_t)(t + T * s) * stride,
+    cp_async_elem(slot + s * SS, src + base + (size_t)(t + T * s) * stride,
                   (keep >> s) & 1u);
 }
 
@@ -441,6 +442,50 @@ struct ZArgs {
   const double2* tw;
 };
 
+// L2 prefetch of one contiguous run (16-byte aligned, a multiple of 16 bytes)
+// by the bulk-copy unit: no registers, no shared memory, nothing to wait for.
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// L2 prefetch of the z pass's input (NS3D_Z_L2PF): 0 none; 1 the CTA's nine
+// input runs (one contiguous run of LPC lines per field) at kernel start, in
+// the order the transforms read them; 2 each transform's two runs one
+// transform ahead (the bulk-copy unit fetches them while the current
+// transform runs, and the loads then hit L2).  Measured on a B200 (z pass per
+// launch, 256^3 / 128^3 FP64): none 503 / 80.4 us, 1: 462 / 81 us, 2: 439 /
+// 67.5 us (two repeats each, within 0.5%).
+#ifndef NS3D_Z_L2PF
+#define NS3D_Z_L2PF 2
+#endif
+
+// L2 prefetch of a CTA's `nv` consecutive z lines (from element run0) of one
+// field: one contiguous run, trimmed to 16-byte boundaries inside it (FP32
+// rows of an odd Mz start at 8-byte offsets).
+template <typename C>
+__device__ __forceinline__ void prefetch_z_run(const C* f, size_t run0, int nv, int Mz) {
+  const uintptr_t a = (uintptr_t)(f + run0) & ~(uintptr_t)15;
+  const uintptr_t e = (uintptr_t)(f + run0 + (size_t)nv * Mz) & ~(uintptr_t)15;
+  if (e > a) prefetch_l2_bulk((const void*)a, (unsigned)(e - a));
+}
+
+// The CTA's runs of one z pass: lines b0 .. b0 + nv - 1 of every field.
+struct ZRun {
+  size_t run0;
+  int nv, Mz;
+};
+__device__ __forceinline__ ZRun z_run(int lpc, int nb, int Mz) {
+  const int b0 = blockIdx.x * lpc;
+  return {(size_t)b0 * Mz, nb - b0 < lpc ? nb - b0 : lpc, Mz};
+}
+// the next transform's two input runs (threads 0 and 1 ask the bulk-copy unit)
+template <typename C>
+__device__ __forceinline__ void prefetch_z_pair(const C* f1, const C* f2, const ZRun& r) {
+  if (NS3D_Z_L2PF == 0) return;
+  if (threadIdx.x == 0) prefetch_z_run(f1, r.run0, r.nv, r.Mz);
+  if (threadIdx.x == 1 && f2 != f1) prefetch_z_run(f2, r.run0, r.nv, r.Mz);
+}
+
 // Load W[k] = H(X1)[k] + i H(X2)[k] for positions k = t + T s, where H is the
 // Hermitian extension of a z half-line (H[0], H[N/2] keep only real parts),
 // X = line (optionally times i kz).
@@ -479,7 +524,8 @@ __device__ __forceinline__ void load_pair(C (&w)[P], const C* __restrict__ f1,
 // 128 points and more (fewer shared-memory wavefronts), the padding else.
 template <int NZ, int P, typename C>
 __host__ __device__ constexpr int z_pw() {
-  return (sizeof(C) == 8 && (NZ & (NZ - 1)) == 0 && NZ >= 128) ? 0 : LineFFT<NZ, P>::PADW;
+  return (sizeof(C) == 8 && P == 8 && (NZ & (NZ - 1)) == 0 && NZ >= 128)
+             ? 0 : LineFFT<NZ, P>::PADW;
 }
 
 template <int NZ, int P, typename C>
@@ -530,15 +576,17 @@ __device__ __forceinline__ void uv_component(Rt (&q)[P], int i, const ZArgs<6, C
                                              const C* tw_s, const Rt (&ux)[P],
                                              const Rt (&uy)[P], const Rt (&uz)[P],
                                              const Rt (&vx)[P], const Rt (&vy)[P],
-                                             const Rt (&vz)[P]) {
+                                             const Rt (&vz)[P], const ZRun& run) {
   using F = LineFFT<NZ, P>;
   C w[P];
   // (d_x u_i, d_y u_i)
+  prefetch_z_pair(a.C[i], a.E[3 + i], run);
   load_pair<NZ, P, false, false>(w, a.E[i], a.D[i], base, t, kfz);
   F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
   for (int s = 0; s < P; ++s) q[s] = vx[s] * (w[s].x * sc) + vy[s] * (w[s].y * sc);
   // (d_z u_i, d_x v_i)
+  prefetch_z_pair(a.D[3 + i], a.C[3 + i], run);
   load_pair<NZ, P, true, false>(w, a.C[i], a.E[3 + i], base, t, kfz);
   F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
@@ -547,6 +595,7 @@ __device__ __forceinline__ void uv_component(Rt (&q)[P], int i, const ZArgs<6, C
     q[s] = q[s] + ux[s] * (w[s].y * sc);
   }
   // (d_y v_i, d_z v_i)
+  if (i < 2) prefetch_z_pair(a.E[i + 1], a.D[i + 1], run);
   load_pair<NZ, P, false, true>(w, a.D[3 + i], a.C[3 + i], base, t, kfz);
   F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
@@ -571,22 +620,26 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
   C* sbuf = sbuf_all[li];
   const Rt sc = (Rt)g.inv_vol;
   const Rt kfz = (Rt)g.kfz;
+  const ZRun run = z_run(LM::LPC, nb, g.Mz);  // one transform ahead into L2
   C w[P];
   Rt ux[P], uy[P], uz[P], q0[P], q1[P], q2[P];
   if constexpr (!UV) {
     // Q_z first, so at most five real lines (u_x, u_y, u_z and two products)
     // are live at any time.
     // (u_x, u_y)
+    prefetch_z_pair(a.C[2], a.C[2], run);
     load_pair<NZ, P, false, false>(w, a.C[0], a.C[1], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { ux[s] = w[s].x * sc; uy[s] = w[s].y * sc; }
     // (u_z, d_z u_z) from one field
+    prefetch_z_pair(a.E[2], a.D[2], run);
     load_pair<NZ, P, false, true>(w, a.C[2], a.C[2], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { uz[s] = w[s].x * sc; q2[s] = w[s].y * sc; }
     // Q_z = u_x d_x u_z + u_y d_y u_z + u_z d_z u_z  (calc_vels_nabla_vels)
+    prefetch_z_pair(a.E[0], a.D[0], run);
     load_pair<NZ, P, false, false>(w, a.E[2], a.D[2], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
@@ -608,6 +661,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { q0[s] = w[s].x * sc; q1[s] = w[s].y * sc; }
+    prefetch_z_pair(a.E[1], a.D[1], run);
     load_pair<NZ, P, false, false>(w, a.E[0], a.D[0], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
@@ -627,21 +681,24 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
   } else {
     // B(u,v)_i = (v.grad) u_i + (u.grad) v_i; fields 0..2 are u, 3..5 are v
     Rt vx[P], vy[P], vz[P];
+    prefetch_z_pair(a.C[2], a.C[3], run);
     load_pair<NZ, P, false, false>(w, a.C[0], a.C[1], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { ux[s] = w[s].x * sc; uy[s] = w[s].y * sc; }
+    prefetch_z_pair(a.C[4], a.C[5], run);
     load_pair<NZ, P, false, false>(w, a.C[2], a.C[3], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { uz[s] = w[s].x * sc; vx[s] = w[s].y * sc; }
+    prefetch_z_pair(a.E[0], a.D[0], run);
     load_pair<NZ, P, false, false>(w, a.C[4], a.C[5], base, t, kfz);
     F::template run<+1, z_pw<NZ, P, C>()>(w, t, sbuf, tw_s);
 #pragma unroll
     for (int s = 0; s < P; ++s) { vy[s] = w[s].x * sc; vz[s] = w[s].y * sc; }
-    uv_component<NZ, P>(q0, 0, a, base, t, kfz, sc, sbuf, tw_s, ux, uy, uz, vx, vy, vz);
-    uv_component<NZ, P>(q1, 1, a, base, t, kfz, sc, sbuf, tw_s, ux, uy, uz, vx, vy, vz);
-    uv_component<NZ, P>(q2, 2, a, base, t, kfz, sc, sbuf, tw_s, ux, uy, uz, vx, vy, vz);
+    uv_component<NZ, P>(q0, 0, a, base, t, kfz, sc, sbuf, tw_s, ux, uy, uz, vx, vy, vz, run);
+    uv_component<NZ, P>(q1, 1, a, base, t, kfz, sc, sbuf, tw_s, ux, uy, uz, vx, vy, vz, run);
+    uv_component<NZ, P>(q2, 2, a, base, t, kfz, sc, sbuf, tw_s, ux, uy, uz, vx, vy, vz, run);
   }
   // forward R2C along z: (Q0, Q1) packed, then Q2 alone
 #pragma unroll
@@ -658,6 +715,120 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, kMinCtasZ) z_kernel(ZArgs<U
       if (k <= NZ / 2) a.Qh[2][base + k] = w[s];
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// z pass with the physical velocities stashed in shared memory (the nonlinear
+// term; the tangent form keeps z_kernel).
+//
+// The line transforms are what bound the z pass: each Stockham exchange moves
+// the whole line through shared memory, so at 8 points per thread a 256-point
+// line takes two exchanges per transform (16 per line and pass) and the
+// shared-memory pipe, not HBM, sets the pace.  With 16 points per thread the
+// same transform needs one exchange, but u_x, u_y, u_z, two products and the
+// line no longer fit in registers.  Here each thread parks its own P samples
+// of u_x, u_y, u_z in a private shared-memory slot ([component][s][thread]:
+// the lanes of a warp touch consecutive words, conflict-free) right after
+// their transforms and reads them back for each product; no other thread
+// reads them, so no barrier is needed.  The arithmetic of every product is
+// the one z_kernel does.
+// ---------------------------------------------------------------------------
+template <int NZ, int P, typename C>
+struct ZStashSmem {
+  using F = LineFFT<NZ, P>;
+  using LM = ZLaneMap<F::T>;
+  using Rt = RealOf<C>;
+  static constexpr size_t SBUF_OFF = align16((size_t)F::TWLEN * sizeof(C));
+  static constexpr size_t ST_OFF = align16(SBUF_OFF + (size_t)LM::LPC * F::BUF * sizeof(C));
+  static constexpr size_t BYTES = ST_OFF + (size_t)3 * P * kThreads * sizeof(Rt);
+  static_assert(BYTES <= 113 * 1024, "two CTAs per SM");
+};
+
+template <int NZ, int P, typename C>
+__global__ void __launch_bounds__(kThreads, kMinCtasZ) z_kernel_st(ZArgs<3, C> a, PassGeom g) {
+  using F = LineFFT<NZ, P>;
+  using Rt = RealOf<C>;
+  using S = ZStashSmem<NZ, P, C>;
+  constexpr int T = F::T;
+  using LM = ZLaneMap<T>;
+  constexpr int PW = z_pw<NZ, P, C>();
+  extern __shared__ __align__(16) unsigned char dsm[];
+  C* tw_s = (C*)dsm;
+  F::load_tw(tw_s, a.tw);
+  int li, t;
+  LM::get(li, t);
+  const int nb = g.Nx * g.Ny;
+  const int b = blockIdx.x * LM::LPC + li;
+  const bool valid = b < nb;
+  const size_t base = (size_t)(valid ? b : 0) * g.Mz;
+  C* sbuf = (C*)(dsm + S::SBUF_OFF) + li * F::BUF;
+  Rt* stash = (Rt*)(dsm + S::ST_OFF) + threadIdx.x;
+  // the CTA's lines are consecutive: each field's input is one run
+  const ZRun run = z_run(LM::LPC, nb, g.Mz);
+  const C* order[9] = {a.C[0], a.C[1], a.C[2], a.E[2], a.D[2], a.E[0], a.D[0], a.E[1], a.D[1]};
+  auto pf = [&](int i) {
+    if (NS3D_Z_L2PF != 0 && i < 9) prefetch_z_run(order[i], run.run0, run.nv, run.Mz);
+  };
+  if (NS3D_Z_L2PF == 1 && threadIdx.x < 9) pf(threadIdx.x);
+  if (NS3D_Z_L2PF == 2 && threadIdx.x < 2) pf(threadIdx.x);  // C0, C1
+  auto ux = [&](int s) -> Rt& { return stash[(0 * P + s) * kThreads]; };
+  auto uy = [&](int s) -> Rt& { return stash[(1 * P + s) * kThreads]; };
+  auto uz = [&](int s) -> Rt& { return stash[(2 * P + s) * kThreads]; };
+  const Rt sc = (Rt)g.inv_vol;
+  const Rt kfz = (Rt)g.kfz;
+  C w[P];
+  Rt q0[P], q1[P];
+  // (u_x, u_y)
+  if (NS3D_Z_L2PF == 2 && threadIdx.x == 0) pf(2);  // C2
+  load_pair<NZ, P, false, false>(w, a.C[0], a.C[1], base, t, kfz);
+  F::template run<+1, PW>(w, t, sbuf, tw_s);
+#pragma unroll
+  for (int s = 0; s < P; ++s) { ux(s) = w[s].x * sc; uy(s) = w[s].y * sc; }
+  // (u_z, d_z u_z); q0 accumulates Q_z first
+  if (NS3D_Z_L2PF == 2 && threadIdx.x < 2) pf(3 + threadIdx.x);  // E2, D2
+  load_pair<NZ, P, false, true>(w, a.C[2], a.C[2], base, t, kfz);
+  F::template run<+1, PW>(w, t, sbuf, tw_s);
+#pragma unroll
+  for (int s = 0; s < P; ++s) { uz(s) = w[s].x * sc; q0[s] = w[s].y * sc; }
+  // Q_z = u_x d_x u_z + u_y d_y u_z + u_z d_z u_z  (calc_vels_nabla_vels)
+  if (NS3D_Z_L2PF == 2 && threadIdx.x < 2) pf(5 + threadIdx.x);  // E0, D0
+  load_pair<NZ, P, false, false>(w, a.E[2], a.D[2], base, t, kfz);
+  F::template run<+1, PW>(w, t, sbuf, tw_s);
+#pragma unroll
+  for (int s = 0; s < P; ++s)
+    q0[s] = ux(s) * (w[s].x * sc) + uy(s) * (w[s].y * sc) + uz(s) * q0[s];
+  // R2C of Q_z alone
+#pragma unroll
+  for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], (Rt)0);
+  F::template run<-1, PW>(w, t, sbuf, tw_s);
+  if (valid) {
+#pragma unroll
+    for (int s = 0; s < P; ++s) {
+      const int k = t + T * s;
+      if (k <= NZ / 2) a.Qh[2][base + k] = w[s];
+    }
+  }
+  // (d_z u_x, d_z u_y)
+  load_pair<NZ, P, true, true>(w, a.C[0], a.C[1], base, t, kfz);
+  F::template run<+1, PW>(w, t, sbuf, tw_s);
+#pragma unroll
+  for (int s = 0; s < P; ++s) { q0[s] = w[s].x * sc; q1[s] = w[s].y * sc; }
+  if (NS3D_Z_L2PF == 2 && threadIdx.x < 2) pf(7 + threadIdx.x);  // E1, D1
+  load_pair<NZ, P, false, false>(w, a.E[0], a.D[0], base, t, kfz);
+  F::template run<+1, PW>(w, t, sbuf, tw_s);
+#pragma unroll
+  for (int s = 0; s < P; ++s)
+    q0[s] = ux(s) * (w[s].x * sc) + uy(s) * (w[s].y * sc) + uz(s) * q0[s];
+  load_pair<NZ, P, false, false>(w, a.E[1], a.D[1], base, t, kfz);
+  F::template run<+1, PW>(w, t, sbuf, tw_s);
+#pragma unroll
+  for (int s = 0; s < P; ++s)
+    q1[s] = ux(s) * (w[s].x * sc) + uy(s) * (w[s].y * sc) + uz(s) * q1[s];
+  // R2C of (Q_x, Q_y) packed
+#pragma unroll
+  for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], q1[s]);
+  F::template run<-1, PW>(w, t, sbuf, tw_s);
+  store_pair_spectrum<NZ, P>(w, sbuf, t, a.Qh[0], a.Qh[1], base, valid);
 }
 
 // ---------------------------------------------------------------------------
@@ -909,6 +1080,19 @@ __host__ __device__ constexpr int fx_chunk(int P) {
          : (NS3D_FX_CHUNK >= 6 && P % 6 == 0) ? 6 : 3;
 }
 
+// Load of an update operand (the state u^s or the RK partner u^n) that the
+// same thread may overwrite afterwards: in the in-place update `out` aliases
+// `us` or `un`.  The read-only (.nc) path is used on purpose.  Every element
+// is read exactly once, by the thread that later writes it, and that store
+// depends on the loaded value; no other thread reads or writes the element.
+// So no load in the kernel can follow a store to its address, and the
+// non-coherent cache can never hand out a stale copy.  Measured on a B200
+// (256^3 FP64, per fwd_x launch): 413 us with this load against 463 us with a
+// coherent ld.global.cg (__ldcg or inline asm); the RK3 step 5.93 against
+// 6.59 ms.  The in-place forms (single_time_step: out == us; RK stage 3:
+// out == un) are covered by parity tests in both precisions.
+__device__ __forceinline__ double2 ld_update(const double2* p) { return __ldg(p); }
+
 template <typename Cx = double2>
 struct FwdXArgs {
   const Cx* Qh[3];
@@ -993,8 +1177,8 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs<C>& a, const PassGeom&
         const size_t idx = off + (size_t)(t + T * (s0 + j)) * nlines;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          us[c][j] = __ldg(a.us[c] + idx);
-          if constexpr (COMBINE) un[c][j] = __ldg(a.un[c] + idx);
+          us[c][j] = ld_update(a.us[c] + idx);
+          if constexpr (COMBINE) un[c][j] = ld_update(a.un[c] + idx);
         }
       }
     }
@@ -1030,7 +1214,7 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs<C>& a, const PassGeom&
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const double2 u = CH > 1 ? us[c][j] : __ldg(a.us[c] + idx);
+        const double2 u = CH > 1 ? us[c][j] : ld_update(a.us[c] + idx);
         double2 r;
         if constexpr (MODE == kExplicit) {
           const double G = 1.0 - kk * dt / Re;
@@ -1043,7 +1227,7 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs<C>& a, const PassGeom&
           r = make_double2(u.x / G, (dt * p[c] + u.y) / G);
         }
         if constexpr (COMBINE) {
-          const double2 n = CH > 1 ? un[c][j] : __ldg(a.un[c] + idx);
+          const double2 n = CH > 1 ? un[c][j] : ld_update(a.un[c] + idx);
           r = make_double2(a.ca * n.x + a.cb * r.x, a.ca * n.y + a.cb * r.y);
         }
         a.out[c][idx] = r;
@@ -1052,11 +1236,6 @@ __device__ __forceinline__ void fwd_x_line(const FwdXArgs<C>& a, const PassGeom&
   }
 }
 
-// L2 prefetch of one contiguous run (16-byte aligned, a multiple of 16 bytes)
-// by the bulk-copy unit: no registers, no shared memory, nothing to wait for.
-__device__ __forceinline__ void prefetch_l2_bulk(const void* p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
-}
 
 // The update at the end of a fwd_x group reads, for every x, the state (and
 // combination partner) elements of the group's LPC consecutive lines: one
@@ -1123,6 +1302,227 @@ __global__ void __launch_bounds__(kThreads, kMinCtasFwdX) fwd_x_kernel(FwdXArgs<
     fwd_x_line<NX, P, MODE, COMBINE, C>(a, g, t, Gc - inst * nlines, line_off(Gc), inst, valid,
                                      sbuf, tw_s, pf, ub, gn < g_end,
                                      line_off(Gn < tlines ? Gn : 0));
+  }
+  cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// fwd_x with the update's operands in the prefetch ring.
+//
+// fwd_x_kernel reads the state (and RK partner) samples of its update with
+// plain loads after the three transforms, two points at a time: every group
+// waits several memory round trips with little in flight.  Here the unit
+// sequence of a group is Qh_x, Qh_y, Qh_z (transformed), then u^s_c (and
+// u^n_c when combining) for c = x, y, z, and every unit goes through one ring
+// of NSLOT per-thread cp.async slots, issued NSLOT - 1 units ahead.  The
+// update runs component by component as its operands arrive: component c of
+// the update needs only u^s_c (u^n_c) and the three transformed products,
+// whose Leray term k (k.Q)/|k|^2 is formed once per point.  Slots hold one
+// 16-byte cell per sample and thread (the state is FP64 in both precisions):
+// an FP32 product sample sits in the first half of its thread's cell, so a
+// slot stays private to each thread whichever kind of unit it holds (with
+// 8-byte product cells a thread's cell would overlap another warp's, and a
+// warp that runs ahead would overwrite samples not yet read).  Arithmetic
+// per point as in fwd_x_line.
+// ---------------------------------------------------------------------------
+// Ring depth of the 8-point lines and the CTAs per SM requested from ptxas:
+// 3 slots at 3 CTAs per SM (168 registers) measured 292 us per plain launch
+// at 256^3 against 399 us with 4 slots at 2 CTAs per SM.  Lines of 12 points
+// keep 3 slots; shapes whose shared memory does not fit 3 CTAs per SM (12
+// points, or the many short lines of 8-point extents) ask for 2.
+#ifndef NS3D_FX_SLOTS
+#define NS3D_FX_SLOTS 3
+#endif
+#ifndef NS3D_MINCTA_FXR
+#define NS3D_MINCTA_FXR 3
+#endif
+
+template <int N, int P, int NSLOT, typename C>
+struct FxRingSmem {
+  using F = LineFFT<N, P>;
+  using LM = LaneMap<F::T>;
+  static constexpr int LPC = LM::LPC;
+  static constexpr int STRIDE = line_stride(F::BUF, xy_stride_target<F::T>());
+  static constexpr size_t SBUF_OFF = align16((size_t)F::TWLEN * sizeof(C));
+  static constexpr size_t RING_OFF = align16(SBUF_OFF + (size_t)LPC * STRIDE * sizeof(C));
+  static constexpr size_t SLOT = (size_t)P * kThreads * sizeof(double2);
+  static constexpr size_t BYTES = RING_OFF + (size_t)NSLOT * SLOT;
+  // CTAs per SM asked of ptxas (registers): as many as the shared memory allows
+  static constexpr int MINC =
+      (P <= 8 && BYTES * NS3D_MINCTA_FXR <= 227 * 1024) ? NS3D_MINCTA_FXR : 2;
+  static_assert(BYTES * MINC <= 227 * 1024, "CTAs per SM");
+};
+
+template <int NX, int P, int MODE, bool COMBINE, int NSLOT, typename C>
+__global__ void __launch_bounds__(kThreads, (FxRingSmem<NX, P, NSLOT, C>::MINC))
+    fwd_x_ring_kernel(FwdXArgs<C> a, PassGeom g) {
+  using S = FxRingSmem<NX, P, NSLOT, C>;
+  using F = typename S::F;
+  using LM = typename S::LM;
+  constexpr int T = F::T;
+  constexpr int NUPD = MODE == kConvOut ? 0 : (COMBINE ? 6 : 3);
+  constexpr int UPG = 3 + NUPD;  // units per group
+  static_assert(NSLOT >= 2 && (!COMBINE || NSLOT >= 3), "ring depth");
+  extern __shared__ __align__(16) unsigned char dsm[];
+  F::load_tw((C*)dsm, a.tw);
+  const C* tw_s = (const C*)dsm;
+  int li, t;
+  LM::get(li, t);
+  C* sbuf = (C*)(dsm + S::SBUF_OFF) + li * S::STRIDE;
+  unsigned char* ring = dsm + S::RING_OFF;
+  const int nlines = g.Ny * g.Mz;
+  const int tlines = nlines * nbatch(g);
+  const int groups = (tlines + LM::LPC - 1) / LM::LPC;
+  auto line_off = [&](int G) -> size_t {
+    const int b = G / nlines;
+    return (size_t)b * NX * nlines + (size_t)(G - b * nlines);
+  };
+  const GroupRange gr = group_range(groups);
+  if (gr.grp >= gr.end) return;  // uniform across the CTA
+  const int ngrp = (gr.end - gr.grp + gr.step - 1) / gr.step;
+  const int nunits = ngrp * UPG;
+  // issue unit k of this CTA's sequence (an empty commit group past the end)
+  auto issue = [&](int k) {
+    if (k < nunits) {
+      const int gi = k / UPG, j = k - gi * UPG;
+      const int G = (gr.grp + gi * gr.step) * LM::LPC + li;
+      const size_t off = line_off(G < tlines ? G : 0);
+      unsigned char* sl = ring + (size_t)(k % NSLOT) * S::SLOT;
+      if (j < 3) {
+        constexpr int CELL = (int)(sizeof(double2) / sizeof(C));  // C elements per cell
+        issue_line<P, T, CELL * kThreads>((C*)sl + CELL * threadIdx.x, a.Qh[j], off,
+                                          (size_t)nlines, t);
+      } else {
+        const int u = j - 3;
+        const double2* src = COMBINE ? ((u & 1) ? a.un[u >> 1] : a.us[u >> 1]) : a.us[u];
+        issue_line<P, T>((double2*)sl + threadIdx.x, src, off, (size_t)nlines, t);
+      }
+    }
+    cp_async_commit();
+  };
+  auto slot = [&](int k) -> unsigned char* { return ring + (size_t)(k % NSLOT) * S::SLOT; };
+#pragma unroll
+  for (int k = 0; k < NSLOT - 1; ++k) issue(k);
+  int k = 0;
+  for (int gi = 0; gi < ngrp; ++gi) {
+    const int G = (gr.grp + gi * gr.step) * LM::LPC + li;
+    const bool valid = G < tlines;
+    const int Gc = valid ? G : 0;
+    const int inst = Gc / nlines;
+    const int L = Gc - inst * nlines;
+    const size_t off = line_off(Gc);
+    // transformed products: Re(Qh) is set to zero (set_to_zero_real), so only
+    // the imaginary parts are kept; Qh(0,0,0) = 0
+    double qi[3][P];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      issue(k + NSLOT - 1);
+      cp_async_wait<NSLOT - 1>();
+      constexpr int CELL = (int)(sizeof(double2) / sizeof(C));
+      const C* cur = (const C*)slot(k) + CELL * threadIdx.x;
+      C v[P];
+#pragma unroll
+      for (int s = 0; s < P; ++s) v[s] = cur[s * CELL * kThreads];
+      F::template run<-1, F::PADW, LM::SW>(v, t, sbuf, tw_s);
+#pragma unroll
+      for (int s = 0; s < P; ++s) {
+        const bool origin = (t + T * s == 0) && (L == 0);
+        qi[c][s] = origin ? 0.0 : (double)v[s].y;
+      }
+      ++k;
+    }
+    if constexpr (MODE == kConvOut) {
+      if (valid) {
+#pragma unroll
+        for (int s = 0; s < P; ++s) {
+          const size_t idx = off + (size_t)(t + T * s) * nlines;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) a.out[c][idx] = make_double2(0.0, qi[c][s]);
+        }
+      }
+      continue;
+    } else {
+      const int y = L / g.Mz, z = L - y * g.Mz;
+      const double ky = g.kfy * (double)signed_idx(y, g.Ny);
+      const double kz = g.kfz * (double)z;
+      const bool dense_f = a.fd[0] != nullptr;
+      const double dt = a.dtRe ? __ldg(a.dtRe + 2 * inst) : a.dt;
+      const double Re = a.dtRe ? __ldg(a.dtRe + 2 * inst + 1) : a.Re;
+      // sparse forcing: does any listed mode lie on this line?  (the scan
+      // per point below is skipped for the lines without one)
+      bool line_f = false;
+      if constexpr (MODE != kImplicit) {
+        if (!dense_f)
+          for (int e = 0; e < a.fnnz; ++e) line_f |= (__ldg(a.fidx + e) % nlines) == L;
+      }
+      // AM.Q with AM_ij = k_i k_j / |k|^2 (0 at k = 0): kq = k.Q / |k|^2
+      double kq[P];
+#pragma unroll
+      for (int s = 0; s < P; ++s) {
+        const double kx = g.kfx * (double)signed_idx(t + T * s, NX);
+        const double kk = kx * kx + ky * ky + kz * kz;
+        kq[s] = kk > 0.0 ? (kx * qi[0][s] + ky * qi[1][s] + kz * qi[2][s]) / kk : 0.0;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        // issued so far: units 0 .. k + NSLOT - 2; the next issue refills the
+        // slot of unit k - 1, consumed already
+        issue(k + NSLOT - 1);
+        // the combining form reads two units (u^s_c, u^n_c) at once: wait for
+        // both, and refill the first one's slot only after the update below
+        if constexpr (COMBINE) {
+          cp_async_wait<NSLOT - 2>();
+        } else {
+          cp_async_wait<NSLOT - 1>();
+        }
+        const double2* us = (const double2*)slot(k) + threadIdx.x;
+        const double2* un = COMBINE ? (const double2*)slot(k + 1) + threadIdx.x : us;
+        const double kc = c == 0 ? 0.0 : (c == 1 ? ky : kz);
+        if (valid) {
+#pragma unroll
+        for (int s = 0; s < P; ++s) {
+          const int x = t + T * s;
+          const size_t fi = (size_t)x * nlines + L;  // index inside the instance (forcing)
+          const size_t idx = off + (size_t)x * nlines;
+          const double kx = g.kfx * (double)signed_idx(x, NX);
+          const double kk = kx * kx + ky * ky + kz * kz;
+          // AM.Q - Q, imaginary part only
+          const double pc = (c == 0 ? kx : kc) * kq[s] - qi[c][s];
+          double2 f = make_double2(0.0, 0.0);
+          if constexpr (MODE != kImplicit) {
+            if (dense_f) {
+              f = __ldg(a.fd[c] + fi);
+            } else if (line_f) {
+              for (int e = 0; e < a.fnnz; ++e)
+                if (__ldg(a.fidx + e) == (int)fi) f = cadd(f, __ldg(a.fval + 3 * e + c));
+            }
+          }
+          const double2 u = us[s * kThreads];
+          double2 r;
+          if constexpr (MODE == kExplicit) {
+            const double Gf = 1.0 - kk * dt / Re;
+            r = make_double2(Gf * u.x + dt * f.x, dt * pc + Gf * u.y + dt * f.y);
+          } else if constexpr (MODE == kRhs) {
+            const double Gf = -kk / Re;
+            r = make_double2(Gf * u.x + f.x, pc + Gf * u.y + f.y);
+          } else {
+            const double Gf = 1.0 + kk * dt / Re;
+            r = make_double2(u.x / Gf, (dt * pc + u.y) / Gf);
+          }
+          if constexpr (COMBINE) {
+            const double2 n = un[s * kThreads];
+            r = make_double2(a.ca * n.x + a.cb * r.x, a.ca * n.y + a.cb * r.y);
+          }
+          a.out[c][idx] = r;
+        }
+        }
+        ++k;
+        if constexpr (COMBINE) {
+          issue(k + NSLOT - 1);  // into the slot of u^s_c, read above
+          ++k;
+        }
+      }
+    }
   }
   cp_async_wait<0>();
 }

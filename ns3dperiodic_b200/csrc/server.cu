@@ -4,11 +4,13 @@
 // process (RK3_SSP_UV, Source/RK_time_step.cu:342-355, called through
 // NSCallMatrixVector_exponential, Source/NS3D_periodic.cu:444-470).
 //
-// A request is (N, Re, T, seed): a Kolmogorov base state u (laminar
+// A request is either (N, Re, T, seed): a Kolmogorov base state u (laminar
 // (Re/16) sin 4y x plus a seeded 1e-3 perturbation) and a seeded unit
-// perturbation v, both generated on the device from the seed; the server
-// advances (u, v) by ceil(T/dt) JVP steps (RK3 base, Heun tangent; dt the
-// CFL-0.3 step of the laminar peak) and reports |v(T)|.
+// perturbation v, both generated on the device from the seed, advanced by
+// ceil(T/dt) JVP steps (RK3 base, Heun tangent; dt the CFL-0.3 step of the
+// laminar peak); or a field request: the caller's own u and v (copied in at
+// admission), dt, Re and step count, with v (and u) copied back to the
+// caller's buffers when it completes.  Either reports |v(T)|.
 //
 // Per grid N the server owns one batched handle of `capacity` instance slots
 // (its memory is reserved when the server is created, from the free HBM),
@@ -26,6 +28,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -239,14 +242,29 @@ struct Group {
 
 }  // namespace
 
+// the caller's buffers of a field request
+struct FieldIO {
+  bool fields = false;
+  double dt = 0.0;
+  const double2* u_in[3] = {};
+  const double2* v_in[3] = {};
+  double2* u_out[3] = {};
+  double2* v_out[3] = {};
+};
+
 struct ns3d_server {
   bool started = false;
   Clock::time_point t0;  // server clock: zero at the first ns3d_server_run
   std::vector<Group> groups;
   std::vector<ns3d_request> req;
+  std::vector<FieldIO> io;  // per request
   std::vector<ns3d_result> res;
   std::map<long long, std::vector<double2>> kept;  // keep = 1 results (3 components)
   std::string err;
+  // ns3d_server_cancel may run on another host thread: the flags it sets and
+  // the finished marks it reads are guarded by `mu`
+  std::mutex mu;
+  std::vector<char> cancel_flag, finished;
 };
 
 namespace {
@@ -275,6 +293,22 @@ size_t slot_bytes(int N) {
   return 45 * Sc;  // u, v (6) + base scratch (21) + tangent scratch (18)
 }
 
+// Frees slot b of a grid whose stream is idle: the last active slot moves
+// into it (compaction), so the active slots stay 0 .. active-1.
+ns3d_status free_slot(ns3d_server* s, Group& g, size_t b) {
+  const size_t last = g.slots.size() - 1;
+  if (b != last) {
+    cudaStream_t st = g.h->stream;
+    SRV_CHECK(s, copy_slot(g.u, g.nc, (int)last, (int)b, st), "compaction");
+    SRV_CHECK(s, copy_slot(g.v, g.nc, (int)last, (int)b, st), "compaction");
+    g.params_host[2 * b] = g.params_host[2 * last];
+    g.params_host[2 * b + 1] = g.params_host[2 * last + 1];
+    g.slots[b] = g.slots[last];
+  }
+  g.slots.pop_back();
+  return NS3D_OK;
+}
+
 // retire finished requests of a grid whose stream is idle
 ns3d_status retire(ns3d_server* s, Group& g, double now) {
   for (size_t b = 0; b < g.slots.size();) {
@@ -299,19 +333,64 @@ ns3d_status retire(ns3d_server* s, Group& g, double now) {
         SRV_CHECK(s, cudaMemcpyAsync(out.data() + c * g.nc, vv[c], sizeof(double2) * g.nc,
                                      cudaMemcpyDeviceToHost, st), "result copy");
     }
+    const FieldIO& io = s->io[(size_t)sl.req];
+    if (io.fields) {  // the caller's output buffers (device or pinned host)
+      for (int c = 0; c < 3; ++c) {
+        SRV_CHECK(s, cudaMemcpyAsync(io.v_out[c], vv[c], sizeof(double2) * g.nc,
+                                     cudaMemcpyDefault, st), "v_out copy");
+        if (io.u_out[c])
+          SRV_CHECK(s, cudaMemcpyAsync(io.u_out[c], g.u[c] + b * g.nc, sizeof(double2) * g.nc,
+                                       cudaMemcpyDefault, st), "u_out copy");
+      }
+    }
     SRV_CHECK(s, cudaStreamSynchronize(st), "retire sync");
     r.v_norm = std::sqrt(*g.norm_host);
     r.done = now;
     r.status = std::isfinite(r.v_norm) ? NS3D_OK : NS3D_ERR_NONFINITE;
-    const size_t last = g.slots.size() - 1;
-    if (b != last) {
-      SRV_CHECK(s, copy_slot(g.u, g.nc, (int)last, (int)b, st), "compaction");
-      SRV_CHECK(s, copy_slot(g.v, g.nc, (int)last, (int)b, st), "compaction");
-      g.params_host[2 * b] = g.params_host[2 * last];
-      g.params_host[2 * b + 1] = g.params_host[2 * last + 1];
-      g.slots[b] = g.slots[last];
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->finished[(size_t)sl.req] = 1;
     }
-    g.slots.pop_back();
+    NS3D_TRY(free_slot(s, g, b));
+  }
+  return NS3D_OK;
+}
+
+// Cancellations flagged by ns3d_server_cancel: queued requests leave the
+// queue; admitted ones leave their slot (the grid's stream is idle here).
+ns3d_status apply_cancels(ns3d_server* s, Group& g, double now) {
+  std::vector<long long> gone;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (auto it = g.queue.begin(); it != g.queue.end();) {
+      if (s->cancel_flag[(size_t)*it]) {
+        s->finished[(size_t)*it] = 1;
+        gone.push_back(*it);
+        it = g.queue.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+  for (size_t b = 0; b < g.slots.size();) {
+    const long long id = g.slots[b].req;
+    bool cancel;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      cancel = s->cancel_flag[(size_t)id] != 0;
+      if (cancel) s->finished[(size_t)id] = 1;
+    }
+    if (!cancel) {
+      ++b;
+      continue;
+    }
+    gone.push_back(id);
+    NS3D_TRY(free_slot(s, g, b));
+  }
+  for (long long id : gone) {
+    ns3d_result& r = s->res[(size_t)id];
+    r.status = NS3D_ERR_CANCELLED;
+    r.done = now;
   }
   return NS3D_OK;
 }
@@ -325,9 +404,19 @@ ns3d_status admit(ns3d_server* s, Group& g, double now) {
     const size_t b = g.slots.size();
     double2* uu[3] = {g.u[0] + b * g.nc, g.u[1] + b * g.nc, g.u[2] + b * g.nc};
     double2* vv[3] = {g.v[0] + b * g.nc, g.v[1] + b * g.nc, g.v[2] + b * g.nc};
-    SRV_CHECK(s, request_fields(uu, vv, g.N, q.Re, q.seed, g.scratch, g.h->stream),
-              "request fields");
-    g.params_host[2 * b] = cfl_dt(g.N, q.Re);
+    const FieldIO& io = s->io[(size_t)id];
+    if (io.fields) {  // the caller's fields, read now
+      for (int c = 0; c < 3; ++c) {
+        SRV_CHECK(s, cudaMemcpyAsync(uu[c], io.u_in[c], sizeof(double2) * g.nc,
+                                     cudaMemcpyDefault, g.h->stream), "u_in copy");
+        SRV_CHECK(s, cudaMemcpyAsync(vv[c], io.v_in[c], sizeof(double2) * g.nc,
+                                     cudaMemcpyDefault, g.h->stream), "v_in copy");
+      }
+    } else {
+      SRV_CHECK(s, request_fields(uu, vv, g.N, q.Re, q.seed, g.scratch, g.h->stream),
+                "request fields");
+    }
+    g.params_host[2 * b] = io.fields ? io.dt : cfl_dt(g.N, q.Re);
     g.params_host[2 * b + 1] = q.Re;
     ns3d_result& r = s->res[(size_t)id];
     r.admitted = now;
@@ -351,6 +440,84 @@ ns3d_status launch_step(ns3d_server* s, Group& g) {
   return NS3D_OK;
 }
 
+// Appends a request (its id is its index) and queues it on its grid.
+void enqueue(ns3d_server* s, const ns3d_request& q, int steps, const FieldIO& io) {
+  const long long id = (long long)s->req.size();
+  s->req.push_back(q);
+  s->io.push_back(io);
+  ns3d_result res{};
+  res.id = id;
+  res.N = q.N;
+  res.Re = q.Re;
+  res.T = q.T;
+  res.steps = steps;
+  res.arrival = q.arrival;
+  res.admitted = -1.0;
+  res.done = -1.0;
+  res.v_norm = 0.0;
+  res.status = -1;
+  s->res.push_back(res);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->cancel_flag.push_back(0);
+    s->finished.push_back(0);
+  }
+  group_of(s, q.N)->queue.push_back(id);
+}
+
+// The engine loop of ns3d_server_run (until < 0) and ns3d_server_run_until.
+ns3d_status engine(ns3d_server* s, double max_seconds, long long until, int* completed) {
+  int done = 0;
+  if (!s->started) {
+    s->t0 = Clock::now();
+    s->started = true;
+  }
+  auto now = [&]() { return std::chrono::duration<double>(Clock::now() - s->t0).count(); };
+  auto target_done = [&]() { return until >= 0 && s->res[(size_t)until].status != -1; };
+  const double deadline = now() + max_seconds;
+  while (!target_done()) {
+    const double t = now();
+    bool work_left = false, progressed = false;
+    for (auto& g : s->groups) {
+      if (g.busy) {
+        const cudaError_t q = cudaEventQuery(g.ev);
+        if (q == cudaErrorNotReady) {
+          work_left = true;
+          continue;
+        }
+        if (q != cudaSuccess) return sfail(s, NS3D_ERR_CUDA, cudaGetErrorString(q));
+        g.busy = false;
+        const size_t before = g.slots.size();
+        NS3D_TRY(retire(s, g, now()));
+        done += (int)(before - g.slots.size());
+        progressed = true;
+      }
+      NS3D_TRY(apply_cancels(s, g, now()));
+      // admission time after this grid's retirements (a slot frees, then fills)
+      if (t <= deadline) NS3D_TRY(admit(s, g, now()));
+      if (!g.slots.empty() && t <= deadline) {
+        NS3D_TRY(launch_step(s, g));
+        progressed = true;
+        work_left = true;
+      }
+      if (!g.queue.empty()) work_left = true;
+    }
+    if (!work_left || t > deadline) break;
+    if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+  // leave no step in flight
+  for (auto& g : s->groups)
+    if (g.busy) {
+      SRV_CHECK(s, cudaEventSynchronize(g.ev), "drain");
+      g.busy = false;
+      const size_t before = g.slots.size();
+      NS3D_TRY(retire(s, g, now()));
+      done += (int)(before - g.slots.size());
+    }
+  if (completed) *completed = done;
+  return NS3D_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -364,6 +531,7 @@ ns3d_status ns3d_server_create(const int* Ns, int nN, const int* capacity, doubl
   ns3d_server* s = new ns3d_server();
   auto bail = [&](ns3d_status st) {
     ns3d_server_destroy(s);
+    cudaGetLastError();  // a failed allocation must not surface at the next launch check
     return st;
   };
   size_t free_b = 0, total_b = 0;
@@ -498,75 +666,87 @@ ns3d_status ns3d_server_submit(ns3d_server* s, const ns3d_request* r, int n, lon
     last = r[i].arrival;
   }
   if (first_id) *first_id = (long long)s->req.size();
+  for (int i = 0; i < n; ++i) enqueue(s, r[i], request_steps(r[i].N, r[i].Re, r[i].T), FieldIO{});
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_server_submit_fields(ns3d_server* s, const ns3d_field_request* r, int n,
+                                      long long* first_id) {
+  if (!s || (!r && n > 0) || n < 0) return NS3D_ERR_BAD_ARG;
+  double last = s->req.empty() ? 0.0 : s->req.back().arrival;
+  std::vector<double> arrival((size_t)n);
+  const double now = s->started
+                         ? std::chrono::duration<double>(Clock::now() - s->t0).count()
+                         : 0.0;
   for (int i = 0; i < n; ++i) {
-    const long long id = (long long)s->req.size();
-    s->req.push_back(r[i]);
-    ns3d_result res{};
-    res.id = id;
-    res.N = r[i].N;
-    res.Re = r[i].Re;
-    res.T = r[i].T;
-    res.steps = request_steps(r[i].N, r[i].Re, r[i].T);
-    res.arrival = r[i].arrival;
-    res.admitted = -1.0;
-    res.done = -1.0;
-    res.v_norm = 0.0;
-    res.status = -1;
-    s->res.push_back(res);
-    group_of(s, r[i].N)->queue.push_back(id);
+    const ns3d_field_request& q = r[i];
+    if (!group_of(s, q.N)) return sfail(s, NS3D_ERR_BAD_ARG, "no grid of that N");
+    if (!(q.Re > 0.0) || !(q.dt > 0.0) || q.steps < 1)
+      return sfail(s, NS3D_ERR_BAD_ARG, "Re and dt must be > 0 and steps >= 1");
+    for (int c = 0; c < 3; ++c)
+      if (!q.u_in[c] || !q.v_in[c] || !q.v_out[c])
+        return sfail(s, NS3D_ERR_BAD_ARG, "u_in, v_in and v_out are required");
+    if ((q.u_out[0] != nullptr) != (q.u_out[1] != nullptr) ||
+        (q.u_out[0] != nullptr) != (q.u_out[2] != nullptr))
+      return sfail(s, NS3D_ERR_BAD_ARG, "u_out: all three components or none");
+    double a = q.arrival;
+    if (a < 0.0) a = std::max(now, last);
+    if (!std::isfinite(a) || a < last)
+      return sfail(s, NS3D_ERR_BAD_ARG, "requests must come in arrival order");
+    arrival[(size_t)i] = last = a;
   }
+  if (first_id) *first_id = (long long)s->req.size();
+  for (int i = 0; i < n; ++i) {
+    const ns3d_field_request& q = r[i];
+    ns3d_request base{};
+    base.N = q.N;
+    base.Re = q.Re;
+    base.T = q.steps * q.dt;
+    base.arrival = arrival[(size_t)i];
+    FieldIO io;
+    io.fields = true;
+    io.dt = q.dt;
+    for (int c = 0; c < 3; ++c) {
+      io.u_in[c] = (const double2*)q.u_in[c];
+      io.v_in[c] = (const double2*)q.v_in[c];
+      io.u_out[c] = (double2*)q.u_out[c];
+      io.v_out[c] = (double2*)q.v_out[c];
+    }
+    enqueue(s, base, q.steps, io);
+  }
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_server_set_forcing(ns3d_server* s, int N, const ns3d_complex* fx,
+                                    const ns3d_complex* fy, const ns3d_complex* fz) {
+  if (!s) return NS3D_ERR_BAD_ARG;
+  Group* g = group_of(s, N);
+  if (!g) return sfail(s, NS3D_ERR_BAD_ARG, "no grid of that N");
+  if (g->busy) return sfail(s, NS3D_ERR_BAD_ARG, "set the forcing between runs");
+  const ns3d_status st = ns3d_set_forcing(g->h, fx, fy, fz);
+  if (st != NS3D_OK) return sfail(s, st, ns3d_last_error(g->h));
+  return NS3D_OK;
+}
+
+ns3d_status ns3d_server_cancel(ns3d_server* s, long long id) {
+  if (!s) return NS3D_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (id < 0 || id >= (long long)s->cancel_flag.size() || s->finished[(size_t)id])
+    return NS3D_ERR_BAD_ARG;
+  s->cancel_flag[(size_t)id] = 1;
   return NS3D_OK;
 }
 
 ns3d_status ns3d_server_run(ns3d_server* s, double max_seconds, int* completed) {
   if (!s || !(max_seconds >= 0.0)) return NS3D_ERR_BAD_ARG;
-  int done = 0;
-  if (!s->started) {
-    s->t0 = Clock::now();
-    s->started = true;
-  }
-  auto now = [&]() { return std::chrono::duration<double>(Clock::now() - s->t0).count(); };
-  const double deadline = now() + max_seconds;
-  for (;;) {
-    const double t = now();
-    bool work_left = false, progressed = false;
-    for (auto& g : s->groups) {
-      if (g.busy) {
-        const cudaError_t q = cudaEventQuery(g.ev);
-        if (q == cudaErrorNotReady) {
-          work_left = true;
-          continue;
-        }
-        if (q != cudaSuccess) return sfail(s, NS3D_ERR_CUDA, cudaGetErrorString(q));
-        g.busy = false;
-        const size_t before = g.slots.size();
-        NS3D_TRY(retire(s, g, now()));
-        done += (int)(before - g.slots.size());
-        progressed = true;
-      }
-      // admission time after this grid's retirements (a slot frees, then fills)
-      if (t <= deadline) NS3D_TRY(admit(s, g, now()));
-      if (!g.slots.empty() && t <= deadline) {
-        NS3D_TRY(launch_step(s, g));
-        progressed = true;
-        work_left = true;
-      }
-      if (!g.queue.empty()) work_left = true;
-    }
-    if (!work_left || t > deadline) break;
-    if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
-  }
-  // leave no step in flight
-  for (auto& g : s->groups)
-    if (g.busy) {
-      SRV_CHECK(s, cudaEventSynchronize(g.ev), "drain");
-      g.busy = false;
-      const size_t before = g.slots.size();
-      NS3D_TRY(retire(s, g, now()));
-      done += (int)(before - g.slots.size());
-    }
-  if (completed) *completed = done;
-  return NS3D_OK;
+  return engine(s, max_seconds, -1, completed);
+}
+
+ns3d_status ns3d_server_run_until(ns3d_server* s, long long id, double max_seconds,
+                                  int* completed) {
+  if (!s || !(max_seconds >= 0.0) || id < 0 || id >= (long long)s->res.size())
+    return NS3D_ERR_BAD_ARG;
+  return engine(s, max_seconds, id, completed);
 }
 
 ns3d_status ns3d_server_results(const ns3d_server* s, ns3d_result* out, int cap, int* n) {
@@ -607,5 +787,52 @@ ns3d_status ns3d_request_fields(ns3d_solver* h, double Re, unsigned long long se
 }
 
 int ns3d_request_steps(int N, double Re, double T) { return request_steps(N, Re, T); }
+
+void ns3d_map_exponential_served(void* user, void* in, void* out) {
+  ns3d_served_map_context* c = static_cast<ns3d_served_map_context*>(user);
+  if (!c) return;
+  ns3d_map_context* m = &c->map;
+  ns3d_status st = (m->solver && c->server) ? NS3D_OK : NS3D_ERR_BAD_ARG;
+  if (st == NS3D_OK && (m->solver->Nx != m->solver->Ny || m->solver->Nx != m->solver->Nz))
+    st = NS3D_ERR_BAD_ARG;
+  if (st == NS3D_OK)
+    st = ns3d_unpack_reduced(m->solver, static_cast<const double*>(in), m->vx, m->vy, m->vz);
+  // the server copies v in on its own stream
+  if (st == NS3D_OK) st = ns3d_synchronize(m->solver);
+  long long id = -1;
+  if (st == NS3D_OK) {
+    ns3d_field_request r{};
+    r.N = m->solver->Nx;
+    r.Re = m->Re;
+    r.dt = m->dt;
+    r.steps = m->steps;
+    ns3d_complex* u[3] = {m->ux, m->uy, m->uz};
+    ns3d_complex* v[3] = {m->vx, m->vy, m->vz};
+    for (int k = 0; k < 3; ++k) {
+      r.u_in[k] = u[k];
+      r.v_in[k] = v[k];
+      r.u_out[k] = u[k];  // the base flow advances with every call
+      r.v_out[k] = v[k];
+    }
+    r.arrival = -1.0;
+    st = ns3d_server_submit_fields(c->server, &r, 1, &id);
+  }
+  if (st == NS3D_OK) st = ns3d_server_run_until(c->server, id, 1e30, nullptr);
+  if (st == NS3D_OK) {
+    const int rs = c->server->res[(size_t)id].status;
+    st = rs == NS3D_OK ? NS3D_OK : (rs == -1 ? NS3D_ERR_CUDA : (ns3d_status)rs);
+  }
+  if (st == NS3D_OK)
+    st = ns3d_pack_reduced(m->solver, m->vx, m->vy, m->vz, static_cast<double*>(out));
+  if (st == NS3D_OK) st = ns3d_synchronize(m->solver);
+  if (st != NS3D_OK) {
+    if (m->status == NS3D_OK) m->status = st;
+    // NaN in the output makes the Krylov driver stop
+    if (out && m->solver)
+      cudaMemset(out, 0xff, sizeof(double) * (size_t)ns3d_krylov_length(m->solver));
+    return;
+  }
+  ++c->requests;
+}
 
 }  // extern "C"

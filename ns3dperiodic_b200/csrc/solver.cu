@@ -266,6 +266,8 @@ const char* ns3d_status_string(ns3d_status s) {
     case NS3D_ERR_CUDA: return "CUDA error";
     case NS3D_ERR_NONFINITE: return "non-finite value";
     case NS3D_ERR_TIMEOUT: return "device wait timed out";
+    case NS3D_ERR_NOT_CONVERGED: return "inner linear solve did not converge";
+    case NS3D_ERR_CANCELLED: return "request cancelled";
   }
   return "unknown status";
 }
@@ -318,6 +320,7 @@ ns3d_status create_solver(int batch, int Nx, int Ny, int Nz, double Lx, double L
 
   auto bail = [&](ns3d_status s) {
     ns3d_destroy(h);
+    cudaGetLastError();  // a failed allocation must not surface at the next launch check
     return s;
   };
   std::vector<uint16_t> qc((size_t)Nx * Ny);

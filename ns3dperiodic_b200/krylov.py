@@ -18,7 +18,8 @@ import ctypes
 
 import numpy as np
 
-from ._lib import LaplaceContext, MAP_FN, MapContext, Ns3dError, ShiftInvertContext, lib
+from ._lib import (LaplaceContext, MAP_FN, MapContext, Ns3dError, ServedMapContext,
+                   ShiftInvertContext, lib)
 
 IM_EIG_TOL = 1.0e-15  # Source/Arnoldi/Macros.h:10
 
@@ -47,6 +48,14 @@ class Map:
 
     def ctx_ptr(self) -> int:
         return ctypes.addressof(self.ctx)
+
+
+class _ServedMap(Map):
+    """A map whose context is an ns3d_served_map_context."""
+
+    @property
+    def status(self) -> int:
+        return int(self.ctx.map.status)
 
 
 class ShiftInvertMap(Map):
@@ -193,6 +202,21 @@ class Krylov:
                          float(Re), 0.0, int(steps), 0)
         return Map(ctypes.cast(self._L.ns3d_map_exponential, ctypes.c_void_p).value, ctx,
                    keep=(U, Vscratch))
+
+    def served_exponential_map(self, server, solver, U, Vscratch, dt: float, Re: float,
+                               steps: int) -> Map:
+        """What exponential_map computes, with every call's tangent steps run
+        by ``server`` (a Server with a grid of solver's N) as a field request
+        (ns3d_map_exponential_served): the Krylov driver's products share
+        the device with the server's other requests.  The result's ``ctx``
+        counts the requests served (``ctx.requests``)."""
+        p = solver._fields(U, "U")
+        q = solver._fields(Vscratch, "V")
+        m = MapContext(solver._h.value, p[0], p[1], p[2], q[0], q[1], q[2], float(dt),
+                       float(Re), 0.0, int(steps), 0)
+        ctx = ServedMapContext(m, server._h.value, 0)
+        return _ServedMap(ctypes.cast(self._L.ns3d_map_exponential_served,
+                                      ctypes.c_void_p).value, ctx, keep=(U, Vscratch, server))
 
     def rhs_map(self, solver, U, Vscratch, Re: float) -> Map:
         """F(x) = RHS(unpack(x)) packed, writing unpack(x) into U first

@@ -12,7 +12,7 @@ import ctypes
 import math
 from typing import Sequence
 
-from ._lib import Ns3dError, Request, Result, lib
+from ._lib import FieldRequest, Ns3dError, Request, Result, lib
 
 _PI2 = 2.0 * math.pi
 
@@ -724,6 +724,8 @@ class Server:
             raise Ns3dError(rc, "ns3d_server_create")
         self._h = h
         self.Ns = Ns
+        self._held = {}     # tensors of field requests not yet done
+        self._forcing = {}  # forcing tensors set per grid
 
     def _check(self, rc, where):
         if rc != 0:
@@ -770,11 +772,83 @@ class Server:
                     "ns3d_server_submit")
         return first.value
 
+    def submit_fields(self, requests):
+        """Requests that carry their own fields (ns3d_field_request), in
+        arrival order: dicts with N, Re, dt, steps, U and V (three CUDA
+        complex128 tensors each, [N, N, N/2+1]), V_out (default V: v(T) is
+        written back in place), U_out (default None: u(T) is not returned)
+        and arrival (default -1: now).  The tensors stay referenced until the
+        request is done.  Returns the first id."""
+        rs, keep = [], []
+        for r in requests:
+            N = int(r["N"])
+            U, V = r["U"], r["V"]
+            Vo = r.get("V_out", V)
+            Uo = r.get("U_out")
+            for F in (U, V, Vo) + ((Uo,) if Uo is not None else ()):
+                self._field_check(F, N)
+            q = FieldRequest()
+            q.N, q.Re, q.dt, q.steps = N, float(r["Re"]), float(r["dt"]), int(r["steps"])
+            for c in range(3):
+                q.u_in[c] = U[c].data_ptr()
+                q.v_in[c] = V[c].data_ptr()
+                q.v_out[c] = Vo[c].data_ptr()
+                q.u_out[c] = Uo[c].data_ptr() if Uo is not None else None
+            q.arrival = float(r.get("arrival", -1.0))
+            rs.append(q)
+            keep.append((U, V, Vo, Uo))
+        arr = (FieldRequest * max(len(rs), 1))(*rs)
+        first = ctypes.c_longlong()
+        self._check(self._L.ns3d_server_submit_fields(self._h, arr, len(rs),
+                                                      ctypes.byref(first)),
+                    "ns3d_server_submit_fields")
+        for i, k in enumerate(keep):
+            self._held[first.value + i] = k
+        return first.value
+
+    @staticmethod
+    def _field_check(F, N):
+        import torch
+
+        Mz = N // 2 + 1
+        if len(F) != 3 or any(f.dtype != torch.complex128 or not f.is_contiguous() or
+                              tuple(f.shape) != (N, N, Mz) for f in F):
+            raise ValueError(f"fields must be 3 contiguous complex128 tensors of shape "
+                             f"({N}, {N}, {Mz})")
+
+    def set_forcing(self, N: int, F):
+        """Forcing of grid N's base flow (three CUDA tensors), between runs."""
+        self._field_check(F, int(N))
+        self._check(self._L.ns3d_server_set_forcing(self._h, int(N),
+                                                    *[f.data_ptr() for f in F]),
+                    "ns3d_server_set_forcing")
+        self._forcing[int(N)] = F
+
+    def cancel(self, rid: int):
+        """ns3d_server_cancel (may be called while run() runs on another thread)."""
+        self._check(self._L.ns3d_server_cancel(self._h, int(rid)), "ns3d_server_cancel")
+
     def run(self, max_seconds: float = 1e30) -> int:
         n = ctypes.c_int()
         self._check(self._L.ns3d_server_run(self._h, float(max_seconds), ctypes.byref(n)),
                     "ns3d_server_run")
+        self._release()
         return n.value
+
+    def run_until(self, rid: int, max_seconds: float = 1e30) -> int:
+        """Runs until request rid is done (ns3d_server_run_until)."""
+        n = ctypes.c_int()
+        self._check(self._L.ns3d_server_run_until(self._h, int(rid), float(max_seconds),
+                                                  ctypes.byref(n)),
+                    "ns3d_server_run_until")
+        self._release()
+        return n.value
+
+    def _release(self):
+        if self._held:
+            done = {r["id"] for r in self.results() if r["status"] != -1}
+            for rid in [k for k in self._held if k in done]:
+                del self._held[rid]
 
     def results(self):
         n = ctypes.c_int()

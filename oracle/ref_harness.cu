@@ -164,6 +164,28 @@ void ref_map_linearised_reduced(void* ctx, void* in, void* out) {
   harness_pack_reduced<<<592, 256>>>(n, S.v[0], S.v[1], S.v[2], static_cast<double*>(out));
 }
 
+// NSCallMatrixVector_exponential (Source/NS3D_periodic.cu:444-470) over the
+// harness state: ctx = double[3] {Re, dt, steps}; vec_in -> S.v (reduced
+// unpacking), `steps` RK3_SSP_UV steps of (S.u, S.v) (the base flow
+// advances with every call, as in the reference), S.v -> vec_out.  The
+// reduced packing is used on both sides, as the library's
+// ns3d_map_exponential does.
+void ref_map_exponential_reduced(void* ctx, void* in, void* out) {
+  const double* c = static_cast<const double*>(ctx);
+  const long long n = (long long)nc();
+  harness_unpack_reduced<<<592, 256>>>(n, static_cast<const double*>(in), S.v[0], S.v[1],
+                                       S.v[2]);
+  const int steps = (int)c[2];
+  for (int s = 0; s < steps; ++s)
+    RK3_SSP_UV(S.dimGrid, S.dimBlock, S.dimGrid_C, S.dimBlock_C, S.dx, S.dy, S.dz, c[1], c[0],
+               S.Nx, S.Ny, S.Nz, S.Mz, S.u[0], S.u[1], S.u[2], S.v[0], S.v[1], S.v[2], S.u1[0],
+               S.u1[1], S.u1[2], S.v1[0], S.v1[1], S.v1[2], S.u2[0], S.u2[1], S.u2[2], S.u3[0],
+               S.u3[1], S.u3[2], S.f[0], S.f[1], S.f[2], S.Q[0], S.Q[1], S.Q[2], S.div_hat,
+               S.kx, S.ky, S.kz, S.din_diffusion, S.din_poisson, S.AM[0], S.AM[1], S.AM[2],
+               S.AM[3], S.AM[4], S.AM[5]);
+  harness_pack_reduced<<<592, 256>>>(n, S.v[0], S.v[1], S.v[2], static_cast<double*>(out));
+}
+
 
 int ref_create(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz) {
   if (S.live) return -2;

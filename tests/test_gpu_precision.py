@@ -32,7 +32,7 @@ def _h(F):
     return [f.cpu().numpy() for f in F]
 
 
-@pytest.mark.parametrize("N", [32, 64, 96])
+@pytest.mark.parametrize("N", [32, 64, 96, 192])
 def test_fp32_steps_track_fp64(torch, N):
     from ns3dperiodic_b200 import Solver
     from ns3dperiodic_b200 import workload as W
@@ -53,6 +53,49 @@ def test_fp32_steps_track_fp64(torch, N):
         S.precision = "fp64"
         again = _h(S.rk3_ssp(S.to_device(U0), dt, Re, nsteps=50))
         assert all(np.array_equal(a, b) for a, b in zip(again, ref50))
+
+
+@pytest.mark.parametrize("N", [48, 96, 192])
+def test_steps_are_deterministic_in_both_precisions(torch, N):
+    """Repeated runs from the same state give the same bits: a race between
+    the warps of a pass (for instance over a shared-memory slot) shows up as
+    run-to-run differences long before it shows up as a wrong answer."""
+    from ns3dperiodic_b200 import Solver
+    from ns3dperiodic_b200 import workload as W
+
+    Re = 200.0
+    U0, F = W.kolmogorov_state(N, Re, 3, rel_amp=0.05)
+    dt = W.kolmogorov_dt(N, Re)
+    with Solver(N, N, N) as S:
+        S.set_forcing(S.to_device(F))
+        for prec in ("fp64", "fp32"):
+            S.precision = prec
+            runs = [_h(S.rk3_ssp(S.to_device(U0), dt, Re, nsteps=20)) for _ in range(3)]
+            assert all(np.isfinite(u).all() for u in runs[0]), prec
+            for r in runs[1:]:
+                assert all(np.array_equal(a, b) for a, b in zip(r, runs[0])), prec
+
+
+@pytest.mark.parametrize("N", [32, 128])
+def test_fp32_in_place_update(torch, N):
+    """single_time_step writes the new state over its input (the fwd_x update's
+    output aliases the state it reads): the FP32 mode against the oracle's FP64
+    Euler step from the same state, 1e-7 relative L2."""
+    from ns3dperiodic_b200 import Solver
+    from ns3dperiodic_b200 import workload as W
+
+    Re = 200.0
+    g = O.Grid(N, N, N)
+    U0, F = W.kolmogorov_state(N, Re, 5, rel_amp=0.05)
+    dt = W.kolmogorov_dt(N, Re)
+    want = O.single_time_step(g, U0, F, dt, Re)
+    with Solver(N, N, N) as S:
+        S.precision = "fp32"
+        S.set_forcing(S.to_device(F))
+        U = S.to_device(U0)
+        S.single_time_step(U, dt, Re)
+        err = O.rel_l2(_h(U), want)
+    assert 0.0 < err < 1e-7, err
 
 
 def test_fp32_shapiro(torch):
