@@ -24,16 +24,20 @@ m = 30 (Source/Arnoldi/cuda_test.cu:63-70); the reference arm runs the
 reference's own Arnoldi_driver (cuBLAS) on the same operator and start
 vector.
 
---workload ira: one "step" is one implicitly restarted Arnoldi run of the
-linearised Navier-Stokes operator J(u0) (NSCallMatrixVector_reduced) about
-the laminar Kolmogorov flow u0 = Re/16 sin(4y) x at 64^3, Re = 200, k = 20,
-m = 40, "LR": a fresh N(0, 2) start vector, --ira-cycles restart cycles
-(tolerance 0, so every run does the same number) and the final Schur /
-Galerkin eigenvector stage.  The reference arm runs the reference's own
-Implicit_restart_Arnoldi_GPU_data (cuBLAS + host LAPACK) with its
-RK3_SSP_UV_RHS-based map on the same base flow.
+--workload ira: one "step" is one implicitly restarted Arnoldi run about the
+laminar Kolmogorov flow u0 = Re/16 sin(4y) x (forced by sin(4y) x) at 64^3,
+Re = 200, k = 20, m = 40, from a fresh N(0, 2) start vector, with the final
+Schur / Galerkin eigenvector stage.  Default (--ira-map exponential): the
+exponential map NSCallMatrixVector_exponential (--ira-steps RK3_SSP_UV steps
+per product at the CFL-0.3 dt), "LM", run until the Ritz norm is below
+--ira-tol (5e-8, main's IRA_tol) - the reference main's IRA branch for
+Timesteps_period > 1 (Source/NS3D_periodic.cu:1714-1718).  --ira-map
+linearised: the Jacobian J(u0) itself (NSCallMatrixVector_reduced), "LR",
+--ira-cycles forced cycles.  The reference arm runs the reference's own
+Implicit_restart_Arnoldi_GPU_data (cuBLAS + host LAPACK) with its own map
+(RK3_SSP_UV, or RK3_SSP_UV_RHS) on the same base flow and forcing.
 
-  python bench.py --workload ira --steps 5 --warmup 3
+  python bench.py --workload ira --steps 3 --warmup 1
 """
 from __future__ import annotations
 
@@ -83,10 +87,23 @@ def parse():
     ap.add_argument("--ira-N", type=int, default=64, help="ira: grid size")
     ap.add_argument("--ira-k", type=int, default=20, help="ira: wanted eigenvalues")
     ap.add_argument("--ira-m", type=int, default=40, help="ira: Krylov basis size")
-    ap.add_argument("--ira-cycles", type=int, default=20, help="ira: restart cycles per run")
+    ap.add_argument("--ira-map", choices=["exponential", "linearised"], default="exponential",
+                    help="ira: the exponential map (NSCallMatrixVector_exponential, 'LM', run "
+                         "to --ira-tol) or the linearised map (NSCallMatrixVector_reduced, "
+                         "'LR', --ira-cycles forced cycles)")
+    ap.add_argument("--ira-steps", type=int, default=20,
+                    help="ira: tangent steps per product of the exponential map")
+    ap.add_argument("--ira-tol", type=float, default=5e-8,
+                    help="ira: Ritz-norm tolerance of the exponential-map run "
+                         "(IRA_tol of the reference's main)")
+    ap.add_argument("--ira-cycles", type=int, default=None,
+                    help="ira: restart cycles per run (linearised map: exactly this many, "
+                         "default 20; exponential map: the cap, default 3000)")
     ap.add_argument("--n-arnoldi", type=int, default=2300000)
     ap.add_argument("--m-arnoldi", type=int, default=30)
     a = ap.parse_args()
+    if a.ira_cycles is None:
+        a.ira_cycles = 3000 if a.ira_map == "exponential" else 20
     if a.Re is None:
         a.Re = 400.0 if (a.workload == "rk3" and a.N >= 256) else 200.0
     return a
@@ -329,8 +346,12 @@ def run_ours(args, world, rank, local, pg):
     dom = max(range(5), key=lambda i: pm[i])
     peak, peak_src = peaks()
     achieved = alg[dom] / (pm[dom] * 1e-3) / 1e9
-    kname = {0: "inv_x_kernel", 1: "inv_y_kernel", 2: "z_kernel", 3: "fwd_y_kernel",
-             4: "fwd_x_kernel"}[dom]
+    # the kernels the step launches: the nonlinear term's z pass with the
+    # velocities in shared memory for FP64 lines; the ring-pipelined fwd_x
+    # where a line fits in a warp (8 points per thread, 12 for multiples of 3)
+    ring = N // (12 if N % 3 == 0 else min(N, 8)) <= 32
+    kname = {0: "inv_x_kernel", 1: "inv_y_kernel", 2: "z_kernel" if fp32 else "z_kernel_st",
+             3: "fwd_y_kernel", 4: "fwd_x_ring_kernel" if ring else "fwd_x_kernel"}[dom]
     traffic = traffic_from_profiles(kname, N)
     roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -678,34 +699,60 @@ def ira_start(n, seed):
     return np.random.default_rng(seed).normal(0.0, 2.0, n)
 
 
+def ira_setup(args):
+    """(N, Re, k, m, which, tol, max_iter, dt, steps) of the ira workload."""
+    from ns3dperiodic_b200 import workload as W
+
+    N, Re, k, m = args.ira_N, args.Re, args.ira_k, args.ira_m
+    if args.ira_map == "exponential":
+        return N, Re, k, m, "LM", args.ira_tol, args.ira_cycles, W.kolmogorov_dt(N, Re), \
+            args.ira_steps
+    return N, Re, k, m, "LR", 0.0, args.ira_cycles, 0.0, 0
+
+
+def ira_metric(args, N, Re, k, m):
+    if args.ira_map == "exponential":
+        return (f"IRA runs/s to Ritz norm <= {args.ira_tol:g} (exponential map, "
+                f"{args.ira_steps} RK3_SSP_UV steps per product, of the linearised NS about "
+                f"laminar Kolmogorov, {N}^3, Re={Re:g}, k={k}, m={m}, LM, FP64)")
+    return (f"IRA runs/s (linearised NS about laminar Kolmogorov, {N}^3, Re={Re:g}, "
+            f"k={k}, m={m}, {args.ira_cycles} restart cycles + eigenvector stage, FP64)")
+
+
 def run_ours_ira(args, world, rank, local, pg):
     import numpy as np
     import torch
 
     from ns3dperiodic_b200 import Krylov, Solver
+    from ns3dperiodic_b200 import workload as W
 
-    N, Re, k, m, R = args.ira_N, args.Re, args.ira_k, args.ira_m, args.ira_cycles
+    N, Re, k, m, which, tol, max_iter, dt, steps = ira_setup(args)
+    expo = args.ira_map == "exponential"
     U = ira_state(N, Re)
     S = Solver(N, N, N)
     tiles = S.tiles if args.no_autotune else S.autotune()["tiles"]
+    S.set_forcing(S.to_device(W.kolmogorov_forcing(N, N, N)))
     Ud = S.to_device(U)
+    Vs = S.zeros()
     n = S.krylov_length
     kr = Krylov(n, m)
-    A = kr.linearised_map(S, Ud, Re)
+    A = kr.exponential_map(S, Ud, Vs, dt, Re, steps) if expo else kr.linearised_map(S, Ud, Re)
+    # launches per map call: unpack, the steps' passes (JVP step: 2 tangent
+    # right-hand sides of 5 launches and a base RK3 step of 15), pack
+    per_call = 2 + 25 * steps if expo else 7
 
     launches = [0]
 
     def one_run(f0d):
-        _, rn, it, V, H = kr.implicit_restart_arnoldi(A, "LR", k, m, 0.0, R, f0=f0d)
-        w, X, res = kr.eigenpairs(A, V, H, k, "LR")
+        _, rn, it, V, H = kr.implicit_restart_arnoldi(A, which, k, m, tol, max_iter, f0=f0d)
+        w, X, res = kr.eigenpairs(A, V, H, k, which)
         cols = list(kr.last_restart_columns)
-        # driver + restart kernels, 7 per map call (unpack, 5 passes, pack),
-        # 3 combines of the eigenvector stage
-        launches[0] += kr.last_restart_launches + 7 * (sum(cols) + k) + 3
-        return w, X, res, rn, cols
+        launches[0] += kr.last_restart_launches + per_call * (sum(cols) + k) + 3
+        return w, X, res, rn, cols, it
 
     f0d = torch.as_tensor(ira_start(n, args.seed + rank), device="cuda")
     for _ in range(args.warmup):
+        Ud_reset(Ud, S, U)
         one_run(f0d)
     barrier(pg)
     sampler = ClockSampler(local)
@@ -714,6 +761,8 @@ def run_ours_ira(args, world, rank, local, pg):
     s0 = torch.cuda.default_stream()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    Ud_reset(Ud, S, U)
+    torch.cuda.synchronize()
     ev0.record(s0)
     out = None
     launches[0] = 0
@@ -728,25 +777,26 @@ def run_ours_ira(args, world, rank, local, pg):
     ms = max_over_ranks(ms_local, pg)
     ms_step = ms / args.steps
     value = world * args.steps / (ms / 1e3)
-    w, X, res, rn, cols = out
+    w, X, res, rn, cols, it = out
     peak, peak_src = peaks()
     # bytes of one run: map calls (P3L) + Gram-Schmidt (one reorthogonalisation)
     _, Sc, Sr = sizes(N)
-    mv_bytes = 84 * Sc + 6 * Sr
+    mv_bytes = steps * (330 * Sc + 30 * Sr) if expo else 84 * Sc + 6 * Sr
     calls = sum(cols) + k
     gs = 0
     for c in cols:
         for j in range(m - c, m):
             gs += 4 * (j + 1) * 8 * n
     B = mv_bytes * calls + gs
-    # the map alone, timed on the device: the dominant kernel sequence
+    # the map alone, timed on the device
     x = torch.as_tensor(ira_start(n, 99), device="cuda")
     y = torch.empty_like(x)
+    Ud_reset(Ud, S, U)
     for _ in range(3):
         kr.apply(A, x, y)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    reps = 50
+    reps = 5 if expo else 50
     e0.record(s0)
     for _ in range(reps):
         kr.apply(A, x, y)
@@ -754,7 +804,9 @@ def run_ours_ira(args, world, rank, local, pg):
     e1.synchronize()
     mv_ms = e0.elapsed_time(e1) / reps
     achieved = mv_bytes / (mv_ms * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "linearised map (unpack, 5-pass B(u,v) + update, pack)",
+    kname = (f"exponential map ({steps} RK3_SSP_UV steps, pack/unpack)" if expo else
+             "linearised map (unpack, 5-pass B(u,v) + update, pack)")
+    roofline = {"bound": "hbm", "kernel": kname,
                 "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_src,
                 "alg_bytes_per_launch": mv_bytes, "ms_per_launch": round(mv_ms, 5),
@@ -769,16 +821,17 @@ def run_ours_ira(args, world, rank, local, pg):
     for _ in range(K):
         for d, h in zip(Ud, hU):
             d.copy_(h, non_blocking=True)
-        w2, X2, _, _, _ = one_run(f0d)
+        w2, X2, _, _, _, _ = one_run(f0d)
         hX.copy_(X2)
     torch.cuda.synchronize()
     el = max_over_ranks(time.perf_counter() - t0, pg)
     kr.close()
     S.close()
     nc = N * N * (N // 2 + 1)
+    cfg_map = (f"ns3d_map_exponential (NSCallMatrixVector_exponential), {steps} steps of "
+               f"dt={dt:.6g}" if expo else "ns3d_map_linearised (NSCallMatrixVector_reduced)")
     return {
-        "metric": f"IRA runs/s (linearised NS about laminar Kolmogorov, {N}^3, Re={Re:g}, "
-                  f"k={k}, m={m}, {R} restart cycles + eigenvector stage, FP64)",
+        "metric": ira_metric(args, N, Re, k, m),
         "value": round(value, 4),
         "unit": "runs/s",
         "n_gpus": world,
@@ -790,9 +843,11 @@ def run_ours_ira(args, world, rank, local, pg):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"ira_kolmogorov_laminar_{N}_Re{Re:g}_k{k}_m{m}_c{R}",
-                   "N": N, "Re": Re, "k": k, "m": m, "cycles": R, "n": n, "which": "LR",
-                   "map": "ns3d_map_linearised (NSCallMatrixVector_reduced)",
+        "config": {"workload": (f"ira_expo{steps}_kolmogorov_laminar_{N}_Re{Re:g}_k{k}_m{m}_"
+                                f"tol{tol:g}" if expo else
+                                f"ira_kolmogorov_laminar_{N}_Re{Re:g}_k{k}_m{m}_c{max_iter}"),
+                   "N": N, "Re": Re, "k": k, "m": m, "n": n, "which": which, "tol": tol,
+                   "max_cycles": max_iter, "cycles": it, "map": cfg_map,
                    "tiles": dict(zip(("inv_x", "inv_y", "fwd_y", "fwd_x"), tiles)),
                    "parallelism": f"replicas x{world}",
                    "l2": f"basis {m * n * 8 / 1e6:.0f} MB + fields > 126 MB L2",
@@ -813,10 +868,22 @@ def run_ours_ira(args, world, rank, local, pg):
     }
 
 
-def cpu_baseline_ira(N, Re, m, calls, seed):
-    """The oracle's Arnoldi factorisation (numpy) over the oracle's
-    linearised map on a bounded sample: one factorisation from k = 0 with
-    min(m, 8) columns, scaled to a run's map calls."""
+def Ud_reset(Ud, S, U):
+    """The base flow back to u0 (the exponential map advances it with every call)."""
+    import torch
+
+    for d, h in zip(Ud, S.to_device(U)):
+        d.copy_(h)
+    torch.cuda.synchronize()
+
+
+def cpu_baseline_ira(N, Re, m, calls, seed, steps=0, dt=0.0):
+    """The oracle on the host cores, on a bounded sample.  Exponential map
+    (steps > 0): one oracle RK3_SSP_UV step (numpy + scipy.fft) timed and
+    scaled to a run's products x steps (the Gram-Schmidt, a few percent of a
+    run, is left out).  Linearised map: one factorisation from k = 0 with
+    min(m, 8) columns over the oracle's linearised map, scaled to a run's
+    map calls."""
     import numpy as np
 
     from oracle import krylov_oracle as K
@@ -824,6 +891,21 @@ def cpu_baseline_ira(N, Re, m, calls, seed):
 
     g = O.Grid(N, N, N)
     U = ira_state(N, Re)
+    if steps > 0:
+        os.environ["NS3D_ORACLE_THREADS"] = str(os.cpu_count() or 1)
+        F = O.kolmogorov_forcing(g)
+        V = O.random_perturbation(g, seed)
+        O.rk3_ssp_uv(g, U, V, F, dt, Re)  # warm-up (plans, page faults)
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            U2, V = O.rk3_ssp_uv(g, U, V, F, dt, Re)
+        el = (time.perf_counter() - t0) / reps
+        return {"value": 1.0 / (el * steps * calls), "unit": "runs/s",
+                "cores": os.cpu_count() or 1, "kind": "port",
+                "sample": f"{reps} oracle RK3_SSP_UV steps at {N}^3 (numpy + scipy.fft), "
+                          f"{el:.2f} s each, scaled to the {calls} products x {steps} steps "
+                          f"of one run (Gram-Schmidt not counted)"}
     n = 3 * (N * N * (N // 2 + 1) - 1)
     mm = min(m, 8)
     f = ira_start(n, seed)
@@ -852,16 +934,26 @@ def run_reference_ira(args, world, rank, local, pg):
                                                     "(needs the reference tree to compile)"}
     from oracle.ref_lib import RefSolver
 
-    N, Re, k, m, R = args.ira_N, args.Re, args.ira_k, args.ira_m, args.ira_cycles
+    from ns3dperiodic_b200 import workload as W
+
+    N, Re, k, m, which, tol, R, dt, steps = ira_setup(args)
+    expo = args.ira_map == "exponential"
     ns = RefSolver(N, N, N)
-    ns.set_u(ira_state(N, Re))
+    U0 = ira_state(N, Re)
+    ns.set_u(U0)
+    ns.set_f(W.kolmogorov_forcing(N, N, N))
     arn = ctypes.CDLL(path)
     arn.ref_ira_map.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                 ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_double)]
     arn.ref_ira_map.restype = ctypes.c_double
-    fn = ctypes.cast(ns.lib.ref_map_linearised_reduced, ctypes.c_void_p).value
-    ctx = (ctypes.c_double * 2)(Re, 0.0)
+    if expo:
+        fn = ctypes.cast(ns.lib.ref_map_exponential_reduced, ctypes.c_void_p).value
+        ctx = (ctypes.c_double * 3)(Re, dt, float(steps))
+    else:
+        fn = ctypes.cast(ns.lib.ref_map_linearised_reduced, ctypes.c_void_p).value
+        ctx = (ctypes.c_double * 2)(Re, 0.0)
+    lm = 1 if which == "LM" else 0
     n = 3 * (N * N * (N // 2 + 1) - 1)
     libc = ctypes.CDLL(None)
     sampler = ClockSampler(local)
@@ -877,12 +969,14 @@ def run_reference_ira(args, world, rank, local, pg):
         try:
             t = ctypes.c_double(0.0)
             for _ in range(args.warmup):
-                arn.ref_ira_map(n, fn, ctypes.cast(ctx, ctypes.c_void_p), k, m, 0.0, R, 0,
+                ns.set_u(U0)  # the exponential map advances the base flow
+                arn.ref_ira_map(n, fn, ctypes.cast(ctx, ctypes.c_void_p), k, m, tol, R, lm,
                                 ctypes.byref(t))
             sampler.start()
             time.sleep(0.3)
             for _ in range(args.steps):
-                rn = arn.ref_ira_map(n, fn, ctypes.cast(ctx, ctypes.c_void_p), k, m, 0.0, R, 0,
+                ns.set_u(U0)  # outside the call's CUDA-event timing
+                rn = arn.ref_ira_map(n, fn, ctypes.cast(ctx, ctypes.c_void_p), k, m, tol, R, lm,
                                      ctypes.byref(t))
                 total += t.value
             clocks = sampler.stop()
@@ -896,18 +990,22 @@ def run_reference_ira(args, world, rank, local, pg):
         return {"impl": "reference", "unavailable": "reference Implicit_restart_Arnoldi_GPU_data "
                                                     "run failed"}
     value = args.steps / (total / 1e3)
+    mapname = (f"RK3_SSP_UV x {steps} as NSCallMatrixVector_exponential (reduced packing)"
+               if expo else "RK3_SSP_UV_RHS as NSCallMatrixVector_reduced")
     return {"impl": "reference",
-            "metric": f"IRA runs/s (linearised NS about laminar Kolmogorov, {N}^3, Re={Re:g}, "
-                      f"k={k}, m={m}, {R} restart cycles + eigenvector stage, FP64)",
+            "metric": ira_metric(args, N, Re, k, m),
             "value": round(value, 4), "unit": "runs/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"ira_kolmogorov_laminar_{N}_Re{Re:g}_k{k}_m{m}_c{R}",
-                       "N": N, "Re": Re, "k": k, "m": m, "cycles": R, "n": n,
+            "config": {"workload": (f"ira_expo{steps}_kolmogorov_laminar_{N}_Re{Re:g}_k{k}_"
+                                    f"m{m}_tol{tol:g}" if expo else
+                                    f"ira_kolmogorov_laminar_{N}_Re{Re:g}_k{k}_m{m}_c{R}"),
+                       "N": N, "Re": Re, "k": k, "m": m, "which": which, "tol": tol,
+                       "max_cycles": R, "n": n,
                        "reference": "unmodified Implicit_restart_Arnoldi_GPU_data (cuBLAS, "
-                                    "LAPACK from scipy's OpenBLAS) with RK3_SSP_UV_RHS as "
-                                    "NSCallMatrixVector_reduced, verbose off, sm_100a",
+                                    f"LAPACK from scipy's OpenBLAS) with {mapname}, verbose "
+                                    "off, sm_100a",
                        "ritz_norm": rn},
             "cpu_baseline": None,
             "e2e": {"value": round(value, 4), "unit": "runs/s", "h2d_bytes_per_step": 0,
@@ -1345,9 +1443,10 @@ def main():
             else:
                 line = run_ours_ira(args, world, rank, local, pg)
                 if rank == 0 and world == 1 and not args.no_cpu_baseline:
+                    _, _, _, _, _, _, _, dt, steps = ira_setup(args)
                     line["cpu_baseline"] = cpu_baseline_ira(
                         args.ira_N, args.Re, args.ira_m, line["config"]["map_calls_per_run"],
-                        args.seed)
+                        args.seed, steps, dt)
         elif args.workload == "arnoldi":
             if args.impl == "reference":
                 line = run_reference_arnoldi(args, world, rank, local, pg)

@@ -45,6 +45,12 @@ constexpr int p_zuv(int n) { return n % 3 == 0 ? 6 : 4; }
 #define NS3D_PZST 16
 #endif
 constexpr int p_zst(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PZST); }
+// FP32 lines of the nonlinear term's z pass: half the registers per point,
+// so 16 points per thread fit without the stash (one exchange per transform)
+#ifndef NS3D_PZ32
+#define NS3D_PZ32 16
+#endif
+constexpr int p_z32(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PZ32); }
 // points per thread of the plain line passes (8 measured slower than 16 at 256^3 and 512^3)
 #ifndef NS3D_PLINE
 #define NS3D_PLINE 16
@@ -205,7 +211,7 @@ cudaError_t launch_z(const ZArgs<UV ? 6 : 3, C>& a, const PassGeom& gi, cudaStre
     if constexpr (!UV && NS3D_Z_STASH && sizeof(C) == 16) {                        \
       return launch_z_stash<N, C>(a, g, st);                                       \
     }                                                                              \
-    constexpr int P = UV ? p_zuv(N) : p_z(N);                                      \
+    constexpr int P = UV ? p_zuv(N) : (sizeof(C) == 8 ? p_z32(N) : p_z(N));        \
     z_kernel<N, P, UV, C><<<blocks_for(lines, lines_per_cta_z<N, P>()),           \
                          kWarpsPerCta * 32, 0, st>>>(a, g);                        \
     return cudaGetLastError();                                                     \

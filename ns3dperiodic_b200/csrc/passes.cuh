@@ -36,6 +36,12 @@ constexpr int kWarpsPerCta = 4;
 #define NS3D_MINCTA_FX 2
 #endif
 constexpr int kMinCtasXY = NS3D_MINCTA_XY;
+// The x / y passes' tiles of 8 points or fewer per thread (the autotuner's
+// alternative for long lines) ask for NS3D_MINCTA_XY8 CTAs per SM.
+#ifndef NS3D_MINCTA_XY8
+#define NS3D_MINCTA_XY8 2
+#endif
+__host__ __device__ constexpr int min_ctas_xy(int p) { return p <= 8 ? NS3D_MINCTA_XY8 : kMinCtasXY; }
 constexpr int kMinCtasZ = NS3D_MINCTA_Z;
 constexpr int kMinCtasFwdX = NS3D_MINCTA_FX;
 
@@ -233,7 +239,7 @@ struct InvXArgs {
 };
 
 template <int NX, int P, int NF, typename C>
-__global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_x_kernel(InvXArgs<NF, C> a, PassGeom g) {
+__global__ void __launch_bounds__(kThreads, min_ctas_xy(P)) inv_x_kernel(InvXArgs<NF, C> a, PassGeom g) {
   using S = PassSmem<NX, P, C, double2>;
   using F = typename S::F;
   using LM = typename S::LM;
@@ -339,7 +345,7 @@ struct InvYArgs {
 };
 
 template <int NY, int P, int NF, typename C>
-__global__ void __launch_bounds__(kThreads, kMinCtasXY) inv_y_kernel(InvYArgs<NF, C> a, PassGeom g) {
+__global__ void __launch_bounds__(kThreads, min_ctas_xy(P)) inv_y_kernel(InvYArgs<NF, C> a, PassGeom g) {
   using S = PassSmem<NY, P, C, C>;
   using F = typename S::F;
   using LM = typename S::LM;
@@ -841,7 +847,7 @@ struct FwdYArgs {
 };
 
 template <int NY, int P, typename C>
-__global__ void __launch_bounds__(kThreads, kMinCtasXY) fwd_y_kernel(FwdYArgs<C> a, PassGeom g) {
+__global__ void __launch_bounds__(kThreads, min_ctas_xy(P)) fwd_y_kernel(FwdYArgs<C> a, PassGeom g) {
   using S = PassSmem<NY, P, C, C>;
   using F = typename S::F;
   using LM = typename S::LM;

@@ -473,3 +473,51 @@ def test_linearised_map_matches_the_reference_map(torch):
         ref.close()
         kr.close()
         S.close()
+
+
+def test_exponential_map_matches_the_reference_map(torch):
+    """ns3d_map_exponential against the reference's own RK3_SSP_UV steps
+    behind the reduced packing (oracle/ref_harness.cu
+    ref_map_exponential_reduced, the map of the converged IRA benchmark's
+    reference arm): two calls in a row, the base flow advancing with each,
+    with the Kolmogorov forcing on both sides."""
+    import ctypes
+
+    from ns3dperiodic_b200 import Solver
+
+    lib = os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref", "libns3d_ref.so")
+    if not os.path.exists(lib):
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    from oracle.ref_lib import RefSolver
+
+    g = O.Grid(16, 16, 16)
+    Re, dt, steps = 40.0, 4e-3, 3
+    U = _kolmogorov(g, Re, 9)
+    F = O.kolmogorov_forcing(g)
+    S = Solver(16, 16, 16)
+    S.set_forcing(S.to_device(F))
+    Ud, Vs = S.to_device(U), S.zeros()
+    n = S.krylov_length
+    kr = _kr(n, 2)
+    A = kr.exponential_map(S, Ud, Vs, dt, Re, steps)
+    ref = RefSolver(16, 16, 16)
+    try:
+        ref.set_u(U)
+        ref.set_f(F)
+        fn = ref.lib.ref_map_exponential_reduced
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        fn.restype = None
+        ctx = (ctypes.c_double * 3)(Re, dt, float(steps))
+        for seed in (1, 2):
+            x = torch.as_tensor(np.random.default_rng(seed).standard_normal(n), device="cuda")
+            y = torch.empty_like(x)
+            yr = torch.empty_like(x)
+            kr.apply(A, x, y)
+            fn(ctypes.cast(ctx, ctypes.c_void_p), x.data_ptr(), yr.data_ptr())
+            torch.cuda.synchronize()
+            assert O.rel_l2(y.cpu().numpy(), yr.cpu().numpy()) < 1e-12
+        assert O.rel_l2([u.cpu().numpy() for u in Ud], ref.get_u()) < 1e-12
+    finally:
+        ref.close()
+        kr.close()
+        S.close()
