@@ -37,9 +37,13 @@ constexpr int kWarpsPerCta = 4;
 #endif
 constexpr int kMinCtasXY = NS3D_MINCTA_XY;
 // The x / y passes' tiles of 8 points or fewer per thread (the autotuner's
-// alternative for long lines) ask for NS3D_MINCTA_XY8 CTAs per SM.
+// alternative for long lines) ask for NS3D_MINCTA_XY8 CTAs per SM (at most
+// 168 registers; 152-168 used, no spills).  B200, 256^3 with 3: the tuner
+// keeps the 8-point tiles of inv_x, inv_y and fwd_y (264 / 463 / 172 us
+// against 293 / 479 / 181 us), RK3 step 5.23 -> 5.08 ms; FP32 mode 4.05 ->
+// 3.94 ms; 128^3 unchanged (the 16-point defaults stay faster there).
 #ifndef NS3D_MINCTA_XY8
-#define NS3D_MINCTA_XY8 2
+#define NS3D_MINCTA_XY8 3
 #endif
 __host__ __device__ constexpr int min_ctas_xy(int p) { return p <= 8 ? NS3D_MINCTA_XY8 : kMinCtasXY; }
 constexpr int kMinCtasZ = NS3D_MINCTA_Z;

@@ -63,6 +63,12 @@ struct ns3d_solver {
   cudaStream_t rk3_stream = nullptr;
   int f_version = 0, rk3_fversion = -1;
   bool graphs_off = false;
+  // the captured tangent step (RK3_SSP_UV) of ns3d_jvp_steps and its key
+  cudaGraphExec_t jvp_exec = nullptr;
+  const void* jvp_key[6] = {};
+  double jvp_dt = 0.0, jvp_Re = 0.0;
+  cudaStream_t jvp_stream = nullptr;
+  int jvp_fversion = -1;
   size_t bytes = 0;
   std::string err;
 };
