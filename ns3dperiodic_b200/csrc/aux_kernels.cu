@@ -90,18 +90,29 @@ __device__ __forceinline__ double sq(double2 a) { return a.x * a.x + a.y * a.y; 
 // Parseval form of get_kinetic_energy / get_dissipation.  The central
 // difference (u(x+h) - u(x-h))/h is i*2 sin(k h)/h in Fourier space, so both
 // physical sums become weighted sums over the half spectrum (weight 1 on the
-// kz = 0 and kz = Nz/2 planes, 2 elsewhere).
+// kz = 0 and kz = Nz/2 planes, 2 elsewhere).  The per-direction factors
+// 2 sin(2 pi q / N) / h come from tables built once per block in shared
+// memory; each thread walks its modes with a stride of the whole grid and
+// carries (j, k, l) along instead of dividing the flat index; the divergence
+// maximum is taken over |div|^2 and rooted once per block.
 __global__ void diag_partial_kernel(const double2* __restrict__ ux, const double2* __restrict__ uy,
                                     const double2* __restrict__ uz, DiagGeom g,
                                     double* __restrict__ partial) {
-  const long long n = (long long)g.Nx * g.Ny * g.Mz;
-  double e = 0.0, d = 0.0, dv = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int l = (int)(i % g.Mz);
-    const long long jk = i / g.Mz;
-    const int k = (int)(jk % g.Ny);
-    const int j = (int)(jk / g.Ny);
+  __shared__ double tab_x[kDiagMaxExtent], tab_y[kDiagMaxExtent], tab_z[kDiagMaxExtent / 2 + 1];
+  for (int q = threadIdx.x; q < g.Nx; q += blockDim.x)
+    tab_x[q] = 2.0 * sinpi(2.0 * (double)q / g.Nx) / g.dx;
+  for (int q = threadIdx.x; q < g.Ny; q += blockDim.x)
+    tab_y[q] = 2.0 * sinpi(2.0 * (double)q / g.Ny) / g.dy;
+  for (int q = threadIdx.x; q < g.Mz; q += blockDim.x)
+    tab_z[q] = 2.0 * sinpi(2.0 * (double)q / g.Nz) / g.dz;
+  __syncthreads();
+  const int n = g.Nx * g.Ny * g.Mz;  // below 2^31 for every compiled grid
+  const int S = gridDim.x * blockDim.x;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int l = i % g.Mz, k = (i / g.Mz) % g.Ny, j = (i / g.Mz) / g.Ny;
+  const int Sl = S % g.Mz, Sk = (S / g.Mz) % g.Ny, Sj = (S / g.Mz) / g.Ny;
+  double e = 0.0, d = 0.0, dv2 = 0.0;
+  for (; i < n; i += S) {
     const int m = j < g.Nx / 2 ? j : j - g.Nx;  // reference signed index (Nyquist -> -N/2)
     const int nn = k < g.Ny / 2 ? k : k - g.Ny;
     double2 a = ux[i], b = uy[i], c = uz[i];
@@ -110,7 +121,7 @@ __global__ void diag_partial_kernel(const double2* __restrict__ ux, const double
       const double kx = g.kfx * (double)m, ky = g.kfy * (double)nn, kz = g.kfz * (double)l;
       const double re = -a.y * kx - b.y * ky - c.y * kz;
       const double im = a.x * kx + b.x * ky + c.x * kz;
-      dv = fmax(dv, sqrt(re * re + im * im));
+      dv2 = fmax(dv2, re * re + im * im);
     }
     const bool edge = (l == 0) || (2 * l == g.Nz);
     double w = 2.0;
@@ -124,9 +135,7 @@ __global__ void diag_partial_kernel(const double2* __restrict__ ux, const double
       c = herm(uz, c, mi);
     }
     e += w * (sq(b) + sq(c));
-    const double Dx = 2.0 * sinpi(2.0 * (double)j / g.Nx) / g.dx;
-    const double Dy = 2.0 * sinpi(2.0 * (double)k / g.Ny) / g.dy;
-    const double Dz = 2.0 * sinpi(2.0 * (double)l / g.Nz) / g.dz;
+    const double Dx = tab_x[j], Dy = tab_y[k], Dz = tab_z[l];
     // |d_b u_a| up to the common factor i: D_b * u_a
     const double2 xx = make_double2(Dx * a.x, Dx * a.y), yy = make_double2(Dy * b.x, Dy * b.y);
     const double2 zz = make_double2(Dz * c.x, Dz * c.y);
@@ -134,30 +143,38 @@ __global__ void diag_partial_kernel(const double2* __restrict__ ux, const double
     const double2 xz = make_double2(Dz * a.x + Dx * c.x, Dz * a.y + Dx * c.y);
     const double2 xy = make_double2(Dy * a.x + Dx * b.x, Dy * a.y + Dx * b.y);
     d += w * (2.0 * (sq(xx) + sq(yy) + sq(zz)) + sq(yz) + sq(xz) + sq(xy));
+    // (j, k, l) of i + S
+    l += Sl;
+    int carry = l >= g.Mz;
+    l -= carry ? g.Mz : 0;
+    k += Sk + carry;
+    carry = k >= g.Ny;
+    k -= carry ? g.Ny : 0;
+    j += Sj + carry;
   }
   __shared__ double red[3][32];
   e = warp_sum(e);
   d = warp_sum(d);
-  dv = warp_max(dv);
+  dv2 = warp_max(dv2);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) {
     red[0][warp] = e;
     red[1][warp] = d;
-    red[2][warp] = dv;
+    red[2][warp] = dv2;
   }
   __syncthreads();
   if (warp == 0) {
     const int nw = blockDim.x >> 5;
     e = lane < nw ? red[0][lane] : 0.0;
     d = lane < nw ? red[1][lane] : 0.0;
-    dv = lane < nw ? red[2][lane] : 0.0;
+    dv2 = lane < nw ? red[2][lane] : 0.0;
     e = warp_sum(e);
     d = warp_sum(d);
-    dv = warp_max(dv);
+    dv2 = warp_max(dv2);
     if (lane == 0) {
       partial[3 * blockIdx.x + 0] = 0.5 * g.dx * g.dy * g.inv_vol * e;
       partial[3 * blockIdx.x + 1] = g.dx * g.dy * g.dz * g.inv_vol * d;
-      partial[3 * blockIdx.x + 2] = dv;
+      partial[3 * blockIdx.x + 2] = sqrt(dv2);  // max |div| (sqrt is monotonic)
     }
   }
 }

@@ -38,6 +38,9 @@ struct DiagGeom {
   double inv_vol;        // 1/(Nx Ny Nz)
 };
 
+// Largest extent per direction (the compiled extents go to 512).
+constexpr int kDiagMaxExtent = 512;
+
 // Per-block partial sums: [0] energy, [1] dissipation, [2] max |div|.
 __global__ void diag_partial_kernel(const double2* __restrict__ ux, const double2* __restrict__ uy,
                                     const double2* __restrict__ uz, DiagGeom g,

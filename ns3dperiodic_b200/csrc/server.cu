@@ -238,7 +238,17 @@ struct Group {
   double* norm_host = nullptr;    // pinned
   std::deque<long long> queue;    // requests of this grid not yet admitted, arrival order
   long long instance_steps = 0;   // JVP steps launched, summed over the active slots
+  // captured JVP step per active-slot count (index active - 1): the 25
+  // launches replay as one graph; dropped when tiles, precision or forcing change
+  std::vector<cudaGraphExec_t> step_exec;
+  bool graphs_off = false;
 };
+
+void drop_step_graphs(Group& g) {
+  for (auto& e : g.step_exec)
+    if (e) cudaGraphExecDestroy(e);
+  g.step_exec.clear();
+}
 
 }  // namespace
 
@@ -431,8 +441,33 @@ ns3d_status launch_step(ns3d_server* s, Group& g) {
   cudaStream_t st = g.h->stream;
   SRV_CHECK(s, cudaMemcpyAsync(g.h->dtRe, g.params_host, sizeof(double) * 2 * active,
                                cudaMemcpyHostToDevice, st), "params");
-  const ns3d_status r = jvp_step_active(g.h, g.u, g.v, active);
-  if (r != NS3D_OK) return sfail(s, r, std::string("jvp step: ") + ns3d_last_error(g.h));
+  if ((int)g.step_exec.size() < g.capacity) g.step_exec.resize((size_t)g.capacity, nullptr);
+  cudaGraphExec_t& exec = g.step_exec[(size_t)active - 1];
+  if (!exec && !g.graphs_off) {
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const ns3d_status r = jvp_step_active(g.h, g.u, g.v, active);
+      e = cudaStreamEndCapture(st, &graph);
+      if (r != NS3D_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return sfail(s, r, std::string("jvp step: ") + ns3d_last_error(g.h));
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+    }
+    if (e != cudaSuccess) {  // launch directly from now on
+      cudaGetLastError();
+      exec = nullptr;
+      g.graphs_off = true;
+    }
+  }
+  if (exec) {
+    SRV_CHECK(s, cudaGraphLaunch(exec, st), "step graph");
+  } else {
+    const ns3d_status r = jvp_step_active(g.h, g.u, g.v, active);
+    if (r != NS3D_OK) return sfail(s, r, std::string("jvp step: ") + ns3d_last_error(g.h));
+  }
   for (auto& sl : g.slots) ++sl.steps_launched;
   g.instance_steps += active;
   SRV_CHECK(s, cudaEventRecord(g.ev, st), "event");
@@ -597,6 +632,7 @@ ns3d_status ns3d_server_destroy(ns3d_server* s) {
   if (!s) return NS3D_ERR_BAD_ARG;
   for (auto& g : s->groups) {
     if (g.h) cudaStreamSynchronize(g.h->stream);
+    drop_step_graphs(g);
     for (int c = 0; c < 3; ++c) {
       cudaFree(g.u[c]);
       cudaFree(g.v[c]);
@@ -629,6 +665,7 @@ ns3d_status ns3d_server_set_precision(ns3d_server* s, int precision) {
     if (g.busy) return sfail(s, NS3D_ERR_BAD_ARG, "set the precision between runs");
     const ns3d_status st = ns3d_set_precision(g.h, precision);
     if (st != NS3D_OK) return sfail(s, st, ns3d_last_error(g.h));
+    drop_step_graphs(g);
   }
   return NS3D_OK;
 }
@@ -640,6 +677,7 @@ ns3d_status ns3d_server_autotune(ns3d_server* s, int reps) {
     g.h->geom.batch = g.h->batch;  // tune for the full slot count
     const ns3d_status st = ns3d_autotune(g.h, reps, 0, nullptr);
     if (st != NS3D_OK) return sfail(s, st, ns3d_last_error(g.h));
+    drop_step_graphs(g);
   }
   return NS3D_OK;
 }
@@ -725,6 +763,7 @@ ns3d_status ns3d_server_set_forcing(ns3d_server* s, int N, const ns3d_complex* f
   if (g->busy) return sfail(s, NS3D_ERR_BAD_ARG, "set the forcing between runs");
   const ns3d_status st = ns3d_set_forcing(g->h, fx, fy, fz);
   if (st != NS3D_OK) return sfail(s, st, ns3d_last_error(g->h));
+  drop_step_graphs(*g);
   return NS3D_OK;
 }
 
