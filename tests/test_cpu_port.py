@@ -16,7 +16,8 @@ TOL = 1e-12
 @pytest.fixture(scope="module")
 def port():
     if not cpu_lib.available():
-        subprocess.run(["make", "-C", os.path.dirname(cpu_lib.LIB_PATH) + "/..", "cpu"],
+        # the oracle folder itself: _cpu/ does not exist before the first build
+        subprocess.run(["make", "-C", os.path.dirname(os.path.dirname(cpu_lib.LIB_PATH)), "cpu"],
                        check=True, capture_output=True)
     return cpu_lib
 
