@@ -350,7 +350,10 @@ def run_ours(args, world, rank, local, pg):
     # velocities in shared memory for FP64 lines; the ring-pipelined fwd_x
     # where a line fits in a warp (8 points per thread, 12 for multiples of 3)
     ring = N // (12 if N % 3 == 0 else min(N, 8)) <= 32
-    kname = {0: "inv_x_kernel", 1: "inv_y_kernel", 2: "z_kernel" if fp32 else "z_kernel_st",
+    # inv_y's tile 2 is the bulk-copy (TMA) form for FP64 lines
+    ytma = S.tiles[1] == 2 and not fp32
+    kname = {0: "inv_x_kernel", 1: "inv_y_tma_kernel" if ytma else "inv_y_kernel",
+             2: "z_kernel" if fp32 else "z_kernel_st",
              3: "fwd_y_kernel", 4: "fwd_x_ring_kernel" if ring else "fwd_x_kernel"}[dom]
     traffic = traffic_from_profiles(kname, N)
     roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),

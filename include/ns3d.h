@@ -347,22 +347,30 @@ ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns
  * 3) and, for extents >= 32 (powers of two) or >= 48 (multiples of 3), an
  * alternative one (8 or 6 points per thread: twice the lines per CTA, half
  * the registers and prefetch buffers).  tiles[f] = 0 picks the default, 1
- * the alternative.  Different tiles change the order of the floating-point
- * operations of the transforms, so results agree to round-off, not bit for
- * bit.  The tiles are per precision; a new handle starts with the defaults. */
+ * the alternative.  The inv_y family has a third tile, 2, for y extents of
+ * 192, 256, 384 and 512: the bulk-copy form, where one thread per CTA loads
+ * each field's whole box of lines into shared memory with a tensor copy (TMA)
+ * instead of every thread copying its own samples (the tangent form and the
+ * FP32 mode run the per-thread copies at the same points per thread).
+ * Different tiles change the order of the floating-point operations of the
+ * transforms, so results agree to round-off, not bit for bit.  The tiles are
+ * per precision; a new handle starts with the defaults. */
 #define NS3D_TILE_FAMILIES 4
+#define NS3D_TUNE_TIMES 9
 ns3d_status ns3d_get_tiles(const ns3d_solver* h, int* tiles);
-/* NS3D_ERR_BAD_ARG for a value other than 0/1 or an alternative the extent
- * lacks.  Synchronises the handle's stream. */
+/* NS3D_ERR_BAD_ARG for a value other than 0/1 (or 2 for inv_y), or a tile
+ * the extent lacks.  Synchronises the handle's stream. */
 ns3d_status ns3d_set_tiles(ns3d_solver* h, const int* tiles);
 /* Times every family with each of its tiles on the handle's own scratch
  * (`reps` launches after one warm-up, CUDA events, as ns3d_profile_passes;
  * the state is not touched), keeps the alternative where it is at least 2%
  * faster, and applies the choice.  Choices are cached per process and
  * device for (Nx, Ny, Nz, batch, precision): unless `force`, a cached
- * choice is applied without timing.  ms (8 doubles, may be NULL) receives
- * per family the mean ms of the default and the alternative tile (-1: not
- * timed).  Synchronous. */
+ * choice is applied without timing.  ms (NS3D_TUNE_TIMES = 9 doubles, may
+ * be NULL) receives per family the mean ms of the default and the
+ * alternative tile, then that of inv_y's bulk-copy tile (-1: not timed).
+ * The bulk-copy tile is kept where it is 2% faster than the better of the
+ * other two.  Synchronous. */
 ns3d_status ns3d_autotune(ns3d_solver* h, int reps, int force, double* ms);
 
 /* ----------------------------------------------------------------------- */

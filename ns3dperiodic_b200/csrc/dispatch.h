@@ -12,6 +12,9 @@ namespace ns3d {
 bool extent_supported(int n);
 // whether extent n has an alternative tile for the autotuner (p_alt)
 bool extent_has_alt_tile(int n);
+// lines per CTA of inv_y's bulk-copy (TMA) form (tile 2 of the inv_y family)
+// for extent n, 0 when the extent has no such form
+int inv_y_tma_lpc(int n);
 
 // FP64 scratch (double2) and the FP32 precision mode (float2 scratch).
 cudaError_t run_inv_x(const InvXArgs<3>& a, const PassGeom& g, cudaStream_t st);

@@ -6,6 +6,7 @@ namespace ns3d {
 
 bool extent_supported(int n) { return extent_supported_inline(n); }
 bool extent_has_alt_tile(int n) { return has_alt_tile(n); }
+int inv_y_tma_lpc(int n) { return inv_y_tma_lpc_inline(n); }
 
 cudaError_t run_inv_x(const InvXArgs<3>& a, const PassGeom& g, cudaStream_t st) {
   return launch_inv_x<3>(a, g, st);
@@ -51,9 +52,11 @@ cudaError_t prepare_xy_prec(const PassGeom& g) {
 }  // namespace
 
 cudaError_t prepare_xy(const PassGeom& g) {
-  for (int tile = 0; tile < 2; ++tile) {  // both tiles of every pass family
+  // both tiles of every pass family, then the inv_y family's bulk-copy tile
+  for (int tile = 0; tile < 3; ++tile) {
     PassGeom gt = g;
-    for (int& f : gt.tile) f = tile;
+    for (int& f : gt.tile) f = tile < 2 ? tile : 0;
+    if (tile == 2) gt.tile[kTileInvY] = 2;
     cudaError_t e = prepare_xy_prec<double2>(gt);
     if (e == cudaSuccess) e = prepare_xy_prec<float2>(gt);
     if (e != cudaSuccess) return e;

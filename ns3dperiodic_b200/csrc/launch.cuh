@@ -74,6 +74,41 @@ inline bool has_alt_tile(int n) {
   }
 }
 
+// The bulk-copy (TMA) form of inv_y (inv_y_tma_kernel): FP64 lines spread
+// over the CTA.  It is tile 2 of the inv_y family, at p_tma(n) points per
+// thread (the default or the alternative points per thread, whichever
+// spreads its lines over the CTA; 0: no such form for this extent), and runs
+// where the handle built tensor maps for its scratch; the tangent form and
+// the FP32 mode run the cp.async form at p_tma(n) points per thread instead.
+// NS3D_Y_TMA 0 compiles no bulk-copy form.
+#ifndef NS3D_Y_TMA
+#define NS3D_Y_TMA 1
+#endif
+// 1: the TMA form runs persistent CTAs (resident CTAs, groups dealt round
+// robin), so each CTA's copy ring runs across many groups; 0: NS3D_SCHED.
+#ifndef NS3D_Y_TMA_PERSIST
+#define NS3D_Y_TMA_PERSIST 0
+#endif
+constexpr int p_tma(int n) {
+  return NS3D_Y_TMA == 0                              ? 0
+         : n / p_xy(n) >= 32                          ? p_xy(n)
+         : (p_alt(n) > 0 && n / p_alt(n) >= 32) ? p_alt(n)
+                                                      : 0;
+}
+
+// Lines per CTA of the TMA form of inv_y for extent n, 0 when it has none.
+inline int inv_y_tma_lpc_inline(int n) {
+  switch (n) {
+#define NS3D_CASE(N) \
+  case N:            \
+    return p_tma(N) > 0 ? LaneMap<N / (p_tma(N) > 0 ? p_tma(N) : 1)>::LPC : 0;
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    default:
+      return 0;
+  }
+}
+
 inline bool extent_supported_inline(int n) {
   switch (n) {
 #define NS3D_CASE(N) case N:
@@ -104,7 +139,9 @@ struct KTag {};
 
 // The caches are atomics: host threads that launch on the same device may
 // race to fill them, and each writes the same values.
-template <typename Tag, typename Kern>
+// kCap: cap the grid at the resident CTAs whatever NS3D_SCHED says (kernels
+// whose CTAs keep a copy pipeline running across their groups).
+template <typename Tag, bool kCap = (NS3D_SCHED != 0), typename Kern>
 inline unsigned persistent_grid(Kern kern, size_t smem, long long groups) {
   static std::atomic<int> per_sm[64] = {};
   static std::atomic<int> sms[64] = {};
@@ -120,8 +157,7 @@ inline unsigned persistent_grid(Kern kern, size_t smem, long long groups) {
     sms[dev].store(n > 0 ? n : 1, std::memory_order_relaxed);
     per_sm[dev].store(occ > 0 ? occ : 1, std::memory_order_release);
   }
-  const long long cap =
-      NS3D_SCHED == 0 ? groups : (long long)sms[dev].load() * per_sm[dev].load();
+  const long long cap = !kCap ? groups : (long long)sms[dev].load() * per_sm[dev].load();
   return (unsigned)(groups < cap ? (groups > 0 ? groups : 1) : cap);
 }
 
@@ -159,9 +195,36 @@ cudaError_t launch_inv_x(const InvXArgs<NF, C>& a, const PassGeom& g, cudaStream
   }
 }
 
+template <int N, int P>
+cudaError_t launch_inv_y_tma(const InvYArgs<3, double2>& a, const PassGeom& g, cudaStream_t st,
+                             bool prepare_only) {
+  using S = InvYTmaSmem<N, P>;
+  const long long groups = (long long)g.Nx * ((g.Mz + S::LPC - 1) / S::LPC);
+  const unsigned grid = persistent_grid<KTag<90, N, P, 3>, NS3D_Y_TMA_PERSIST != 0>(
+      inv_y_tma_kernel<N, P, 3>, S::BYTES, groups);
+  if (prepare_only) return cudaGetLastError();
+  InvYTmaArgs<3> t;
+  t.m = *a.maps;
+  for (int f = 0; f < 3; ++f) {
+    t.C[f] = a.C[f];
+    t.D[f] = a.D[f];
+    t.E[f] = a.E[f];
+  }
+  t.tw = a.tw;
+  t.err = a.err;
+  inv_y_tma_kernel<N, P, 3><<<grid, kThreads, S::BYTES, st>>>(t, g);
+  return cudaGetLastError();
+}
+
 template <int N, int P, int NF, typename C>
 cudaError_t launch_inv_y_p(const InvYArgs<NF, C>& a, const PassGeom& g, cudaStream_t st,
-                           bool prepare_only) {
+                           bool prepare_only, bool bulk = false) {
+  if constexpr (NF == 3 && sizeof(C) == 16 && P == p_tma(N)) {
+    if (bulk && (a.maps || prepare_only)) {
+      const cudaError_t e = launch_inv_y_tma<N, P>(a, g, st, prepare_only);
+      if (!prepare_only || e != cudaSuccess) return e;
+    }
+  }
   const long long lines = (long long)g.Nx * g.Mz;
   using S = PassSmem<N, P, C, C>;
   const unsigned grid = persistent_grid<KTag<1, N, P, NF + prec_tag<C>()>>(
@@ -178,8 +241,12 @@ cudaError_t launch_inv_y(const InvYArgs<NF, C>& a, const PassGeom& gi, cudaStrea
   switch (g.Ny) {
 #define NS3D_CASE(N)                                                         \
   case N:                                                                    \
+    if constexpr (p_tma(N) > 0) {                                            \
+      if (g.tile[kTileInvY] == 2)                                            \
+        return launch_inv_y_p<N, p_tma(N), NF, C>(a, g, st, prepare_only, true); \
+    }                                                                        \
     if constexpr (p_alt(N) > 0) {                                            \
-      if (g.tile[kTileInvY])                                                 \
+      if (g.tile[kTileInvY] == 1)                                            \
         return launch_inv_y_p<N, p_alt(N), NF, C>(a, g, st, prepare_only);   \
     }                                                                        \
     return launch_inv_y_p<N, p_xy(N), NF, C>(a, g, st, prepare_only);

@@ -21,6 +21,7 @@
 #include <cstdint>
 
 #include "fft_engine.cuh"
+#include "tma.cuh"
 
 namespace ns3d {
 
@@ -338,6 +339,7 @@ __global__ void __launch_bounds__(kThreads, min_ctas_xy(P)) inv_x_kernel(InvXArg
 // ---------------------------------------------------------------------------
 // inv_y: lines along y, batch b = x*Mz + z, base = x*Ny*Mz + z, stride Mz
 // ---------------------------------------------------------------------------
+struct InvYMaps;
 template <int NF, typename Cx = double2>
 struct InvYArgs {
   const Cx* A[NF];
@@ -346,6 +348,10 @@ struct InvYArgs {
   Cx* D[NF];
   Cx* E[NF];
   const double2* tw;
+  // tensor maps over A and B for the bulk-copy form of the nonlinear term's
+  // pass (InvYMaps, built for the handle's scratch), or null
+  const InvYMaps* maps = nullptr;
+  int* err = nullptr;  // error flag of the bulk-copy form's bounded waits
 };
 
 template <int NY, int P, int NF, typename C>
@@ -437,6 +443,169 @@ __global__ void __launch_bounds__(kThreads, min_ctas_xy(P)) inv_y_kernel(InvYArg
     }
   }
   cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// inv_y fed by bulk tensor copies (TMA), FP64 lines spread over the CTA.
+//
+// The cp.async form makes every thread issue P 16-byte copies per unit (a
+// field of the group's lines): at 12 warps per SM the memory-instruction
+// queue saturates (MIO-throttle and long-scoreboard stalls).  Here one thread
+// asks the TMA unit for a unit's whole box - the LPC consecutive z lines of
+// one x plane, all Ny samples - with one instruction per 256 samples, into a
+// ring of NST shared-memory slots whose completions are counted on
+// mbarriers; the other threads only wait and read.  A group never straddles
+// two x planes: a plane has ceil(Mz / LPC) groups, and the lines past Mz of
+// its last group are filled with zeros by the copy and not stored.  In a
+// slot, sample y of line li sits at y * LPC + li (the box's own order), so
+// the lanes of a load (consecutive li, then t) read consecutive 16-byte
+// words.  A slot is refilled only after every thread has passed the CTA
+// barrier at the start of the transforms of the unit that used it, and only
+// after the issuing thread's own wait for that unit succeeded: a slot's
+// barrier never holds two armed phases.  When a wait gives up, the issuer
+// stops issuing and, before it returns, drains (with bounded waits) the
+// copies it issued and did not see complete.
+// ---------------------------------------------------------------------------
+// Rows of one box along y: the largest divisor of ny that is at most 256
+// (the longest box side a tensor map allows); a unit takes ny / that boxes.
+constexpr int tma_box_y(int ny, int b = 256) {
+  return b <= 1 ? 1 : (ny % b == 0 ? b : tma_box_y(ny, b - 1));
+}
+
+// Tensor maps of one pass: A_f at 2f, B_f at 2f + 1.  Dimensions (2 Mz
+// doubles, Ny, planes), box (2 LPC, tma_box_y(Ny), 1).
+struct alignas(64) InvYMaps {
+  CUtensorMap map[6];
+};
+
+template <int NF>
+struct alignas(64) InvYTmaArgs {
+  InvYMaps m;
+  double2* C[NF];
+  double2* D[NF];
+  double2* E[NF];
+  const double2* tw;
+  int* err;
+};
+
+template <int NY, int P>
+struct InvYTmaSmem {
+  using F = LineFFT<NY, P>;
+  using LM = LaneMap<F::T>;
+  static constexpr int LPC = LM::LPC;
+  static constexpr int STRIDE = line_stride(F::BUF, xy_stride_target<F::T>());
+  static constexpr int BOXY = tma_box_y(NY);
+  static constexpr uint32_t SLOT = (uint32_t)NY * LPC * sizeof(double2);
+  static constexpr size_t REST = align16((size_t)F::TWLEN * sizeof(double2)) +
+                                 align16((size_t)LPC * STRIDE * sizeof(double2)) + 64;
+  // ring depth: 3 slots where the CTAs the registers allow still fit, else 2
+  static constexpr int NST =
+      (3 * (size_t)SLOT + REST) * (size_t)min_ctas_xy(P) <= 227 * 1024 ? 3 : 2;
+  static constexpr size_t TW_OFF = (size_t)NST * SLOT;  // slots are 128-byte multiples
+  static constexpr size_t SBUF_OFF = TW_OFF + align16((size_t)F::TWLEN * sizeof(double2));
+  static constexpr size_t BAR_OFF = SBUF_OFF + align16((size_t)LPC * STRIDE * sizeof(double2));
+  static constexpr size_t BAD_OFF = BAR_OFF + 8 * NST;  // the CTA's broken-ring flag
+  static constexpr size_t BYTES = BAD_OFF + 8;
+  static_assert(SLOT % 128 == 0, "slot alignment");
+  static_assert(NY % BOXY == 0 && (BOXY * LPC * sizeof(double2)) % 128 == 0, "box alignment");
+  static_assert(BYTES * min_ctas_xy(P) <= 227 * 1024 || min_ctas_xy(P) <= 1, "CTAs per SM");
+};
+
+template <int NY, int P, int NF>
+__global__ void __launch_bounds__(kThreads, min_ctas_xy(P))
+    inv_y_tma_kernel(const __grid_constant__ InvYTmaArgs<NF> a, PassGeom g) {
+  using S = InvYTmaSmem<NY, P>;
+  using F = typename S::F;
+  using LM = typename S::LM;
+  static_assert(LM::kSpread, "lines spread over the CTA");
+  constexpr int T = F::T, LPC = LM::LPC, NST = S::NST;
+  constexpr int UPG = 2 * NF;  // units per group: A_f, B_f
+  extern __shared__ __align__(128) unsigned char dsm[];
+  double2* tw_s = (double2*)(dsm + S::TW_OFF);
+  uint64_t* full = (uint64_t*)(dsm + S::BAR_OFF);
+  int li, t;
+  LM::get(li, t);
+  double2* sbuf = (double2*)(dsm + S::SBUF_OFF) + li * S::STRIDE;
+  const int gpp = (g.Mz + LPC - 1) / LPC;  // groups per x plane
+  const int groups = g.Nx * gpp;
+  const GroupRange gr = group_range(groups);
+  if (gr.grp >= gr.end) return;  // uniform across the CTA
+  const int ngrp = (gr.end - gr.grp + gr.step - 1) / gr.step;
+  const int nunits = ngrp * UPG;
+  volatile int* bad = (volatile int*)(dsm + S::BAD_OFF);  // a wait of this CTA gave up
+  auto issue = [&](int k) {  // thread 0
+    const int gi = k / UPG, j = k - gi * UPG;
+    const int grp = gr.grp + gi * gr.step;
+    const int x = grp / gpp, z0 = (grp - x * gpp) * LPC;
+    unsigned char* dst = dsm + (size_t)(k % NST) * S::SLOT;
+    uint64_t* bar = &full[k % NST];
+    mbar_expect_tx(bar, S::SLOT);
+#pragma unroll
+    for (int by = 0; by < NY / S::BOXY; ++by)
+      tma_load_3d(dst + (size_t)by * S::BOXY * LPC * sizeof(double2), &a.m.map[j], 2 * z0,
+                  by * S::BOXY, x, bar);
+  };
+  // thread 0: units issued so far, and the first whose completion it did not see
+  int issued = 0, unseen = nunits;
+  if (threadIdx.x == 0) {
+    // a slot ring off its 128-byte alignment: no copies, the host sees the
+    // flag at its next synchronisation
+    *bad = (smem_u32(dsm) & 127u) != 0u;
+    if (*bad && a.err) atomicExch(a.err, kErrTimeout);
+    for (int s = 0; s < NST; ++s) mbar_init(&full[s], 1);
+    mbar_init_fence();
+    // the first copies start before the twiddle table is read
+    if (!*bad)
+      for (; issued < NST - 1 && issued < nunits; ++issued) issue(issued);
+  }
+  F::load_tw(tw_s, a.tw);  // ends with a CTA barrier: the barriers are initialised
+  if (*bad) return;        // uniform: read after the barrier
+  for (int k = 0; k < nunits; ++k) {
+    if (threadIdx.x == 0 && unseen == nunits && k + NST - 1 < nunits) {
+      fence_proxy_async_smem();  // the slot's earlier reads (generic proxy) come first
+      issue(k + NST - 1);
+      issued = k + NST;
+    }
+    const bool seen = mbar_wait(&full[k % NST], (uint32_t)((k / NST) & 1), a.err, bad);
+    if (threadIdx.x == 0 && !seen && unseen == nunits) unseen = k;
+    const double2* cur = (const double2*)(dsm + (size_t)(k % NST) * S::SLOT) + li;
+    const int gi = k / UPG, j = k - gi * UPG, f = j >> 1;
+    const int grp = gr.grp + gi * gr.step;
+    const int x = grp / gpp, z = (grp - x * gpp) * LPC + li;
+    const bool valid = z < g.Mz;
+    const size_t base = (size_t)x * g.Ny * g.Mz + (valid ? z : 0);
+    const size_t stride = (size_t)g.Mz;
+    double2 v[P];
+#pragma unroll
+    for (int s = 0; s < P; ++s) v[s] = cur[(t + T * s) * LPC];
+    F::template run<+1, F::PADW, LM::SW>(v, t, sbuf, tw_s);
+    if ((j & 1) == 0) {
+      // unit A_f -> C_f = IFFT_y A, D_f = IFFT_y(i ky A)
+      if (valid) {
+#pragma unroll
+        for (int s = 0; s < P; ++s) a.C[f][base + (size_t)(t + T * s) * stride] = v[s];
+      }
+#pragma unroll
+      for (int s = 0; s < P; ++s) {
+        const double2 u = cur[(t + T * s) * LPC];
+        const double ky = g.kfy * (double)signed_idx(t + T * s, NY);
+        v[s] = make_double2(-u.y * ky, u.x * ky);
+      }
+      F::template run<+1, F::PADW, LM::SW>(v, t, sbuf, tw_s);
+      if (valid) {
+#pragma unroll
+        for (int s = 0; s < P; ++s) a.D[f][base + (size_t)(t + T * s) * stride] = v[s];
+      }
+    } else {
+      // unit B_f -> E_f = IFFT_y B
+      if (valid) {
+#pragma unroll
+        for (int s = 0; s < P; ++s) a.E[f][base + (size_t)(t + T * s) * stride] = v[s];
+      }
+    }
+  }
+  if (threadIdx.x == 0)  // a broken ring: the copies that may still be in flight
+    for (int k = unseen; k < issued; ++k) mbar_drain(&full[k % NST], (uint32_t)((k / NST) & 1));
 }
 
 // ---------------------------------------------------------------------------

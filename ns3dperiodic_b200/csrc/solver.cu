@@ -10,6 +10,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 
 #include "../../include/ns3d.h"
 #include "aux_kernels.cuh"
@@ -141,6 +142,10 @@ ns3d_status conv_front_t(ns3d_solver* h, const double2* const u[3],
     ax.qcut = h->qcut; ax.tw = h->tw[0];
     ay.tw = h->tw[1];
     az.tw = h->tw[2];
+    if (sizeof(C) == 16 && g.tile[ns3d::kTileInvY] == 2) {  // FP64: the bulk-copy form
+      ay.maps = h->ymaps;
+      ay.err = h->dev_err;
+    }
     NS3D_CHECK(h, ns3d::run_inv_x(ax, g, st), "inv_x");
     NS3D_CHECK(h, ns3d::run_inv_y(ay, g, st), "inv_y");
     NS3D_CHECK(h, ns3d::run_z(az, g, st), "z");
@@ -295,6 +300,63 @@ ns3d_status ns3d_twiddles(int N, double* tw) {
 
 extern "C++" {
 namespace ns3d_detail {
+// L2 promotion of inv_y's bulk copies (CUtensorMapL2promotion: 0 none,
+// 1 64 B, 2 128 B, 3 256 B)
+#ifndef NS3D_TMA_L2PROMO
+#define NS3D_TMA_L2PROMO 3
+#endif
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link the driver; null when it is not available)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// Tensor maps of inv_y's bulk-copy form over the FP64 scratch A_f, B_f (all
+// instances of a batch as x planes).  A field is dims (2 Mz doubles, Ny,
+// planes) with row strides Mz * 16 and Ny * Mz * 16 bytes; a box is
+// (2 LPC, tma_box_y(Ny), 1).  Any failure leaves the handle without the form
+// (ns3d_set_tiles then refuses tile 2 of the inv_y family).
+void build_inv_y_maps(ns3d_solver* h) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return;
+  {
+    const int lpc = ns3d::inv_y_tma_lpc(h->Ny);
+    if (lpc <= 0) return;
+    auto* m = new ns3d::InvYMaps();
+    bool ok = true;
+    for (int f = 0; f < 6 && ok; ++f) {
+      const double2* base = (f & 1) ? h->B[f >> 1] : h->A[f >> 1];
+      const cuuint64_t dims[3] = {2ull * (cuuint64_t)h->Mz, (cuuint64_t)h->Ny,
+                                  (cuuint64_t)h->Nx * (cuuint64_t)h->batch};
+      const cuuint64_t strides[2] = {16ull * (cuuint64_t)h->Mz,
+                                     16ull * (cuuint64_t)h->Mz * (cuuint64_t)h->Ny};
+      const cuuint32_t box[3] = {2u * (cuuint32_t)lpc, (cuuint32_t)ns3d::tma_box_y(h->Ny), 1u};
+      const cuuint32_t estr[3] = {1u, 1u, 1u};
+      ok = enc(&m->map[f], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)base, dims, strides, box,
+               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               (CUtensorMapL2promotion)NS3D_TMA_L2PROMO, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+    }
+    if (ok) {
+      h->ymaps = m;
+    } else {
+      delete m;
+    }
+  }
+}
+
 ns3d_status create_solver(int batch, int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
                           ns3d_solver** out) {
   if (!out) return NS3D_ERR_BAD_ARG;
@@ -360,6 +422,9 @@ ns3d_status create_solver(int batch, int Nx, int Ny, int Nz, double Lx, double L
       cudaMalloc(&h->diag_partial, sizeof(double) * 3 * kDiagBlocks) != cudaSuccess ||
       cudaMalloc(&h->diag_out, sizeof(double) * 3 * batch) != cudaSuccess)
     return bail(NS3D_ERR_OOM);
+  if (cudaMalloc(&h->dev_err, sizeof(int)) != cudaSuccess) return bail(NS3D_ERR_OOM);
+  cudaMemset(h->dev_err, 0, sizeof(int));
+  build_inv_y_maps(h);
   if (batch > 1) {
     if (cudaMalloc(&h->dtRe, sizeof(double) * 2 * batch) != cudaSuccess) return bail(NS3D_ERR_OOM);
     std::vector<double> ones(2 * batch, 1.0);
@@ -398,6 +463,8 @@ ns3d_status ns3d_destroy(ns3d_solver* h) {
   cudaFree(h->rec_tab);
   cudaFree(h->rec_partial);
   cudaFree(h->rec_out);
+  cudaFree(h->dev_err);
+  delete h->ymaps;
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return NS3D_OK;
@@ -419,6 +486,17 @@ ns3d_status ns3d_set_stream(ns3d_solver* h, void* stream) {
 ns3d_status ns3d_synchronize(ns3d_solver* h) {
   NS3D_TRY(check_handle(h));
   NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+  // a bounded wait of a bulk-copy pass that gave up (its results are invalid)
+  int flag = 0;
+  if (h->dev_err) {
+    NS3D_CHECK(h, cudaMemcpyAsync(&flag, h->dev_err, sizeof(int), cudaMemcpyDeviceToHost,
+                                  h->stream), "error flag");
+    NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "error flag");
+  }
+  if (flag) {
+    cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream);
+    return fail(h, NS3D_ERR_TIMEOUT, "a bounded wait of a pass kernel gave up");
+  }
   return NS3D_OK;
 }
 
@@ -1184,6 +1262,10 @@ ns3d_status profile_passes_t(ns3d_solver* h, const ns3d_complex* ux, const ns3d_
   }
   ax.qcut = h->qcut; ax.tw = h->tw[0];
   ay.tw = h->tw[1]; az.tw = h->tw[2]; fy.tw = h->tw[1]; fx.tw = h->tw[0];
+  if (sizeof(C) == 16 && g.tile[ns3d::kTileInvY] == 2) {  // as conv_front
+    ay.maps = h->ymaps;
+    ay.err = h->dev_err;
+  }
   fx.fidx = h->f_idx; fx.fval = h->f_val; fx.fnnz = h->f_dense[0] ? 0 : h->f_nnz;
   fx.dt = dt; fx.Re = Re; fx.ca = 0.0; fx.cb = 1.0;
   cudaEvent_t ev[6];
@@ -1251,7 +1333,12 @@ ns3d_status ns3d_set_tiles(ns3d_solver* h, const int* tiles) {
   NS3D_TRY(check_handle(h));
   if (!tiles) return fail(h, NS3D_ERR_BAD_ARG, "null tiles");
   for (int f = 0; f < 4; ++f) {
-    if (tiles[f] != 0 && tiles[f] != 1) return fail(h, NS3D_ERR_BAD_ARG, "a tile is 0 or 1");
+    if (tiles[f] == 2 && f == ns3d::kTileInvY) {
+      if (!h->ymaps) return fail(h, NS3D_ERR_BAD_ARG, "no bulk-copy form of inv_y here");
+      continue;
+    }
+    if (tiles[f] != 0 && tiles[f] != 1)
+      return fail(h, NS3D_ERR_BAD_ARG, "a tile is 0 or 1 (2: inv_y's bulk-copy form)");
     if (tiles[f] == 1 && !ns3d::extent_has_alt_tile(family_extent(h, f)))
       return fail(h, NS3D_ERR_BAD_ARG, "no alternative tile for this extent");
   }
@@ -1267,8 +1354,10 @@ ns3d_status ns3d_autotune(ns3d_solver* h, int reps, int force, double* ms) {
   bool alt[4];
   bool any = false;
   for (int f = 0; f < 4; ++f) any |= (alt[f] = ns3d::extent_has_alt_tile(family_extent(h, f)));
+  // the inv_y family's bulk-copy tile (FP64 lines only)
+  const bool bulk = h->ymaps && h->precision == NS3D_PRECISION_FP64;
   if (ms)
-    for (int i = 0; i < 8; ++i) ms[i] = -1.0;
+    for (int i = 0; i < NS3D_TUNE_TIMES; ++i) ms[i] = -1.0;
   NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "autotune sync");
   if (!force) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -1286,9 +1375,12 @@ ns3d_status ns3d_autotune(ns3d_solver* h, int reps, int force, double* ms) {
   const ns3d_complex* u[3] = {(const ns3d_complex*)h->u2[0], (const ns3d_complex*)h->u2[1],
                               (const ns3d_complex*)h->u2[2]};
   const int saved[4] = {h->geom.tile[0], h->geom.tile[1], h->geom.tile[2], h->geom.tile[3]};
-  double t[2][5] = {};
-  for (int tile = 0; tile < (any ? 2 : 1); ++tile) {
-    for (int f = 0; f < 4; ++f) h->geom.tile[f] = alt[f] ? tile : 0;
+  double t[3][5] = {};
+  for (int tile = 0; tile < 3; ++tile) {
+    if (tile == 1 && !any) continue;
+    if (tile == 2 && !bulk) continue;
+    for (int f = 0; f < 4; ++f) h->geom.tile[f] = (tile == 1 && alt[f]) ? 1 : 0;
+    if (tile == 2) h->geom.tile[ns3d::kTileInvY] = 2;
     const ns3d_status s =
         h->precision == NS3D_PRECISION_FP32
             ? profile_passes_t<float2>(h, u[0], u[1], u[2], 1.0e-3, 100.0, reps, t[tile])
@@ -1308,6 +1400,12 @@ ns3d_status ns3d_autotune(ns3d_solver* h, int reps, int force, double* ms) {
       ms[2 * f] = t0;
       ms[2 * f + 1] = alt[f] ? t1 : -1.0;
     }
+  }
+  if (bulk) {  // inv_y's bulk-copy tile against the better of the other two
+    const double t2 = t[2][pass_of[ns3d::kTileInvY]];
+    const double tb = best[ns3d::kTileInvY] ? t[1][1] : t[0][1];
+    if (t2 < 0.98 * tb) best[ns3d::kTileInvY] = 2;
+    if (ms) ms[8] = t2;
   }
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);

@@ -69,6 +69,10 @@ struct ns3d_solver {
   double jvp_dt = 0.0, jvp_Re = 0.0;
   cudaStream_t jvp_stream = nullptr;
   int jvp_fversion = -1;
+  // tensor maps of inv_y's bulk-copy form (tile 2 of the inv_y family) over
+  // A and B; null when the extent has no such form
+  ns3d::InvYMaps* ymaps = nullptr;
+  int* dev_err = nullptr;  // device flag of the bounded mbarrier waits (0: none gave up)
   size_t bytes = 0;
   std::string err;
 };

@@ -404,7 +404,8 @@ class Solver:
     @property
     def tiles(self):
         """Tile of each pass family (inv_x, inv_y, fwd_y, fwd_x): 0 default,
-        1 alternative (see ns3d_set_tiles)."""
+        1 alternative, and for inv_y at y extents 192-512 also 2, the
+        bulk-copy (TMA) form (see ns3d_set_tiles)."""
         return _get_tiles(self._L.ns3d_get_tiles, self._h)
 
     @tiles.setter
@@ -413,9 +414,10 @@ class Solver:
         self._check(self._L.ns3d_set_tiles(self._h, t), "ns3d_set_tiles")
 
     def autotune(self, reps: int = 20, force: bool = False) -> dict:
-        """Times each pass family with both tiles and keeps the faster
-        (ns3d_autotune).  Returns {"tiles": [...], "ms": 4 x (default,
-        alternative) ms, None when a cached choice was applied}."""
+        """Times each pass family with each of its tiles and keeps the faster
+        (ns3d_autotune).  Returns {"tiles": [...], "ms": per family [default,
+        alternative] ms (inv_y adds its bulk-copy tile where it has one), None
+        when a cached choice was applied}."""
         return _autotune(self._L.ns3d_autotune, self._h, self._check, reps, force,
                          self._L.ns3d_get_tiles)
 
@@ -432,9 +434,11 @@ def _get_tiles(fn, h):
 
 
 def _autotune(fn, h, check, reps, force, get_fn):
-    ms = (ctypes.c_double * 8)()
+    ms = (ctypes.c_double * 9)()  # NS3D_TUNE_TIMES
     check(fn(h, int(reps), int(bool(force)), ms), "autotune")
     times = [[ms[2 * f], ms[2 * f + 1]] for f in range(4)]
+    if ms[8] >= 0.0:  # inv_y's bulk-copy tile
+        times[1].append(ms[8])
     timed = any(x >= 0.0 for row in times for x in row)
     return {"tiles": _get_tiles(get_fn, h), "ms": times if timed else None}
 

@@ -73,6 +73,59 @@ def test_alternative_tiles_match_the_default(torch, shape, precision):
     assert _rel(out[1][1], out[0][1], torch) < tol
 
 
+@pytest.mark.parametrize("shape", [(8, 192, 8), (16, 256, 16), (8, 384, 16), (8, 512, 8),
+                                   (24, 256, 24)])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_bulk_copy_inv_y_matches_the_default(torch, shape, precision):
+    """inv_y's tile 2: one thread per CTA loads each field's box of lines with
+    a tensor copy (FP64; the FP32 mode and the tangent form run per-thread
+    copies at the same points per thread).  Odd Mz leaves a last group of
+    lines past the end of each x plane (filled with zeros by the copy, not
+    stored); 384 takes each box in two copies of 192 rows."""
+    from ns3dperiodic_b200 import Solver
+
+    Re, dt = 200.0, 1.0e-3
+    U0, F = _state(shape, Re, 5)
+    out = []
+    for tiles in ([0, 0, 0, 0], [0, 2, 0, 0]):
+        with Solver(*shape) as S:
+            S.precision = precision
+            S.tiles = tiles
+            assert S.tiles == tiles
+            S.set_forcing(S.to_device(F))
+            U = S.rk3_ssp(S.to_device(U0), dt, Re, nsteps=3)
+            V = S.to_device([0.5 * u for u in U0])
+            Uj, Vj = S.rk3_ssp_uv(S.to_device(U0), V, dt, Re, nsteps=2)
+            S.synchronize()  # NS3D_ERR_TIMEOUT if a bounded wait gave up
+            out.append((U, Vj))
+    tol = 1e-12 if precision == "fp64" else 2e-6
+    assert _rel(out[1][0], out[0][0], torch) < tol
+    assert _rel(out[1][1], out[0][1], torch) < tol
+
+
+def test_bulk_copy_ensemble_equals_instances_alone(torch):
+    """The tensor maps cover every instance of a batch as x planes."""
+    from ns3dperiodic_b200 import Ensemble, Solver
+    from ns3dperiodic_b200 import workload as W
+
+    shape, Res = (8, 256, 8), [80.0, 160.0, 320.0]
+    states = [_state(shape, Re, 7 + b) for b, Re in enumerate(Res)]
+    E = Ensemble(len(Res), *shape)
+    E.tiles = [0, 2, 0, 0]
+    E.set_forcing(states[0][1])
+    E.set_params([1.0e-3] * len(Res), Res)
+    U = E.to_device([np.stack([st[0][c] for st in states]) for c in range(3)])
+    E.rk3_steps(U, 4)
+    with Solver(*shape) as S:
+        S.tiles = [0, 2, 0, 0]
+        S.set_forcing(S.to_device(states[0][1]))
+        for b, Re in enumerate(Res):
+            Ub = S.rk3_ssp(S.to_device(states[b][0]), 1.0e-3, Re, nsteps=4)
+            for c in range(3):
+                assert torch.equal(U[c][b], Ub[c])
+    E.close()
+
+
 def test_autotune_keeps_what_it_measured_and_caches(torch):
     from ns3dperiodic_b200 import Solver
 
@@ -92,6 +145,23 @@ def test_autotune_keeps_what_it_measured_and_caches(torch):
         assert all(t1 < 0.0 for _, t1 in r["ms"])
 
 
+def test_autotune_times_the_bulk_copy_tile(torch):
+    """inv_y's third tile is timed and kept where it is 2% faster than the
+    better of the other two."""
+    from ns3dperiodic_b200 import Solver
+
+    with Solver(16, 256, 16) as S:
+        r = S.autotune(reps=5, force=True)
+        t0, t1, t2 = r["ms"][1]
+        assert min(t0, t1, t2) > 0.0
+        best = int(t1 < 0.98 * t0)
+        want = 2 if t2 < 0.98 * (t1 if best else t0) else best
+        assert r["tiles"][1] == want and S.tiles == r["tiles"]
+        S.precision = "fp32"  # FP32 lines have no bulk-copy form to time
+        r = S.autotune(reps=3, force=True)
+        assert len(r["ms"][1]) == 2 and r["tiles"][1] in (0, 1)
+
+
 def test_set_tiles_rejects_what_the_extent_lacks(torch):
     from ns3dperiodic_b200 import Solver
     from ns3dperiodic_b200._lib import Ns3dError
@@ -100,7 +170,9 @@ def test_set_tiles_rejects_what_the_extent_lacks(torch):
         with pytest.raises(Ns3dError):
             S.tiles = [1, 0, 0, 0]  # x = 16 has no alternative
         with pytest.raises(Ns3dError):
-            S.tiles = [0, 2, 0, 0]
+            S.tiles = [0, 2, 0, 0]   # no bulk-copy form of a 64-point y line
+        with pytest.raises(Ns3dError):
+            S.tiles = [0, 0, 2, 0]   # only inv_y has a tile 2
         S.tiles = [0, 1, 1, 0]       # y = 64 has one
         assert S.tiles == [0, 1, 1, 0]
 

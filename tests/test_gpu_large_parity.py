@@ -7,7 +7,8 @@ tangent.  One and three RK3_SSP steps, one RK3_SSP_UV step and one
 single_time_step_iUV_RHS are compared with the reference's own CUDA build
 (oracle/_ref, unmodified Source/RK_time_step.cu:265-355 with cuFFT) on the
 same inputs, at 1e-12 relative L2, for the default pass tiles, the
-alternative tiles of every pass family and the tiles the autotuner picks.
+alternative tiles of every pass family, inv_y's bulk-copy (TMA) tile and the
+tiles the autotuner picks.
 512^3: one RK3 step against the reference build (the lines spread over the
 CTA, LaneMap::kSpread, and the fwd_x update without grouped loads); the two
 arms run one after the other so only one holds device memory at a time.
@@ -87,7 +88,7 @@ def _host(F):
     return [f.cpu().numpy() for f in F]
 
 
-@pytest.mark.parametrize("tiles", ["default", "alternative", "autotuned"])
+@pytest.mark.parametrize("tiles", ["default", "alternative", "bulk_copy", "autotuned"])
 def test_256_cube_against_reference_build(torch, case256, ref256, tiles):
     from ns3dperiodic_b200 import Solver
 
@@ -97,6 +98,8 @@ def test_256_cube_against_reference_build(torch, case256, ref256, tiles):
             S.tiles = [0, 0, 0, 0]
         elif tiles == "alternative":
             S.tiles = [1, 1, 1, 1]
+        elif tiles == "bulk_copy":  # inv_y fed by tensor copies (TMA)
+            S.tiles = [0, 2, 0, 0]
         else:
             S.autotune(reps=5, force=True)
         S.set_forcing(S.to_device(F))
