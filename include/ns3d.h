@@ -342,35 +342,40 @@ ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns
                                 double* ms);
 
 /* Autotuner of the pass tiles (no reference counterpart).  Each of the four
- * pipelined pass families -- 0 inv_x, 1 inv_y, 2 fwd_y, 3 fwd_x -- has a
- * default tile (16 points per thread for powers of two, 12 for multiples of
- * 3) and, for extents >= 32 (powers of two) or >= 48 (multiples of 3), an
- * alternative one (8 or 6 points per thread: twice the lines per CTA, half
- * the registers and prefetch buffers).  tiles[f] = 0 picks the default, 1
- * the alternative.  The inv_y family has a third tile, 2, for y extents of
- * 192, 256, 384 and 512: the bulk-copy form, where one thread per CTA loads
- * each field's whole box of lines into shared memory with a tensor copy (TMA)
- * instead of every thread copying its own samples (the tangent form and the
- * FP32 mode run the per-thread copies at the same points per thread).
+ * pipelined pass families -- 0 inv_x, 1 inv_y, 2 fwd_y, 3 fwd_x -- has up to
+ * five tiles:
+ *   0  the default: 16 points per thread for powers of two, 12 for multiples
+ *      of 3, with its radix schedule (16.16 at 256, 16.16.2 at 512, ...);
+ *   1  the alternative, for extents >= 32 (powers of two) or >= 48 (multiples
+ *      of 3): 8 or 6 points per thread (twice the lines per CTA, half the
+ *      registers and prefetch buffers) and their schedule (8.8.4 at 256);
+ *   2  inv_y only, y extents 192, 256, 384 and 512: the bulk-copy form, where
+ *      one thread per CTA loads each field's box of lines into shared memory
+ *      with a tensor copy (TMA) instead of every thread copying its own
+ *      samples (the tangent form and the FP32 mode run the per-thread copies
+ *      at the same points per thread);
+ *   3, 4  inv_x, inv_y and fwd_y: tile 0's or tile 1's points per thread with
+ *      the radices in reverse order (4.8.8 instead of 8.8.4 at 256, 2.16.16
+ *      instead of 16.16.2 at 512), where that order differs.
  * Different tiles change the order of the floating-point operations of the
  * transforms, so results agree to round-off, not bit for bit.  The tiles are
  * per precision; a new handle starts with the defaults. */
 #define NS3D_TILE_FAMILIES 4
-#define NS3D_TUNE_TIMES 9
+#define NS3D_TILES_PER_FAMILY 5
+#define NS3D_TUNE_TIMES 20
 ns3d_status ns3d_get_tiles(const ns3d_solver* h, int* tiles);
-/* NS3D_ERR_BAD_ARG for a value other than 0/1 (or 2 for inv_y), or a tile
- * the extent lacks.  Synchronises the handle's stream. */
+/* NS3D_ERR_BAD_ARG for a tile the family or the extent lacks.  Synchronises
+ * the handle's stream. */
 ns3d_status ns3d_set_tiles(ns3d_solver* h, const int* tiles);
 /* Times every family with each of its tiles on the handle's own scratch
  * (`reps` launches after one warm-up, CUDA events, as ns3d_profile_passes;
- * the state is not touched), keeps the alternative where it is at least 2%
- * faster, and applies the choice.  Choices are cached per process and
- * device for (Nx, Ny, Nz, batch, precision): unless `force`, a cached
- * choice is applied without timing.  ms (NS3D_TUNE_TIMES = 9 doubles, may
- * be NULL) receives per family the mean ms of the default and the
- * alternative tile, then that of inv_y's bulk-copy tile (-1: not timed).
- * The bulk-copy tile is kept where it is 2% faster than the better of the
- * other two.  Synchronous. */
+ * the state is not touched), keeps the fastest where it is at least 2%
+ * faster than the default, and applies the choice.  Choices are cached per
+ * process and device for (Nx, Ny, Nz, batch, precision): unless `force`, a
+ * cached choice is applied without timing.  ms (NS3D_TUNE_TIMES = 20
+ * doubles, may be NULL) receives the mean ms of tile t of family f at
+ * ms[5 f + t] (-1: the family has no such tile here, or it was not timed).
+ * Synchronous. */
 ns3d_status ns3d_autotune(ns3d_solver* h, int reps, int force, double* ms);
 
 /* ----------------------------------------------------------------------- */

@@ -22,7 +22,7 @@ LIB = os.path.join(HERE, "libns3d_b200.so")
 COMPAT_LIB = os.path.join(HERE, "libns3d_compat.so")
 COMPAT_SOURCE = "compat.cu"
 
-SOURCES = ["k_fwdx.cu", "k_fwdx32.cu", "k_xy.cu", "k_z.cu", "k_fft3d.cu", "aux_kernels.cu", "solver.cu",
+SOURCES = ["k_fwdx.cu", "k_fwdx32.cu", "k_xy.cu", "k_xy_rev.cu", "k_z.cu", "k_fft3d.cu", "aux_kernels.cu", "solver.cu",
            "noalloc.cu", "krylov.cu", "qr_shifts.cpp", "checkpoint.cpp",
            "diag_kernels.cu", "series.cpp", "server.cu"]
 

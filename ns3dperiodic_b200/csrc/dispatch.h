@@ -15,6 +15,22 @@ bool extent_has_alt_tile(int n);
 // lines per CTA of inv_y's bulk-copy (TMA) form (tile 2 of the inv_y family)
 // for extent n, 0 when the extent has no such form
 int inv_y_tma_lpc(int n);
+// whether the x / y families' tile 3 (default points per thread) or 4 (the
+// alternative) - the reversed radix schedule - exists for extent n
+bool rev_tile_exists(int n, int tile);
+// Tiles 3 and 4 of inv_x, inv_y and fwd_y (k_xy_rev.cu); run_inv_x etc.
+// forward to these for those tiles.
+cudaError_t run_inv_x_rev(const InvXArgs<3>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_x_rev(const InvXArgs<6>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_x_rev(const InvXArgs<3, float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_x_rev(const InvXArgs<6, float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_y_rev(const InvYArgs<3>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_y_rev(const InvYArgs<6>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_y_rev(const InvYArgs<3, float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_inv_y_rev(const InvYArgs<6, float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_fwd_y_rev(const FwdYArgs<>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t run_fwd_y_rev(const FwdYArgs<float2>& a, const PassGeom& g, cudaStream_t st);
+cudaError_t prepare_xy_rev(const PassGeom& g);
 
 // FP64 scratch (double2) and the FP32 precision mode (float2 scratch).
 cudaError_t run_inv_x(const InvXArgs<3>& a, const PassGeom& g, cudaStream_t st);

@@ -22,6 +22,7 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
 #include <utility>
 
 namespace ns3d {
@@ -388,10 +389,38 @@ struct StageTw<N, NS, RadixList<R, Rest...>> {
   }
 };
 
+// Radix schedules of one (N, P): V = 0 the plan above, V = 1 the same
+// radices in reverse order (a different first-exchange stride and padding,
+// other twiddle tables per stage); the tile autotuner times both where they
+// differ.
+template <typename L, typename Acc = RadixList<>>
+struct ReverseList;
+template <int... A>
+struct ReverseList<RadixList<>, RadixList<A...>> {
+  using type = RadixList<A...>;
+};
+template <int R, int... Rs, int... A>
+struct ReverseList<RadixList<R, Rs...>, RadixList<A...>> {
+  using type = typename ReverseList<RadixList<Rs...>, RadixList<R, A...>>::type;
+};
+template <int N, int P, int V>
+struct PlanV {
+  using L = typename Plan<N, P>::L;
+};
 template <int N, int P>
+struct PlanV<N, P, 1> {
+  using L = typename ReverseList<typename Plan<N, P>::L>::type;
+};
+// whether the reversed schedule differs from the plan (not a palindrome)
+template <int N, int P>
+__host__ __device__ constexpr bool plan_reversible() {
+  return !std::is_same<typename PlanV<N, P, 0>::L, typename PlanV<N, P, 1>::L>::value;
+}
+
+template <int N, int P, int V = 0>
 struct LineFFT {
   static constexpr int T = N / P;
-  using L = typename Plan<N, P>::L;
+  using L = typename PlanV<N, P, V>::L;
   static constexpr int PADW = FirstRadix<L>::value < 4 ? 4 : FirstRadix<L>::value;
   static constexpr int BUF = line_buf_len<N, PADW>();
   // shared-memory twiddle words the plan needs (N - first radix), at least 1

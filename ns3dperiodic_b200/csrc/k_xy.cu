@@ -9,33 +9,43 @@ bool extent_has_alt_tile(int n) { return has_alt_tile(n); }
 int inv_y_tma_lpc(int n) { return inv_y_tma_lpc_inline(n); }
 
 cudaError_t run_inv_x(const InvXArgs<3>& a, const PassGeom& g, cudaStream_t st) {
+  if (g.tile[kTileInvX] >= 3) return run_inv_x_rev(a, g, st);
   return launch_inv_x<3>(a, g, st);
 }
 cudaError_t run_inv_x(const InvXArgs<6>& a, const PassGeom& g, cudaStream_t st) {
+  if (g.tile[kTileInvX] >= 3) return run_inv_x_rev(a, g, st);
   return launch_inv_x<6>(a, g, st);
 }
 cudaError_t run_inv_y(const InvYArgs<3>& a, const PassGeom& g, cudaStream_t st) {
+  if (g.tile[kTileInvY] >= 3) return run_inv_y_rev(a, g, st);
   return launch_inv_y<3>(a, g, st);
 }
 cudaError_t run_inv_y(const InvYArgs<6>& a, const PassGeom& g, cudaStream_t st) {
+  if (g.tile[kTileInvY] >= 3) return run_inv_y_rev(a, g, st);
   return launch_inv_y<6>(a, g, st);
 }
 cudaError_t run_fwd_y(const FwdYArgs<>& a, const PassGeom& g, cudaStream_t st) {
+  if (g.tile[kTileFwdY] >= 3) return run_fwd_y_rev(a, g, st);
   return launch_fwd_y(a, g, st);
 }
 cudaError_t run_inv_x(const InvXArgs<3, float2>& a, const PassGeom& g, cudaStream_t st) {
+  if (g.tile[kTileInvX] >= 3) return run_inv_x_rev(a, g, st);
   return launch_inv_x<3>(a, g, st);
 }
 cudaError_t run_inv_x(const InvXArgs<6, float2>& a, const PassGeom& g, cudaStream_t st) {
+  if (g.tile[kTileInvX] >= 3) return run_inv_x_rev(a, g, st);
   return launch_inv_x<6>(a, g, st);
 }
 cudaError_t run_inv_y(const InvYArgs<3, float2>& a, const PassGeom& g, cudaStream_t st) {
+  if (g.tile[kTileInvY] >= 3) return run_inv_y_rev(a, g, st);
   return launch_inv_y<3>(a, g, st);
 }
 cudaError_t run_inv_y(const InvYArgs<6, float2>& a, const PassGeom& g, cudaStream_t st) {
+  if (g.tile[kTileInvY] >= 3) return run_inv_y_rev(a, g, st);
   return launch_inv_y<6>(a, g, st);
 }
 cudaError_t run_fwd_y(const FwdYArgs<float2>& a, const PassGeom& g, cudaStream_t st) {
+  if (g.tile[kTileFwdY] >= 3) return run_fwd_y_rev(a, g, st);
   return launch_fwd_y(a, g, st);
 }
 
@@ -61,7 +71,7 @@ cudaError_t prepare_xy(const PassGeom& g) {
     if (e == cudaSuccess) e = prepare_xy_prec<float2>(gt);
     if (e != cudaSuccess) return e;
   }
-  return cudaSuccess;
+  return prepare_xy_rev(g);  // tiles 3 and 4
 }
 
 }  // namespace ns3d

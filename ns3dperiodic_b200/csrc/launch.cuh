@@ -165,29 +165,68 @@ inline unsigned persistent_grid(Kern kern, size_t smem, long long groups) {
 template <typename C>
 constexpr int prec_tag() { return sizeof(C) == 16 ? 0 : 100; }
 
-template <int N, int P, int NF, typename C>
+template <int N, int P, int NF, typename C, int V = 0>
 cudaError_t launch_inv_x_p(const InvXArgs<NF, C>& a, const PassGeom& g, cudaStream_t st,
                            bool prepare_only) {
   const long long lines = (long long)g.Ny * g.Mz * nbatch(g);
-  using S = PassSmem<N, P, C, double2>;
-  const unsigned grid = persistent_grid<KTag<0, N, P, NF + prec_tag<C>()>>(
-      inv_x_kernel<N, P, NF, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);
+  using S = PassSmem<N, P, C, double2, V>;
+  const unsigned grid = persistent_grid<KTag<0, N, P, NF + prec_tag<C>() + 1000 * V>>(
+      inv_x_kernel<N, P, NF, C, V>, S::BYTES, (lines + S::LPC - 1) / S::LPC);
   if (prepare_only) return cudaGetLastError();
-  inv_x_kernel<N, P, NF, C><<<grid, kThreads, S::BYTES, st>>>(a, g);
+  inv_x_kernel<N, P, NF, C, V><<<grid, kThreads, S::BYTES, st>>>(a, g);
   return cudaGetLastError();
 }
 
-template <int NF, typename C>
+// The x / y families' tiles 3 and 4: the default and the alternative points
+// per thread with the reversed radix schedule, where it differs.
+template <int N>
+constexpr bool rev_tile_default() {
+  return plan_reversible<N, p_xy(N)>();
+}
+template <int N>
+constexpr bool rev_tile_alt() {
+  if constexpr (p_alt(N) > 0) {
+    return plan_reversible<N, p_alt(N)>();
+  } else {
+    return false;
+  }
+}
+inline bool rev_tile_exists_inline(int n, int tile) {
+  switch (n) {
+#define NS3D_CASE(N) \
+  case N:            \
+    return tile == 3 ? rev_tile_default<N>() : (tile == 4 ? rev_tile_alt<N>() : false);
+    NS3D_FOR_EACH_EXTENT(NS3D_CASE)
+#undef NS3D_CASE
+    default:
+      return false;
+  }
+}
+
+// V = 0: tiles 0 and 1; V = 1: tiles 3 and 4 (the reversed schedules)
+template <int NF, typename C, int V = 0>
 cudaError_t launch_inv_x(const InvXArgs<NF, C>& a, const PassGeom& g, cudaStream_t st,
                          bool prepare_only = false) {
+  const int tile = g.tile[kTileInvX];
   switch (g.Nx) {
-#define NS3D_CASE(N)                                                         \
-  case N:                                                                    \
-    if constexpr (p_alt(N) > 0) {                                            \
-      if (g.tile[kTileInvX])                                                 \
-        return launch_inv_x_p<N, p_alt(N), NF, C>(a, g, st, prepare_only);   \
-    }                                                                        \
-    return launch_inv_x_p<N, p_xy(N), NF, C>(a, g, st, prepare_only);
+#define NS3D_CASE(N)                                                                \
+  case N:                                                                           \
+    if constexpr (V == 0) {                                                         \
+      if constexpr (p_alt(N) > 0) {                                                 \
+        if (tile == 1) return launch_inv_x_p<N, p_alt(N), NF, C>(a, g, st, prepare_only); \
+      }                                                                             \
+      return launch_inv_x_p<N, p_xy(N), NF, C>(a, g, st, prepare_only);             \
+    } else {                                                                        \
+      if constexpr (rev_tile_alt<N>()) {                                            \
+        if (tile == 4)                                                              \
+          return launch_inv_x_p<N, p_alt(N), NF, C, 1>(a, g, st, prepare_only);     \
+      }                                                                             \
+      if constexpr (rev_tile_default<N>()) {                                        \
+        if (tile == 3)                                                              \
+          return launch_inv_x_p<N, p_xy(N), NF, C, 1>(a, g, st, prepare_only);      \
+      }                                                                             \
+      return cudaErrorInvalidValue;                                                 \
+    }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE
     default:
@@ -216,40 +255,52 @@ cudaError_t launch_inv_y_tma(const InvYArgs<3, double2>& a, const PassGeom& g, c
   return cudaGetLastError();
 }
 
-template <int N, int P, int NF, typename C>
+template <int N, int P, int NF, typename C, int V = 0>
 cudaError_t launch_inv_y_p(const InvYArgs<NF, C>& a, const PassGeom& g, cudaStream_t st,
                            bool prepare_only, bool bulk = false) {
-  if constexpr (NF == 3 && sizeof(C) == 16 && P == p_tma(N)) {
+  if constexpr (V == 0 && NF == 3 && sizeof(C) == 16 && P == p_tma(N)) {
     if (bulk && (a.maps || prepare_only)) {
       const cudaError_t e = launch_inv_y_tma<N, P>(a, g, st, prepare_only);
       if (!prepare_only || e != cudaSuccess) return e;
     }
   }
   const long long lines = (long long)g.Nx * g.Mz;
-  using S = PassSmem<N, P, C, C>;
-  const unsigned grid = persistent_grid<KTag<1, N, P, NF + prec_tag<C>()>>(
-      inv_y_kernel<N, P, NF, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);
+  using S = PassSmem<N, P, C, C, V>;
+  const unsigned grid = persistent_grid<KTag<1, N, P, NF + prec_tag<C>() + 1000 * V>>(
+      inv_y_kernel<N, P, NF, C, V>, S::BYTES, (lines + S::LPC - 1) / S::LPC);
   if (prepare_only) return cudaGetLastError();
-  inv_y_kernel<N, P, NF, C><<<grid, kThreads, S::BYTES, st>>>(a, g);
+  inv_y_kernel<N, P, NF, C, V><<<grid, kThreads, S::BYTES, st>>>(a, g);
   return cudaGetLastError();
 }
 
-template <int NF, typename C>
+template <int NF, typename C, int V = 0>
 cudaError_t launch_inv_y(const InvYArgs<NF, C>& a, const PassGeom& gi, cudaStream_t st,
                          bool prepare_only = false) {
   const PassGeom g = planes_geom(gi);
+  const int tile = g.tile[kTileInvY];
   switch (g.Ny) {
-#define NS3D_CASE(N)                                                         \
-  case N:                                                                    \
-    if constexpr (p_tma(N) > 0) {                                            \
-      if (g.tile[kTileInvY] == 2)                                            \
-        return launch_inv_y_p<N, p_tma(N), NF, C>(a, g, st, prepare_only, true); \
-    }                                                                        \
-    if constexpr (p_alt(N) > 0) {                                            \
-      if (g.tile[kTileInvY] == 1)                                            \
-        return launch_inv_y_p<N, p_alt(N), NF, C>(a, g, st, prepare_only);   \
-    }                                                                        \
-    return launch_inv_y_p<N, p_xy(N), NF, C>(a, g, st, prepare_only);
+#define NS3D_CASE(N)                                                                \
+  case N:                                                                           \
+    if constexpr (V == 0) {                                                         \
+      if constexpr (p_tma(N) > 0) {                                                 \
+        if (tile == 2)                                                              \
+          return launch_inv_y_p<N, p_tma(N), NF, C>(a, g, st, prepare_only, true);  \
+      }                                                                             \
+      if constexpr (p_alt(N) > 0) {                                                 \
+        if (tile == 1) return launch_inv_y_p<N, p_alt(N), NF, C>(a, g, st, prepare_only); \
+      }                                                                             \
+      return launch_inv_y_p<N, p_xy(N), NF, C>(a, g, st, prepare_only);             \
+    } else {                                                                        \
+      if constexpr (rev_tile_alt<N>()) {                                            \
+        if (tile == 4)                                                              \
+          return launch_inv_y_p<N, p_alt(N), NF, C, 1>(a, g, st, prepare_only);     \
+      }                                                                             \
+      if constexpr (rev_tile_default<N>()) {                                        \
+        if (tile == 3)                                                              \
+          return launch_inv_y_p<N, p_xy(N), NF, C, 1>(a, g, st, prepare_only);      \
+      }                                                                             \
+      return cudaErrorInvalidValue;                                                 \
+    }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE
     default:
@@ -356,30 +407,40 @@ cudaError_t launch_fwd_x(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t s
   }
 }
 
-template <int N, int P, typename C>
+template <int N, int P, typename C, int V = 0>
 cudaError_t launch_fwd_y_p(const FwdYArgs<C>& a, const PassGeom& g, cudaStream_t st,
                            bool prepare_only) {
   const long long lines = (long long)g.Nx * g.Mz;
-  using S = PassSmem<N, P, C, C>;
-  const unsigned grid = persistent_grid<KTag<20, N, P, prec_tag<C>()>>(
-      fwd_y_kernel<N, P, C>, S::BYTES, (lines + S::LPC - 1) / S::LPC);
+  using S = PassSmem<N, P, C, C, V>;
+  const unsigned grid = persistent_grid<KTag<20, N, P, prec_tag<C>() + 1000 * V>>(
+      fwd_y_kernel<N, P, C, V>, S::BYTES, (lines + S::LPC - 1) / S::LPC);
   if (prepare_only) return cudaGetLastError();
-  fwd_y_kernel<N, P, C><<<grid, kThreads, S::BYTES, st>>>(a, g);
+  fwd_y_kernel<N, P, C, V><<<grid, kThreads, S::BYTES, st>>>(a, g);
   return cudaGetLastError();
 }
 
-template <typename C>
+template <typename C, int V = 0>
 cudaError_t launch_fwd_y(const FwdYArgs<C>& a, const PassGeom& gi, cudaStream_t st,
                          bool prepare_only = false) {
   const PassGeom g = planes_geom(gi);
+  const int tile = g.tile[kTileFwdY];
   switch (g.Ny) {
-#define NS3D_CASE(N)                                                      \
-  case N:                                                                 \
-    if constexpr (p_alt(N) > 0) {                                         \
-      if (g.tile[kTileFwdY])                                              \
-        return launch_fwd_y_p<N, p_alt(N), C>(a, g, st, prepare_only);    \
-    }                                                                     \
-    return launch_fwd_y_p<N, p_xy(N), C>(a, g, st, prepare_only);
+#define NS3D_CASE(N)                                                                \
+  case N:                                                                           \
+    if constexpr (V == 0) {                                                         \
+      if constexpr (p_alt(N) > 0) {                                                 \
+        if (tile == 1) return launch_fwd_y_p<N, p_alt(N), C>(a, g, st, prepare_only); \
+      }                                                                             \
+      return launch_fwd_y_p<N, p_xy(N), C>(a, g, st, prepare_only);                 \
+    } else {                                                                        \
+      if constexpr (rev_tile_alt<N>()) {                                            \
+        if (tile == 4) return launch_fwd_y_p<N, p_alt(N), C, 1>(a, g, st, prepare_only); \
+      }                                                                             \
+      if constexpr (rev_tile_default<N>()) {                                        \
+        if (tile == 3) return launch_fwd_y_p<N, p_xy(N), C, 1>(a, g, st, prepare_only); \
+      }                                                                             \
+      return cudaErrorInvalidValue;                                                 \
+    }
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
 #undef NS3D_CASE
     default:

@@ -59,8 +59,10 @@ struct PassGeom {
   // the x passes split their line index into (instance, y*Mz + z).  0 or 1:
   // a single instance.
   int batch;
-  // Tile choice per pipelined pass family (TileFamily): 0 the default points
-  // per thread, 1 the alternative (p_alt), set by the autotuner.
+  // Tile choice per pipelined pass family (TileFamily), set by the autotuner:
+  // 0 the default points per thread, 1 the alternative (p_alt), 2 inv_y's
+  // bulk-copy form, 3 / 4 the default / alternative points per thread with
+  // the reversed radix schedule (x / y families inv_x, inv_y, fwd_y).
   int tile[4];
 };
 enum TileFamily { kTileInvX = 0, kTileInvY = 1, kTileFwdY = 2, kTileFwdX = 3 };
@@ -200,9 +202,10 @@ constexpr size_t align16(size_t b) { return (b + 15) / 16 * 16; }
 // Dynamic shared memory of a pipelined pass: the stage twiddles and the line
 // buffers in the line precision C, then each thread's double buffer of
 // prefetched elements of type E (the pass's input, FP64 state or scratch).
-template <int N, int P, typename C = double2, typename E = C>
+// V: the radix schedule (PlanV).
+template <int N, int P, typename C = double2, typename E = C, int V = 0>
 struct PassSmem {
-  using F = LineFFT<N, P>;
+  using F = LineFFT<N, P, V>;
   using LM = LaneMap<F::T>;
   static constexpr int LPC = LM::LPC;
   static constexpr int STRIDE = line_stride(F::BUF, xy_stride_target<F::T>());
@@ -243,9 +246,9 @@ struct InvXArgs {
   const double2* tw;
 };
 
-template <int NX, int P, int NF, typename C>
+template <int NX, int P, int NF, typename C, int V = 0>
 __global__ void __launch_bounds__(kThreads, min_ctas_xy(P)) inv_x_kernel(InvXArgs<NF, C> a, PassGeom g) {
-  using S = PassSmem<NX, P, C, double2>;
+  using S = PassSmem<NX, P, C, double2, V>;
   using F = typename S::F;
   using LM = typename S::LM;
   using Rt = RealOf<C>;
@@ -354,9 +357,9 @@ struct InvYArgs {
   int* err = nullptr;  // error flag of the bulk-copy form's bounded waits
 };
 
-template <int NY, int P, int NF, typename C>
+template <int NY, int P, int NF, typename C, int V = 0>
 __global__ void __launch_bounds__(kThreads, min_ctas_xy(P)) inv_y_kernel(InvYArgs<NF, C> a, PassGeom g) {
-  using S = PassSmem<NY, P, C, C>;
+  using S = PassSmem<NY, P, C, C, V>;
   using F = typename S::F;
   using LM = typename S::LM;
   using Rt = RealOf<C>;
@@ -1019,9 +1022,9 @@ struct FwdYArgs {
   const double2* tw;
 };
 
-template <int NY, int P, typename C>
+template <int NY, int P, typename C, int V = 0>
 __global__ void __launch_bounds__(kThreads, min_ctas_xy(P)) fwd_y_kernel(FwdYArgs<C> a, PassGeom g) {
-  using S = PassSmem<NY, P, C, C>;
+  using S = PassSmem<NY, P, C, C, V>;
   using F = typename S::F;
   using LM = typename S::LM;
   constexpr int T = F::T;

@@ -1312,6 +1312,27 @@ int family_extent(const ns3d_solver* h, int f) {
   return (f == ns3d::kTileInvX || f == ns3d::kTileFwdX) ? h->Nx : h->Ny;
 }
 
+// whether family f (TileFamily) has tile `tile` on this handle: 0 always; 1
+// the alternative points per thread; 2 inv_y's bulk-copy form (tensor maps
+// built); 3 / 4 the reversed radix schedule of the default / alternative
+// points per thread (inv_x, inv_y, fwd_y)
+bool tile_exists(const ns3d_solver* h, int f, int tile) {
+  const int n = family_extent(h, f);
+  switch (tile) {
+    case 0:
+      return true;
+    case 1:
+      return ns3d::extent_has_alt_tile(n);
+    case 2:
+      return f == ns3d::kTileInvY && h->ymaps != nullptr;
+    case 3:
+    case 4:
+      return f != ns3d::kTileFwdX && ns3d::rev_tile_exists(n, tile);
+    default:
+      return false;
+  }
+}
+
 void apply_tiles(ns3d_solver* h, const int* tiles) {
   drop_graph(h);  // a captured step holds the previous kernels
   for (int f = 0; f < 4; ++f) {
@@ -1333,14 +1354,10 @@ ns3d_status ns3d_set_tiles(ns3d_solver* h, const int* tiles) {
   NS3D_TRY(check_handle(h));
   if (!tiles) return fail(h, NS3D_ERR_BAD_ARG, "null tiles");
   for (int f = 0; f < 4; ++f) {
-    if (tiles[f] == 2 && f == ns3d::kTileInvY) {
-      if (!h->ymaps) return fail(h, NS3D_ERR_BAD_ARG, "no bulk-copy form of inv_y here");
-      continue;
-    }
-    if (tiles[f] != 0 && tiles[f] != 1)
-      return fail(h, NS3D_ERR_BAD_ARG, "a tile is 0 or 1 (2: inv_y's bulk-copy form)");
-    if (tiles[f] == 1 && !ns3d::extent_has_alt_tile(family_extent(h, f)))
-      return fail(h, NS3D_ERR_BAD_ARG, "no alternative tile for this extent");
+    if (tiles[f] < 0 || tiles[f] >= NS3D_TILES_PER_FAMILY)
+      return fail(h, NS3D_ERR_BAD_ARG, "a tile is 0 .. 4");
+    if (!tile_exists(h, f, tiles[f]))
+      return fail(h, NS3D_ERR_BAD_ARG, "no such tile for this family and extent");
   }
   NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "tiles sync");
   apply_tiles(h, tiles);
@@ -1351,11 +1368,13 @@ ns3d_status ns3d_autotune(ns3d_solver* h, int reps, int force, double* ms) {
   NS3D_TRY(check_handle(h));
   if (reps < 1) return fail(h, NS3D_ERR_BAD_ARG, "reps must be >= 1");
   const std::array<int, 6> key = {h->device, h->Nx, h->Ny, h->Nz, h->batch, h->precision};
-  bool alt[4];
-  bool any = false;
-  for (int f = 0; f < 4; ++f) any |= (alt[f] = ns3d::extent_has_alt_tile(family_extent(h, f)));
-  // the inv_y family's bulk-copy tile (FP64 lines only)
-  const bool bulk = h->ymaps && h->precision == NS3D_PRECISION_FP64;
+  constexpr int kT = NS3D_TILES_PER_FAMILY;
+  // the tiles each family has here (the bulk-copy tile is timed for FP64 lines)
+  bool has[4][kT];
+  for (int f = 0; f < 4; ++f)
+    for (int tile = 0; tile < kT; ++tile)
+      has[f][tile] = tile_exists(h, f, tile) &&
+                     (tile != 2 || h->precision == NS3D_PRECISION_FP64);
   if (ms)
     for (int i = 0; i < NS3D_TUNE_TIMES; ++i) ms[i] = -1.0;
   NS3D_CHECK(h, cudaStreamSynchronize(h->stream), "autotune sync");
@@ -1368,19 +1387,22 @@ ns3d_status ns3d_autotune(ns3d_solver* h, int reps, int force, double* ms) {
     }
   }
   // time every pass with each tile on the handle's own scratch: zeros in
-  // u2 stand for the state, fwd_x writes u1 (profile_passes_t)
+  // u2 stand for the state, fwd_x writes u1 (profile_passes_t).  Round r
+  // runs tile r in every family that has it, the default elsewhere.
   const size_t fb = sizeof(double2) * h->nc * (size_t)h->batch;
   for (int c = 0; c < 3; ++c)
     NS3D_CHECK(h, cudaMemsetAsync(h->u2[c], 0, fb, h->stream), "autotune input");
   const ns3d_complex* u[3] = {(const ns3d_complex*)h->u2[0], (const ns3d_complex*)h->u2[1],
                               (const ns3d_complex*)h->u2[2]};
   const int saved[4] = {h->geom.tile[0], h->geom.tile[1], h->geom.tile[2], h->geom.tile[3]};
-  double t[3][5] = {};
-  for (int tile = 0; tile < 3; ++tile) {
-    if (tile == 1 && !any) continue;
-    if (tile == 2 && !bulk) continue;
-    for (int f = 0; f < 4; ++f) h->geom.tile[f] = (tile == 1 && alt[f]) ? 1 : 0;
-    if (tile == 2) h->geom.tile[ns3d::kTileInvY] = 2;
+  double t[kT][5] = {};
+  for (int tile = 0; tile < kT; ++tile) {
+    bool any = tile == 0;
+    for (int f = 0; f < 4; ++f) {
+      h->geom.tile[f] = has[f][tile] ? tile : 0;
+      any |= has[f][tile];
+    }
+    if (!any) continue;
     const ns3d_status s =
         h->precision == NS3D_PRECISION_FP32
             ? profile_passes_t<float2>(h, u[0], u[1], u[2], 1.0e-3, 100.0, reps, t[tile])
@@ -1390,22 +1412,19 @@ ns3d_status ns3d_autotune(ns3d_solver* h, int reps, int force, double* ms) {
       return s;
     }
   }
-  // pass index of each family in profile_passes_t: inv_x 0, inv_y 1, fwd_y 3, fwd_x 4
+  // pass index of each family in profile_passes_t: inv_x 0, inv_y 1, fwd_y 3, fwd_x 4;
+  // the fastest tile, kept if at least 2% faster than the default
   const int pass_of[4] = {0, 1, 3, 4};
   std::array<int, 4> best{};
   for (int f = 0; f < 4; ++f) {
-    const double t0 = t[0][pass_of[f]], t1 = t[1][pass_of[f]];
-    best[f] = (alt[f] && t1 < 0.98 * t0) ? 1 : 0;  // the default unless 2% faster
-    if (ms) {
-      ms[2 * f] = t0;
-      ms[2 * f + 1] = alt[f] ? t1 : -1.0;
-    }
-  }
-  if (bulk) {  // inv_y's bulk-copy tile against the better of the other two
-    const double t2 = t[2][pass_of[ns3d::kTileInvY]];
-    const double tb = best[ns3d::kTileInvY] ? t[1][1] : t[0][1];
-    if (t2 < 0.98 * tb) best[ns3d::kTileInvY] = 2;
-    if (ms) ms[8] = t2;
+    const double t0 = t[0][pass_of[f]];
+    int b = 0;
+    for (int tile = 1; tile < kT; ++tile)
+      if (has[f][tile] && t[tile][pass_of[f]] < t[b][pass_of[f]]) b = tile;
+    best[f] = t[b][pass_of[f]] < 0.98 * t0 ? b : 0;
+    if (ms)
+      for (int tile = 0; tile < kT; ++tile)
+        ms[kT * f + tile] = (tile == 0 || has[f][tile]) ? t[tile][pass_of[f]] : -1.0;
   }
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);

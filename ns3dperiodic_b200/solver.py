@@ -404,8 +404,10 @@ class Solver:
     @property
     def tiles(self):
         """Tile of each pass family (inv_x, inv_y, fwd_y, fwd_x): 0 default,
-        1 alternative, and for inv_y at y extents 192-512 also 2, the
-        bulk-copy (TMA) form (see ns3d_set_tiles)."""
+        1 alternative points per thread, 2 inv_y's bulk-copy (TMA) form
+        (y extents 192-512), 3 / 4 the default / alternative points per
+        thread with the reversed radix schedule (inv_x, inv_y, fwd_y; see
+        ns3d_set_tiles)."""
         return _get_tiles(self._L.ns3d_get_tiles, self._h)
 
     @tiles.setter
@@ -414,10 +416,10 @@ class Solver:
         self._check(self._L.ns3d_set_tiles(self._h, t), "ns3d_set_tiles")
 
     def autotune(self, reps: int = 20, force: bool = False) -> dict:
-        """Times each pass family with each of its tiles and keeps the faster
-        (ns3d_autotune).  Returns {"tiles": [...], "ms": per family [default,
-        alternative] ms (inv_y adds its bulk-copy tile where it has one), None
-        when a cached choice was applied}."""
+        """Times each pass family with each of its tiles and keeps the fastest
+        where it beats the default by 2% (ns3d_autotune).  Returns {"tiles":
+        [...], "ms": per family {tile: ms} of the tiles timed, None when a
+        cached choice was applied}."""
         return _autotune(self._L.ns3d_autotune, self._h, self._check, reps, force,
                          self._L.ns3d_get_tiles)
 
@@ -433,13 +435,15 @@ def _get_tiles(fn, h):
     return list(t)
 
 
+TILES_PER_FAMILY = 5  # NS3D_TILES_PER_FAMILY
+
+
 def _autotune(fn, h, check, reps, force, get_fn):
-    ms = (ctypes.c_double * 9)()  # NS3D_TUNE_TIMES
+    ms = (ctypes.c_double * (4 * TILES_PER_FAMILY))()  # NS3D_TUNE_TIMES
     check(fn(h, int(reps), int(bool(force)), ms), "autotune")
-    times = [[ms[2 * f], ms[2 * f + 1]] for f in range(4)]
-    if ms[8] >= 0.0:  # inv_y's bulk-copy tile
-        times[1].append(ms[8])
-    timed = any(x >= 0.0 for row in times for x in row)
+    times = [{t: ms[TILES_PER_FAMILY * f + t] for t in range(TILES_PER_FAMILY)
+              if ms[TILES_PER_FAMILY * f + t] >= 0.0} for f in range(4)]
+    timed = any(row for row in times)
     return {"tiles": _get_tiles(get_fn, h), "ms": times if timed else None}
 
 
