@@ -312,10 +312,12 @@ template <int N, typename C>
 cudaError_t launch_z_stash(const ZArgs<3, C>& a, const PassGeom& g, cudaStream_t st) {
   constexpr int P = p_zst(N);
   using S = ZStashSmem<N, P, C>;
+  constexpr bool TM = z_tmem(N);
+  constexpr size_t bytes = TM ? S::TM_BYTES : S::BYTES;
   const long long lines = (long long)g.Nx * g.Ny;
   const unsigned grid = persistent_grid<KTag<40, N, P, prec_tag<C>()>>(
-      z_kernel_st<N, P, C>, S::BYTES, blocks_for(lines, lines_per_cta_z<N, P>()));
-  z_kernel_st<N, P, C><<<grid, kThreads, S::BYTES, st>>>(a, g);
+      z_kernel_st<N, P, C, TM>, bytes, blocks_for(lines, lines_per_cta_z<N, P>()));
+  z_kernel_st<N, P, C, TM><<<grid, kThreads, bytes, st>>>(a, g);
   return cudaGetLastError();
 }
 

@@ -22,6 +22,7 @@
 
 #include "fft_engine.cuh"
 #include "tma.cuh"
+#include "tmem.cuh"
 
 namespace ns3d {
 
@@ -924,9 +925,32 @@ struct ZStashSmem {
   static constexpr size_t ST_OFF = align16(SBUF_OFF + (size_t)LM::LPC * F::BUF * sizeof(C));
   static constexpr size_t BYTES = ST_OFF + (size_t)3 * P * kThreads * sizeof(Rt);
   static_assert(BYTES <= 113 * 1024, "two CTAs per SM");
+  // The TMEM form (NS3D_Z_TMEM) keeps the stash in tensor memory instead:
+  // TM_COLS columns per CTA (3 P doubles per thread = 6 P words, rounded up
+  // to a power of two).  Its launch asks for at least TM_BYTES of shared
+  // memory, which caps the CTAs per SM that hold columns at
+  // kTmemColsPerSm / TM_COLS, so an allocation never waits for good.
+  static constexpr uint32_t TM_COLS = 6 * P <= 32 ? 32 : (6 * P <= 64 ? 64 : (6 * P <= 128 ? 128 : 256));
+  static constexpr int TM_MAXCTAS = (int)(kTmemColsPerSm / TM_COLS);
+  static constexpr size_t TM_BYTES =
+      BYTES > (228 * 1024) / (TM_MAXCTAS + 1) + 1 ? BYTES : (228 * 1024) / (TM_MAXCTAS + 1) + 1;
+  static_assert(sizeof(Rt) == 8, "the TMEM form holds FP64 stash words in pairs");
+  static_assert(P % 4 == 0 && 6 * P <= 256, "TMEM stash columns");
+  static_assert((TM_BYTES + 1024) * (TM_MAXCTAS + 1) > 228 * 1024, "CTAs per SM bound");
 };
 
-template <int NZ, int P, typename C>
+// Where the nonlinear term's z pass keeps its velocity stash: 0 in shared
+// memory, 1 in tensor memory, 2 in tensor memory for z extents from 512.
+// Measured on a B200 (z pass per launch, shared / tensor memory): 128^3
+// 69.4 / 71.5 us, 256^3 453.5 / 457 us, 512^3 4553 / 4453 us.
+#ifndef NS3D_Z_TMEM
+#define NS3D_Z_TMEM 2
+#endif
+__host__ __device__ constexpr bool z_tmem(int nz) {
+  return NS3D_Z_TMEM == 1 || (NS3D_Z_TMEM == 2 && nz >= 512);
+}
+
+template <int NZ, int P, typename C, bool TM = false>
 __global__ void __launch_bounds__(kThreads, kMinCtasZ) z_kernel_st(ZArgs<3, C> a, PassGeom g) {
   using F = LineFFT<NZ, P>;
   using Rt = RealOf<C>;
@@ -935,8 +959,19 @@ __global__ void __launch_bounds__(kThreads, kMinCtasZ) z_kernel_st(ZArgs<3, C> a
   using LM = ZLaneMap<T>;
   constexpr int PW = z_pw<NZ, P, C>();
   extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ uint32_t tm_base_s;  // TMEM address of the CTA's columns (TM)
+  const int warp = threadIdx.x >> 5;
+  if constexpr (TM) {
+    if (warp == 0) tmem_alloc_warp(&tm_base_s, S::TM_COLS);
+    tmem_fence_before_sync();
+  }
   C* tw_s = (C*)dsm;
-  F::load_tw(tw_s, a.tw);
+  F::load_tw(tw_s, a.tw);  // ends with a CTA barrier: the TMEM address is published
+  uint32_t tm = 0;         // this warp's lane quarter, column 0
+  if constexpr (TM) {
+    tmem_fence_after_sync();
+    tm = tmem_addr(tm_base_s, 32 * (warp & 3), 0);
+  }
   int li, t;
   LM::get(li, t);
   const int nb = g.Nx * g.Ny;
@@ -956,29 +991,73 @@ __global__ void __launch_bounds__(kThreads, kMinCtasZ) z_kernel_st(ZArgs<3, C> a
   auto ux = [&](int s) -> Rt& { return stash[(0 * P + s) * kThreads]; };
   auto uy = [&](int s) -> Rt& { return stash[(1 * P + s) * kThreads]; };
   auto uz = [&](int s) -> Rt& { return stash[(2 * P + s) * kThreads]; };
+  // stash component c (0 u_x, 1 u_y, 2 u_z): the P values v(s)
+  auto park = [&](int c, auto v) {
+    if constexpr (TM) {
+#pragma unroll
+      for (int s0 = 0; s0 < P; s0 += 4) {
+        uint32_t r[8];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const double d = v(s0 + k);
+          r[2 * k] = (uint32_t)__double2loint(d);
+          r[2 * k + 1] = (uint32_t)__double2hiint(d);
+        }
+        tmem_st8(tm + (uint32_t)(c * 2 * P + 2 * s0), r);
+      }
+      tmem_wait_st();
+    } else {
+#pragma unroll
+      for (int s = 0; s < P; ++s) stash[(c * P + s) * kThreads] = v(s);
+    }
+  };
   const Rt sc = (Rt)g.inv_vol;
   const Rt kfz = (Rt)g.kfz;
   C w[P];
   Rt q0[P], q1[P];
+  // q[s] = u_x(s) (w[s].x sc) + u_y(s) (w[s].y sc) + u_z(s) q[s]  (calc_vels_nabla_vels)
+  auto product = [&](Rt (&q)[P]) {
+    if constexpr (TM) {
+#pragma unroll
+      for (int s0 = 0; s0 < P; s0 += 4) {
+        uint32_t rx[8], ry[8], rz[8];
+        tmem_ld8(tm + (uint32_t)(0 * 2 * P + 2 * s0), rx);
+        tmem_ld8(tm + (uint32_t)(1 * 2 * P + 2 * s0), ry);
+        tmem_ld8(tm + (uint32_t)(2 * 2 * P + 2 * s0), rz);
+        tmem_wait_ld();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int s = s0 + k;
+          const Rt vx = __hiloint2double((int)rx[2 * k + 1], (int)rx[2 * k]);
+          const Rt vy = __hiloint2double((int)ry[2 * k + 1], (int)ry[2 * k]);
+          const Rt vz = __hiloint2double((int)rz[2 * k + 1], (int)rz[2 * k]);
+          q[s] = vx * (w[s].x * sc) + vy * (w[s].y * sc) + vz * q[s];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < P; ++s)
+        q[s] = ux(s) * (w[s].x * sc) + uy(s) * (w[s].y * sc) + uz(s) * q[s];
+    }
+  };
   // (u_x, u_y)
   if (NS3D_Z_L2PF == 2 && threadIdx.x == 0) pf(2);  // C2
   load_pair<NZ, P, false, false>(w, a.C[0], a.C[1], base, t, kfz);
   F::template run<+1, PW>(w, t, sbuf, tw_s);
-#pragma unroll
-  for (int s = 0; s < P; ++s) { ux(s) = w[s].x * sc; uy(s) = w[s].y * sc; }
+  park(0, [&](int s) { return w[s].x * sc; });
+  park(1, [&](int s) { return w[s].y * sc; });
   // (u_z, d_z u_z); q0 accumulates Q_z first
   if (NS3D_Z_L2PF == 2 && threadIdx.x < 2) pf(3 + threadIdx.x);  // E2, D2
   load_pair<NZ, P, false, true>(w, a.C[2], a.C[2], base, t, kfz);
   F::template run<+1, PW>(w, t, sbuf, tw_s);
+  park(2, [&](int s) { return w[s].x * sc; });
 #pragma unroll
-  for (int s = 0; s < P; ++s) { uz(s) = w[s].x * sc; q0[s] = w[s].y * sc; }
-  // Q_z = u_x d_x u_z + u_y d_y u_z + u_z d_z u_z  (calc_vels_nabla_vels)
+  for (int s = 0; s < P; ++s) q0[s] = w[s].y * sc;
+  // Q_z = u_x d_x u_z + u_y d_y u_z + u_z d_z u_z
   if (NS3D_Z_L2PF == 2 && threadIdx.x < 2) pf(5 + threadIdx.x);  // E0, D0
   load_pair<NZ, P, false, false>(w, a.E[2], a.D[2], base, t, kfz);
   F::template run<+1, PW>(w, t, sbuf, tw_s);
-#pragma unroll
-  for (int s = 0; s < P; ++s)
-    q0[s] = ux(s) * (w[s].x * sc) + uy(s) * (w[s].y * sc) + uz(s) * q0[s];
+  product(q0);
   // R2C of Q_z alone
 #pragma unroll
   for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], (Rt)0);
@@ -998,19 +1077,22 @@ __global__ void __launch_bounds__(kThreads, kMinCtasZ) z_kernel_st(ZArgs<3, C> a
   if (NS3D_Z_L2PF == 2 && threadIdx.x < 2) pf(7 + threadIdx.x);  // E1, D1
   load_pair<NZ, P, false, false>(w, a.E[0], a.D[0], base, t, kfz);
   F::template run<+1, PW>(w, t, sbuf, tw_s);
-#pragma unroll
-  for (int s = 0; s < P; ++s)
-    q0[s] = ux(s) * (w[s].x * sc) + uy(s) * (w[s].y * sc) + uz(s) * q0[s];
+  product(q0);
   load_pair<NZ, P, false, false>(w, a.E[1], a.D[1], base, t, kfz);
   F::template run<+1, PW>(w, t, sbuf, tw_s);
-#pragma unroll
-  for (int s = 0; s < P; ++s)
-    q1[s] = ux(s) * (w[s].x * sc) + uy(s) * (w[s].y * sc) + uz(s) * q1[s];
+  product(q1);
   // R2C of (Q_x, Q_y) packed
 #pragma unroll
   for (int s = 0; s < P; ++s) w[s] = mkc<C>(q0[s], q1[s]);
   F::template run<-1, PW>(w, t, sbuf, tw_s);
   store_pair_spectrum<NZ, P>(w, sbuf, t, a.Qh[0], a.Qh[1], base, valid);
+  if constexpr (TM) {
+    // every thread's TMEM reads have completed (waited); free the columns
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    if (warp == 0) tmem_dealloc_warp(tm_base_s, S::TM_COLS);
+  }
 }
 
 // ---------------------------------------------------------------------------
