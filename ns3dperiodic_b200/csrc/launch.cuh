@@ -56,6 +56,11 @@ constexpr int p_z32(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PZ32); }
 #define NS3D_PLINE 16
 #endif
 constexpr int p_line(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PLINE); }
+// points per thread of the plain transforms' z passes (pairs of real lines)
+#ifndef NS3D_PZPLAIN
+#define NS3D_PZPLAIN 8
+#endif
+constexpr int p_zplain(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PZPLAIN); }
 // The autotuner's alternative tile of the pipelined x / y passes: 8 points
 // per thread for powers of two from 32, 6 for multiples of 3 from 48 (twice
 // the lines per CTA, half the registers and prefetch buffers); 0: none.
@@ -478,7 +483,7 @@ cudaError_t launch_z_plain(const ZPlainArgs& a, const PassGeom& g, cudaStream_t 
   switch (g.Nz) {
 #define NS3D_CASE(N)                                                                  \
   case N: {                                                                           \
-    constexpr int P = p_z(N);                                                         \
+    constexpr int P = p_zplain(N);                                                    \
     const unsigned grid = blocks_for(pairs, lines_per_cta_z<N, P>());                 \
     if (C2R)                                                                          \
       z_c2r_kernel<N, P><<<grid, kWarpsPerCta * 32, 0, st>>>(a, g);                   \
