@@ -349,7 +349,7 @@ ns3d_status ns3d_profile_passes(ns3d_solver* h, const ns3d_complex* ux, const ns
  *   1  the alternative, for extents >= 32 (powers of two) or >= 48 (multiples
  *      of 3): 8 or 6 points per thread (twice the lines per CTA, half the
  *      registers and prefetch buffers) and their schedule (8.8.4 at 256);
- *   2  inv_y only, y extents 192, 256, 384 and 512: the bulk-copy form, where
+ *   2  inv_y only, y extents from 48: the bulk-copy form, where
  *      one thread per CTA loads each field's box of lines into shared memory
  *      with a tensor copy (TMA) instead of every thread copying its own
  *      samples (the tangent form and the FP32 mode run the per-thread copies

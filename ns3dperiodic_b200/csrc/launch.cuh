@@ -80,7 +80,7 @@ inline bool has_alt_tile(int n) {
 }
 
 // The bulk-copy (TMA) form of inv_y (inv_y_tma_kernel): FP64 lines spread
-// over the CTA.  It is tile 2 of the inv_y family, at p_tma(n) points per
+// over the CTA (y extents from 48).  It is tile 2 of the inv_y family, at p_tma(n) points per
 // thread (the default or the alternative points per thread, whichever
 // spreads its lines over the CTA; 0: no such form for this extent), and runs
 // where the handle built tensor maps for its scratch; the tangent form and
@@ -96,8 +96,8 @@ inline bool has_alt_tile(int n) {
 #endif
 constexpr int p_tma(int n) {
   return NS3D_Y_TMA == 0                              ? 0
-         : n / p_xy(n) >= 32                          ? p_xy(n)
-         : (p_alt(n) > 0 && n / p_alt(n) >= 32) ? p_alt(n)
+         : n / p_xy(n) >= NS3D_SPREAD_T                          ? p_xy(n)
+         : (p_alt(n) > 0 && n / p_alt(n) >= NS3D_SPREAD_T) ? p_alt(n)
                                                       : 0;
 }
 

@@ -84,16 +84,24 @@ __device__ __forceinline__ int signed_idx(int j, int n) { return j < (n >> 1) ? 
 
 // Thread -> (line slot, t) for passes whose batch index is contiguous in
 // memory: lanes with the same t and consecutive lines are adjacent, so a warp
-// reads runs of consecutive elements of each row.  Lines of fewer than 32
-// threads stay inside a warp (LPW lines per warp, synchronised per warp).
-// Lines of 32 threads or more are interleaved over the whole CTA (line
-// threadIdx % LPC, t = threadIdx / LPC, synchronised per CTA): with one line
-// per warp every 16-byte load would sit alone in its 32-byte sector.
+// reads runs of consecutive elements of each row.  Lines of NS3D_SPREAD_T
+// threads or more are interleaved over the whole CTA (line threadIdx % LPC,
+// t = threadIdx / LPC, synchronised per CTA), so the LPC = 128 / T lines of
+// a CTA put LPC x 16 contiguous bytes of each row into one load: 64 bytes
+// for 32-thread lines, 128 for 16, 256 for 8.  Narrower lines stay inside
+// their warp (LPW lines per warp, synchronised per warp).  Measured on a B200
+// (us per launch, 16 points per thread, lines of 16 threads: 32-byte rows
+// inside a warp -> 128-byte rows over the CTA): 256^3 inv_x 294 -> 217,
+// inv_y 535 -> 440, fwd_y 182 -> 151; 128^3 (8 threads, 32 -> 256 bytes)
+// inv_y 64.5 -> 58.8; the extra CTA barriers cost less than the narrow rows.
+#ifndef NS3D_SPREAD_T
+#define NS3D_SPREAD_T 8
+#endif
 template <int T>
 struct LaneMap {
-  static constexpr bool kSpread = T >= 32;
+  static constexpr bool kSpread = T >= NS3D_SPREAD_T;
   static constexpr int LPW = T < 32 ? 32 / T : 1;
-  static constexpr int LPC = T < 32 ? kWarpsPerCta * LPW : (kWarpsPerCta * 32) / T;
+  static constexpr int LPC = (kWarpsPerCta * 32) / T;
   static constexpr int SW = kSpread ? kWarpsPerCta * 32 : T;  // line_sync width
   // lines side by side in the lanes of one load
   static constexpr int ADJ = kSpread ? LPC : LPW;

@@ -405,7 +405,7 @@ class Solver:
     def tiles(self):
         """Tile of each pass family (inv_x, inv_y, fwd_y, fwd_x): 0 default,
         1 alternative points per thread, 2 inv_y's bulk-copy (TMA) form
-        (y extents 192-512), 3 / 4 the default / alternative points per
+        (y extents from 48), 3 / 4 the default / alternative points per
         thread with the reversed radix schedule (inv_x, inv_y, fwd_y; see
         ns3d_set_tiles)."""
         return _get_tiles(self._L.ns3d_get_tiles, self._h)

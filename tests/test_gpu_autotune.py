@@ -74,7 +74,7 @@ def test_alternative_tiles_match_the_default(torch, shape, precision):
 
 
 @pytest.mark.parametrize("shape", [(8, 192, 8), (16, 256, 16), (8, 384, 16), (8, 512, 8),
-                                   (24, 256, 24)])
+                                   (24, 256, 24), (16, 64, 24), (8, 48, 8), (8, 128, 16)])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_bulk_copy_inv_y_matches_the_default(torch, shape, precision):
     """inv_y's tile 2: one thread per CTA loads each field's box of lines with
@@ -195,6 +195,7 @@ def test_autotune_keeps_what_it_measured_and_caches(torch):
             assert r["tiles"][f] == want
         assert set(r["ms"][3]) == {0, 1}                     # fwd_x: two tiles
         assert set(r["ms"][0]) == {0, 1, 3}                  # 64: 16.4 reverses, 8.8 does not
+        assert set(r["ms"][1]) == {0, 1, 2, 3}               # inv_y adds the bulk copy
         assert S.tiles == r["tiles"]
         with Solver(64, 64, 64) as S2:
             r2 = S2.autotune()
@@ -226,11 +227,12 @@ def test_set_tiles_rejects_what_the_extent_lacks(torch):
     from ns3dperiodic_b200 import Solver
     from ns3dperiodic_b200._lib import Ns3dError
 
+    with Solver(16, 32, 16) as S:
+        with pytest.raises(Ns3dError):
+            S.tiles = [0, 2, 0, 0]   # 32-point y lines never span 8 threads: no bulk copy
     with Solver(16, 64, 16) as S:
         with pytest.raises(Ns3dError):
             S.tiles = [1, 0, 0, 0]  # x = 16 has no alternative
-        with pytest.raises(Ns3dError):
-            S.tiles = [0, 2, 0, 0]   # no bulk-copy form of a 64-point y line
         with pytest.raises(Ns3dError):
             S.tiles = [0, 0, 2, 0]   # only inv_y has a tile 2
         with pytest.raises(Ns3dError):
