@@ -349,7 +349,9 @@ def run_ours(args, world, rank, local, pg):
     # the kernels the step launches: the nonlinear term's z pass with the
     # velocities in shared memory for FP64 lines; the ring-pipelined fwd_x
     # where a line fits in a warp (8 points per thread, 12 for multiples of 3)
-    ring = N // (12 if N % 3 == 0 else min(N, 8)) <= 32
+    t_ring = N // (12 if N % 3 == 0 else min(N, 8))
+    t_plain = N // (12 if N % 3 == 0 else min(N, 16))
+    ring = t_ring <= 32 and (t_ring == 32 or t_plain < 8)
     # inv_y's tile 2 is the bulk-copy (TMA) form for FP64 lines
     ytma = S.tiles[1] == 2 and not fp32
     kname = {0: "inv_x_kernel", 1: "inv_y_tma_kernel" if ytma else "inv_y_kernel",

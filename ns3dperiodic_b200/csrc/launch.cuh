@@ -378,6 +378,16 @@ cudaError_t launch_fwd_x_p(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t
 #endif
 constexpr int p_fxr(int n) { return n % 3 == 0 ? 12 : p_pow2(n, NS3D_PFXR); }
 constexpr int nslot_fxr(int p) { return p > 8 ? 3 : NS3D_FX_SLOTS; }
+// The ring where its lines are a warp wide (64-byte rows over the CTA), or
+// where fwd_x_kernel's own lines would stay inside their warps; elsewhere
+// fwd_x_kernel's lines, interleaved over the CTA, read wider rows than the
+// ring's.  Per plain launch on a B200: 256^3 ring 295 us, fwd_x_kernel (16
+// points) 383 us; 128^3 ring 65.5 us, fwd_x_kernel 61.7 us.
+template <int N, typename C>
+constexpr bool fx_use_ring() {
+  return NS3D_FX_RING && N / p_fxr(N) <= 32 && (NS3D_FX_RING32 || sizeof(C) == 16) &&
+         (N / p_fxr(N) == 32 || N / p_fx(N) < NS3D_SPREAD_T);
+}
 
 template <int N, int P, int MODE, bool COMBINE, typename C>
 cudaError_t launch_fwd_x_ring(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t st,
@@ -404,7 +414,7 @@ cudaError_t launch_fwd_x(const FwdXArgs<C>& a, const PassGeom& g, cudaStream_t s
       if (g.tile[kTileFwdX])                                                          \
         return launch_fwd_x_p<N, p_alt(N), MODE, COMBINE, C>(a, g, st, prepare_only); \
     }                                                                                 \
-    if constexpr (NS3D_FX_RING && N / p_fxr(N) <= 32 && (NS3D_FX_RING32 || sizeof(C) == 16)) \
+    if constexpr (fx_use_ring<N, C>())                                                \
       return launch_fwd_x_ring<N, p_fxr(N), MODE, COMBINE, C>(a, g, st, prepare_only); \
     return launch_fwd_x_p<N, p_fx(N), MODE, COMBINE, C>(a, g, st, prepare_only);
     NS3D_FOR_EACH_EXTENT(NS3D_CASE)
