@@ -80,6 +80,15 @@ ns3d_status ns3d_synchronize(ns3d_solver* h);
 const char* ns3d_last_error(const ns3d_solver* h);
 const char* ns3d_status_string(ns3d_status s);
 
+/* Self-test of the bounded device waits (no reference counterpart): one CTA
+ * waits, with the waits the tensor-copy (TMA) passes use, on an mbarrier
+ * phase that nothing completes.  The wait gives up after about 0.1 s, writes
+ * the timeout code to a device flag and the kernel returns, leaving the
+ * context usable.  *seconds (may be NULL) receives the time the launch
+ * took.  NS3D_OK when the wait gave up and flagged it, NS3D_ERR_CUDA
+ * otherwise.  Synchronous on the current device; allocates a 4-byte flag. */
+ns3d_status ns3d_selftest_bounded_wait(double* seconds);
+
 /* Device bytes the handle holds (scratch + tables). */
 size_t ns3d_device_bytes(const ns3d_solver* h);
 

@@ -26,7 +26,7 @@ STATUS = {
 
 # every symbol include/ns3d.h declares
 EXPORTS = (
-    "ns3d_create", "ns3d_destroy", "ns3d_supported_extent", "ns3d_set_stream",
+    "ns3d_create", "ns3d_destroy", "ns3d_supported_extent", "ns3d_selftest_bounded_wait", "ns3d_set_stream",
     "ns3d_synchronize", "ns3d_last_error", "ns3d_status_string", "ns3d_device_bytes",
     "ns3d_set_forcing", "ns3d_forcing_modes", "ns3d_rk3_step", "ns3d_rk3_steps",
     "ns3d_euler_step", "ns3d_rhs", "ns3d_convolution", "ns3d_convolution_uv",
@@ -145,6 +145,7 @@ def _sig(lib):
                          ctypes.POINTER(c_void_p)], c_int),
         "ns3d_destroy": ([_P], c_int),
         "ns3d_supported_extent": ([c_int], c_int),
+        "ns3d_selftest_bounded_wait": ([_P], c_int),
         "ns3d_set_stream": ([_P, _P], c_int),
         "ns3d_synchronize": ([_P], c_int),
         "ns3d_last_error": ([_P], ctypes.c_char_p),

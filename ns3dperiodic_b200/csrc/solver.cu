@@ -290,6 +290,50 @@ ns3d_status ns3d_mask_cutoff(int Nx, int Ny, int Nz, double Lx, double Ly, doubl
   return build_mask_cutoff(Nx, Ny, Nz, Lx, Ly, Lz, qcut) ? NS3D_OK : NS3D_ERR_BAD_ARG;
 }
 
+extern "C++" {
+namespace {
+// One CTA waits on a phase of an mbarrier that nothing arrives on.
+__global__ void bounded_wait_probe(int* err) {
+  __shared__ uint64_t bar;
+  __shared__ int bad;
+  if (threadIdx.x == 0) {
+    ns3d::mbar_init(&bar, 1);
+    bad = 0;
+  }
+  __syncthreads();
+  ns3d::mbar_wait(&bar, 0, err, &bad);
+}
+}  // namespace
+}  // extern "C++"
+
+ns3d_status ns3d_selftest_bounded_wait(double* seconds) {
+  int* flag = nullptr;
+  if (cudaMalloc(&flag, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    return NS3D_ERR_OOM;
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int got = 0;
+  cudaError_t e = cudaMemset(flag, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    cudaEventRecord(e0);
+    bounded_wait_probe<<<1, 64>>>(flag);
+    cudaEventRecord(e1);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  if (e == cudaSuccess) e = cudaMemcpy(&got, flag, sizeof(int), cudaMemcpyDeviceToHost);
+  float ms = 0.f;
+  if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(flag);
+  if (seconds) *seconds = 1e-3 * ms;
+  return (e == cudaSuccess && got == ns3d::kErrTimeout) ? NS3D_OK : NS3D_ERR_CUDA;
+}
+
 ns3d_status ns3d_twiddles(int N, double* tw) {
   if (N <= 0 || !tw) return NS3D_ERR_BAD_ARG;
   std::vector<double2> t;
